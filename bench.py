@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Benchmark: full fcgrid core index + densest search on one seeded graph.
+
+A step is one pass of the hot path over the graph: the core index of every
+node for every lambda (the whole fcgrid), then the densest-subgraph search
+(beta = 1.0).  The default workload is the 2.5M-node / 34M-edge / 4-layer
+Chung-Lu configuration (gamma = 2.1, 50% layer copy).  The metric is
+edge-visits/s: one lambda column removes every node once and visits all of
+its adjacency, so a full fcgrid is L * 2M edge visits (M = undirected edges
+summed over layers).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is device-timed with CUDA events on the launching stream (graph
+resident in HBM); `e2e` is the same step through the public API from pinned
+host memory, with the upload and the table read-back inside the timed region.
+Under torchrun every rank runs its own copy of the workload (no collective
+in the data path; weak scaling) and rank 0 prints the max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fcgrid time & edge-visits/s, batched vs plain GPU (bit-exact), vs ParGrid CPU"
+UNIT = "edge-visits/s"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3"])
+    ap.add_argument("--beta", type=float, default=1.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def describe(name):
+    from pargridcpu_b200 import synth
+    c = synth.CONFIGS[name]
+    if c["kind"] == "chung_lu":
+        return (f"{name}: Chung-Lu n={c['n']:,} L={c['L']} {c['m']:,} edges/layer gamma={c['gamma']}"
+                f" copy={c['copy']} seed={c['seed']}; full fcgrid + densest(beta)")
+    return (f"{name}: Erdos-Renyi n={c['n']} L={c['L']} p~U[{c['p_lo']},{c['p_hi']}] "
+            f"seed={c['seed']}; full fcgrid + densest(beta)")
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return json.load(open(p))["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic(workload):
+    """DRAM bytes per peel launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", f"peel_{workload}_traffic.json")
+    if os.path.exists(p):
+        return json.load(open(p)).get("dram_bytes_per_launch")
+    return None
+
+
+def cpu_baseline(layers, L, visits, beta, steps=1, warmup=0):
+    """The reference's own ParGrid + WdsList (compiled from its sources into
+    oracle/_ref) on this host's cores, on the same graph."""
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    if not os.path.exists(harness):
+        return None, "oracle/_ref/ref_harness not built"
+    from pargridcpu_b200 import synth
+    cores = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as d:
+        fcg = os.path.join(d, "g.fcg")
+        synth.write_fcg(synth.Graph(layers), fcg)
+        env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+        r = subprocess.run([harness, fcg, "bench", str(steps), str(warmup), repr(beta), str(cores)],
+                           capture_output=True, text=True, env=env, timeout=3000)
+    if r.returncode != 0:
+        return None, r.stderr.strip()[-300:]
+    runs = [json.loads(x[5:]) for x in r.stdout.splitlines() if x.startswith("STEP ")]
+    timed = [x for x in runs if not x["warmup"]] or runs
+    secs = [x["pargrid_s"] + x["wdslist_s"] for x in timed]
+    mean = sum(secs) / len(secs)
+    return {"value": visits / mean, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"{len(timed)} run(s) of the reference ParGrid (full fcgrid) + WdsList "
+                      f"(beta={beta}) on the same graph, OpenMP threads={cores}; its own "
+                      f"timers (load excluded)",
+            "pargrid_s": statistics.mean(x["pargrid_s"] for x in timed),
+            "wdslist_s": statistics.mean(x["wdslist_s"] for x in timed),
+            "densest": {k: timed[-1][k] for k in ("density", "k", "lmd", "len")}}, None
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from pargridcpu_b200 import synth
+    g = synth.config_graph(args.workload)
+    import oracle as O  # noqa: F401  (the checker package, for the loader restatement)
+    og = O.OracleGraph(g.layers)
+    L = og.L
+    m2 = int(og.layer_m().sum())
+    visits = L * m2
+    base, err = cpu_baseline(g.layers, L, visits, args.beta, steps=args.steps, warmup=args.warmup)
+    if base is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return
+    secs = visits / base["value"]
+    line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": secs * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": describe(args.workload), "n": og.n, "L": L,
+                       "directed_entries": m2, "beta": args.beta},
+            "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "detail": {"pargrid_s": base["pargrid_s"], "wdslist_s": base["wdslist_s"],
+                       "densest": base["densest"]}}
+    print(json.dumps(line))
+
+
+def run_ours(args, world, rank, local):
+    import torch
+    from pargridcpu_b200 import MultilayerGraph, launch_count, synth
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    gen = synth.config_graph(args.workload)
+    g = MultilayerGraph.from_pairs(gen.layers)
+    n, L = g.n, g.L
+    m2 = int(g.layer_m().sum())
+    visits = L * m2
+    stream = torch.cuda.Stream(device=dev)
+    beta = [args.beta]
+
+    def step():
+        g.reset_results()
+        g.coreindex(stream=stream, copy=False)
+        return g.densest(beta, stream=stream)[0]
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    g.upload(stream=stream)
+    for _ in range(args.warmup):
+        step()
+    clocks = Clocks(local)
+    barrier()
+    clocks.start()
+    time.sleep(0.3)
+    l0 = launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    peel_ms, peel_launches, dens_ms = [], [], []
+    ev0.record(stream)
+    res = None
+    for _ in range(args.steps):
+        res = step()
+        st = g.stats()
+        peel_ms.append(st["peel_ms"])
+        peel_launches.append(st["peel_launches"])
+        dens_ms.append(st["densest_ms"])
+    ev1.record(stream)
+    barrier()
+    launches = launch_count() - l0
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * visits * args.steps / (ms / 1e3)
+    stats = g.stats()
+
+    # e2e: through the public API from pinned host memory, upload + read-back inside
+    e2e = None
+    if not args.no_e2e:
+        out_t = torch.empty((L, n), dtype=torch.int32, pin_memory=True)
+        out = out_t.numpy().view(np.uint32)
+        h2d = L * (n + 1) * 8 + m2 * 4
+        d2h = L * n * 4 + 48
+
+        def e2e_step():
+            g.release_device()
+            g.upload(stream=stream)
+            g.coreindex(out=out, stream=stream)
+            return g.densest(beta, stream=stream)[0]
+
+        for _ in range(max(1, min(args.warmup, 2))):
+            e2e_step()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record(stream)
+        barrier()
+        ems = e0.elapsed_time(e1)
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([ems], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": world * visits * args.steps / (ems / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": ems / args.steps}
+
+    if rank != 0:
+        return
+    # roofline of the dominant kernel (the peel): algorithmic bytes per launch
+    # (per lambda column: 4*2M adjacency + 4*L*(n+1) offsets + 2*4*L*n degree
+    # table + 4*n core output) over the mean CUDA-event launch time
+    cols = stats["columns_per_launch"] or L
+    per_col = 4 * m2 + 4 * L * (n + 1) + 8 * L * n + 4 * n
+    bytes_per_launch = cols * per_col
+    launch_ms = statistics.mean(p / max(1, q) for p, q in zip(peel_ms, peel_launches))
+    achieved = bytes_per_launch / (launch_ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = committed_traffic(args.workload)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded; shapes of the named configuration)",
+            "config": {"workload": describe(args.workload), "n": n, "L": L,
+                       "directed_entries": m2, "edge_visits_per_step": visits,
+                       "beta": args.beta,
+                       "l2": f"inputs larger than L2 (adjacency {m2 * 4 / 2**20:.0f} MiB > 126 MiB)"
+                       if m2 * 4 > L2_BYTES else "inputs smaller than L2 (no flush)",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "k_peel", "peak_kind": peak_kind,
+                         "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms},
+            "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+            "detail": {"peel_ms_per_step": statistics.mean(peel_ms),
+                       "densest_ms_per_step": statistics.mean(dens_ms),
+                       "levels": stats["levels"], "subrounds": stats["subrounds"],
+                       "densest": {k: res[k] for k in ("k", "lmd", "length", "lstar", "density",
+                                                       "max_density_f")}}}
+    if world == 1 and not args.no_cpu_baseline:
+        base, err = cpu_baseline(gen.layers, L, visits, args.beta)
+        if base is not None:
+            line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind",
+                                                         "sample")}
+            line["detail"]["cpu_baseline_s"] = {"pargrid_s": base["pargrid_s"],
+                                                "wdslist_s": base["wdslist_s"]}
+        else:
+            line["cpu_baseline"] = None
+            line["detail"]["cpu_baseline_error"] = err
+    print(json.dumps(line))
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_setup()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

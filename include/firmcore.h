@@ -1,0 +1,217 @@
+/* firmcore.h -- C ABI of the B200 FirmCore engine (libfirmcore.so).
+ *
+ * FirmCore decomposition of a multilayer graph: L layers over one node set,
+ * each layer an undirected simple graph.  The (k,lambda)-FirmCore C_{k,l} is
+ * the largest node set in which every node has at least lambda layers with
+ * degree >= k inside the set; core_lambda(v) = max{k : v in C_{k,lambda}}
+ * (0 when no such k).  The engine computes the full fcgrid table core_lambda(v)
+ * for lambda = 1..L and every node, and the densest-subgraph search over every
+ * non-empty cell, on one NVIDIA B200 (sm_100a).
+ *
+ * Conventions
+ *   - Plain C types only.  `stream` arguments are cudaStream_t passed as
+ *     void* (NULL = the legacy default stream).
+ *   - Node ids are the reference loader's internal ids: 0..n-1 in order of
+ *     first appearance (layer by layer in file order, u before v); fc_graph_id2vtx
+ *     maps them back to the ids in the input.
+ *   - Tables are lambda-major: out[(lambda-1)*n + v] = core_lambda(v).
+ *   - Caller allocates every output buffer; the library owns the graph handle
+ *     and all device memory behind it; every handle is freed explicitly.
+ *   - Every entry point returns fc_status; nothing aborts the process.  There
+ *     is no CPU fallback: with no usable CUDA device the compute entry points
+ *     return FC_ERR_NO_DEVICE.
+ *   - Calls on different handles are independent and may run concurrently
+ *     from different host threads; calls on one handle must not overlap.
+ */
+#ifndef FIRMCORE_H
+#define FIRMCORE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FC_ABI_VERSION 1
+
+typedef enum fc_status {
+    FC_OK = 0,
+    FC_ERR_IO = 1,          /* a file could not be read or written */
+    FC_ERR_PARSE = 2,       /* malformed input */
+    FC_ERR_OOM = 3,         /* host or device allocation failed */
+    FC_ERR_BUDGET = 4,      /* request larger than the device-memory budget */
+    FC_ERR_DEVICE = 5,      /* a CUDA call failed */
+    FC_ERR_ITER_LIMIT = 6,  /* a device loop or wait hit its bound */
+    FC_ERR_INVALID = 7,     /* bad argument or call order */
+    FC_ERR_TOO_LARGE = 8,   /* graph exceeds the 32-bit index limits below */
+    FC_ERR_NO_DEVICE = 9    /* no CUDA device */
+} fc_status;
+
+/* Opaque multilayer graph: host CSR, and device CSR once uploaded. */
+typedef struct fc_graph fc_graph;
+
+/* Result of the densest-subgraph search for one beta. */
+typedef struct fc_densest_result {
+    double beta;
+    double density;        /* FP64 density of the winning cell (its layer_density) */
+    float max_density_f;   /* the float running maximum the reference prints */
+    uint32_t k, lmd;       /* winning cell (0, 0 when the graph has no edges) */
+    uint32_t length;       /* |C_{k,lmd}| */
+    uint32_t lstar;        /* number of selected layers */
+    uint32_t n_cells;      /* non-empty cells searched */
+} fc_densest_result;
+
+/* One non-empty fcgrid cell with its best density. */
+typedef struct fc_cell {
+    uint32_t k, lmd, length, lstar;
+    double density;
+} fc_cell;
+
+const char* fc_status_string(fc_status s);
+int fc_abi_version(void);
+
+/* ---- loading -------------------------------------------------------------
+ * Replaces MultilayerGraph::LoadFromFile + SetGraphOrder
+ * (Graph/MultilayerGraph.cpp:65-102, 9-45; Graph/MultilayerGraph.h:26-28) and
+ * Graph::BuildFromEdgeLst (Graph/Graph.cpp:17-50).  `dir` holds mlg.conf (one
+ * layer file name per non-empty line) and the layer files of `u v` lines.
+ * Same parse, self-loop and duplicate removal, and first-seen id remap as the
+ * reference.  With write_vtx_map != 0 the map is written to dir/__vtx_map.txt
+ * as the reference does (`u uid` lines).  `order` is the -o layer order
+ * (0 keep, 1/2 density ascending/descending, 3/4 edge count ascending/
+ * descending); it permutes the layers, which changes no result. */
+fc_status fc_graph_load_dir(const char* dir, int order, int write_vtx_map, fc_graph** out);
+
+/* Same semantics from raw pairs in memory: pairs holds every layer's
+ * interleaved (u,v) raw ids, layer after layer; m[l] pairs in layer l. */
+fc_status fc_graph_from_pairs(uint32_t n_layers, const uint64_t* m, const uint32_t* pairs,
+                              fc_graph** out);
+
+/* From the reference's in-memory form (Graph::adj_lst_buf, Graph/Graph.cpp:
+ * 20-47): for each layer l, adj_lst_buf[l] holds n rows [deg, nbr_1..nbr_deg]
+ * (internal ids, neighbours ascending, no duplicates), n + m[l] entries where
+ * m[l] is the layer's directed entry count (Graph::m). */
+fc_status fc_graph_from_adjbuf(uint32_t n, uint32_t n_layers, const uint32_t* const* adj_lst_buf,
+                               const uint64_t* m, fc_graph** out);
+
+void fc_graph_free(fc_graph* g);
+uint32_t fc_graph_n(const fc_graph* g);
+uint32_t fc_graph_layers(const fc_graph* g);
+/* directed entry count of layer l (the reference's Graph::getM) */
+uint64_t fc_graph_layer_m(const fc_graph* g, uint32_t l);
+/* original id of every internal id (MultilayerGraph::LoadId2VtxMap) */
+fc_status fc_graph_id2vtx(const fc_graph* g, uint64_t* out);
+/* layer order after -o (MultilayerGraph::GetOrder) */
+fc_status fc_graph_order(const fc_graph* g, uint32_t* out);
+/* per-layer CSR, layer by layer in the current order:
+ * off[l*(n+1) + v] .. off[l*(n+1) + v + 1] index adj (internal ids). */
+fc_status fc_graph_csr(const fc_graph* g, uint64_t* off, uint32_t* adj);
+
+/* ---- device residency ----------------------------------------------------
+ * Copies the graph to the device and builds the node-major CSR the kernels
+ * read.  Called implicitly by the compute entry points; explicit calls let a
+ * caller time or overlap the upload.  Limits: n*L < 2^32 and total directed
+ * entries < 2^32 (FC_ERR_TOO_LARGE otherwise). */
+fc_status fc_graph_upload(fc_graph* g, void* stream);
+fc_status fc_graph_release_device(fc_graph* g);
+/* drop the resident core table and densest state but keep the device CSR:
+ * the next compute call recomputes them */
+fc_status fc_graph_reset_results(fc_graph* g);
+/* bytes of device memory the graph holds now (CSR + resident results) */
+uint64_t fc_graph_device_bytes(const fc_graph* g);
+
+/* ---- core index ----------------------------------------------------------
+ * The full fcgrid table.  Replaces the table-producing methods behind -m
+ * ParGrid / ParGridPlus / CoreIndex / ParCoreIndex: FCSyncLeft::Execute and
+ * ExecuteMix (CoreParallel/FCSyncLeft.h:18,34), CoreIndex::Execute and
+ * ExecuteParallel (CoreIndexParallel/CoreIndex.h:15-17).  All four compute
+ * the same table; the reference keeps it in trees or drops it, this call
+ * returns it.  out: L*n uint32, host memory when out_on_device == 0 (the call
+ * then returns after the copy), device memory otherwise (the call is then
+ * asynchronous on `stream`).  The table stays resident for fc_densest. */
+fc_status fc_coreindex(fc_graph* g, uint32_t* out, int out_on_device, void* stream);
+
+/* ---- densest subgraph ----------------------------------------------------
+ * Replaces FCPathLevelLeft::Execute(mg, tree, true, beta) + FCTree::
+ * WeightDenestSubgraph (Core/FCPathLevelLeft.h:14, Core/FCTree.h:66) as used
+ * by -m WdsList (main.cpp:402-424).  Every non-empty cell C_{k,lmd} is scored
+ * (e_(l)/|C|) * l^beta over its layers sorted by edge count, the best l per
+ * cell is kept, and the cells are compared in the reference's order with its
+ * float running maximum.  Runs fc_coreindex first when the table is not
+ * resident.  One result per beta. */
+fc_status fc_densest(fc_graph* g, const double* betas, uint32_t n_betas, fc_densest_result* res,
+                     void* stream);
+/* Node set (ascending internal ids, res->length entries) and layer set
+ * (ascending layer indices, res->lstar entries) of a result from fc_densest
+ * on the same graph.  Either pointer may be NULL. */
+fc_status fc_densest_members(fc_graph* g, const fc_densest_result* res, uint32_t* nodes,
+                             uint32_t* layers, void* stream);
+/* Every non-empty cell with its best density for `beta`, in the reference's
+ * order (lambda-major, k ascending), as its fcgrid trees hold them
+ * (coreNode / coreNodeP: k, lmd, length, layer_density, num_select_layer).
+ * Writes min(cap, count) cells; *count receives the total. */
+fc_status fc_cells(fc_graph* g, double beta, fc_cell* cells, uint32_t cap, uint32_t* count,
+                   void* stream);
+
+/* ---- batch ---------------------------------------------------------------
+ * Many graphs at once: all (graph, lambda) columns in one persistent kernel
+ * launch that pulls work items from a device queue, captured in a CUDA graph,
+ * plus the densest search for `beta` on every graph.  tables[i] (host, may be
+ * NULL) receives graph i's L*n table, res[i] (may be NULL) its densest result.
+ * The equivalent of running the reference once per graph. */
+typedef struct fc_batch_options {
+    uint32_t block_threads;    /* 0 = autotuned */
+    uint32_t hub_threshold;    /* adjacency length above which a node is split; 0 = autotuned */
+    int use_cuda_graph;        /* capture the launch sequence in a CUDA graph (default 1) */
+} fc_batch_options;
+
+fc_status fc_batch_run(fc_graph* const* graphs, uint32_t count, double beta,
+                       uint32_t* const* tables, fc_densest_result* res,
+                       const fc_batch_options* opt, void* stream);
+
+/* ---- serving -------------------------------------------------------------
+ * A continuous-batching request loop: requests (a graph + beta) are admitted
+ * while their device footprint fits the budget and a slot is free, their work
+ * overlaps on the device with requests already running, and each completes
+ * independently.  Results are identical to fc_coreindex + fc_densest on the
+ * graph alone. */
+typedef struct fc_server fc_server;
+
+typedef struct fc_server_options {
+    uint64_t hbm_budget_bytes;  /* admission budget (0 = 150 GB) */
+    uint32_t max_inflight;      /* concurrent requests on the device (0 = 16) */
+} fc_server_options;
+
+fc_status fc_server_create(const fc_server_options* opt, fc_server** out);
+/* Enqueue a request.  The graph must stay alive until the request completes;
+ * table (host, L*n, may be NULL) and res (may be NULL) are filled on
+ * completion.  *ticket identifies it. */
+fc_status fc_server_submit(fc_server* s, fc_graph* g, double beta, uint32_t* table,
+                           fc_densest_result* res, uint64_t* ticket);
+/* Wait up to timeout_ms (negative = forever) for a ticket; FC_ERR_ITER_LIMIT
+ * on timeout.  *status receives the request's own status. */
+fc_status fc_server_wait(fc_server* s, uint64_t ticket, int64_t timeout_ms, fc_status* status,
+                         double* latency_ms);
+fc_status fc_server_destroy(fc_server* s);
+
+/* ---- diagnostics ---------------------------------------------------------
+ * Timings of the last fc_coreindex / fc_densest on a graph, taken with CUDA
+ * events recorded around the kernels on the stream they ran on, and the
+ * number of kernels this library has launched in the process. */
+typedef struct fc_stats {
+    double peel_ms;          /* peel kernels of the last table computation */
+    double densest_ms;       /* histogram + scoring kernels of the last fc_densest */
+    uint32_t peel_launches;  /* peel launches (one per column group) */
+    uint32_t levels;         /* peel levels, summed over column groups */
+    uint32_t subrounds;      /* peel sub-rounds, summed over column groups */
+    uint32_t columns_per_launch;
+} fc_stats;
+
+fc_status fc_graph_stats(const fc_graph* g, fc_stats* out);
+uint64_t fc_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FIRMCORE_H */

@@ -1,0 +1,226 @@
+// extern "C" entry points of libfirmcore.so (declared in include/firmcore.h)
+// and the table driver that runs the peel over column groups.
+#include <atomic>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "device.h"
+
+namespace fc {
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launch(uint32_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
+fc_status coreindex(fc_graph* g, uint32_t* out, bool out_on_device, cudaStream_t s) {
+    FC_TRY(upload(g, s));
+    DeviceGraph* d = g->dev;
+    if (!d->table_valid) {
+        invalidate_densest(d);
+        d->stats.peel_ms = 0;
+        d->stats.peel_launches = d->stats.levels = d->stats.subrounds = 0;
+        if (d->n && d->L) {
+            const uint32_t per = peel_columns_per_group(d);
+            d->stats.columns_per_launch = per;
+            for (uint32_t c0 = 0; c0 < d->L; c0 += per) {
+                uint32_t nc = d->L - c0 < per ? d->L - c0 : per;
+                PeelStats st;
+                FC_TRY(peel_columns(d, c0, nc, s, &st));
+                d->stats.peel_ms += st.ms;
+                d->stats.peel_launches++;
+                d->stats.levels += st.levels;
+                d->stats.subrounds += st.subrounds;
+            }
+        }
+        d->table_valid = true;
+    }
+    if (out) {
+        uint64_t bytes = (uint64_t)d->n * d->L * 4;
+        if (bytes) {
+            FC_CUDA_TRY(cudaMemcpyAsync(out, d->table, bytes,
+                                        out_on_device ? cudaMemcpyDeviceToDevice
+                                                      : cudaMemcpyDeviceToHost,
+                                        s));
+            if (!out_on_device) FC_CUDA_TRY(cudaStreamSynchronize(s));
+        }
+    }
+    return FC_OK;
+}
+
+}  // namespace fc
+
+using namespace fc;
+
+static fc_graph* new_graph() { return new (std::nothrow) fc_graph(); }
+
+extern "C" {
+
+const char* fc_status_string(fc_status s) {
+    switch (s) {
+        case FC_OK: return "ok";
+        case FC_ERR_IO: return "i/o error";
+        case FC_ERR_PARSE: return "malformed input";
+        case FC_ERR_OOM: return "out of memory";
+        case FC_ERR_BUDGET: return "over the device-memory budget";
+        case FC_ERR_DEVICE: return "CUDA error";
+        case FC_ERR_ITER_LIMIT: return "device loop or wait bound reached";
+        case FC_ERR_INVALID: return "invalid argument";
+        case FC_ERR_TOO_LARGE: return "graph exceeds the 32-bit index limits";
+        case FC_ERR_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+int fc_abi_version(void) { return FC_ABI_VERSION; }
+
+fc_status fc_graph_load_dir(const char* dir, int order, int write_vtx_map, fc_graph** out) {
+    if (!dir || !out) return FC_ERR_INVALID;
+    fc_graph* g = new_graph();
+    if (!g) return FC_ERR_OOM;
+    std::string d(dir);
+    if (!d.empty() && d.back() != '/') d.push_back('/');
+    fc_status s = load_dir(d, order, write_vtx_map != 0, g);
+    if (s != FC_OK) {
+        delete g;
+        return s;
+    }
+    *out = g;
+    return FC_OK;
+}
+
+fc_status fc_graph_from_pairs(uint32_t n_layers, const uint64_t* m, const uint32_t* pairs,
+                              fc_graph** out) {
+    if (!out || (n_layers && !m)) return FC_ERR_INVALID;
+    uint64_t total = 0;
+    for (uint32_t l = 0; l < n_layers; l++) total += m[l];
+    if (total && !pairs) return FC_ERR_INVALID;
+    fc_graph* g = new_graph();
+    if (!g) return FC_ERR_OOM;
+    fc_status s = build_from_pairs(n_layers, m, pairs, g);
+    if (s != FC_OK) {
+        delete g;
+        return s;
+    }
+    *out = g;
+    return FC_OK;
+}
+
+fc_status fc_graph_from_adjbuf(uint32_t n, uint32_t n_layers, const uint32_t* const* bufs,
+                               const uint64_t* m, fc_graph** out) {
+    if (!out || (n_layers && (!bufs || !m))) return FC_ERR_INVALID;
+    fc_graph* g = new_graph();
+    if (!g) return FC_ERR_OOM;
+    fc_status s = build_from_adjbuf(n, n_layers, bufs, m, g);
+    if (s != FC_OK) {
+        delete g;
+        return s;
+    }
+    *out = g;
+    return FC_OK;
+}
+
+void fc_graph_free(fc_graph* g) {
+    if (!g) return;
+    release_device(g);
+    delete g;
+}
+
+uint32_t fc_graph_n(const fc_graph* g) { return g ? g->n : 0; }
+uint32_t fc_graph_layers(const fc_graph* g) { return g ? g->L : 0; }
+uint64_t fc_graph_layer_m(const fc_graph* g, uint32_t l) {
+    return (g && l < g->L) ? g->layer_m(l) : 0;
+}
+
+fc_status fc_graph_id2vtx(const fc_graph* g, uint64_t* out) {
+    if (!g || (!out && g->n)) return FC_ERR_INVALID;
+    if (g->n) memcpy(out, g->id2vtx.data(), (size_t)g->n * 8);
+    return FC_OK;
+}
+
+fc_status fc_graph_order(const fc_graph* g, uint32_t* out) {
+    if (!g || (!out && g->L)) return FC_ERR_INVALID;
+    if (g->L) memcpy(out, g->order.data(), (size_t)g->L * 4);
+    return FC_OK;
+}
+
+fc_status fc_graph_csr(const fc_graph* g, uint64_t* off, uint32_t* adj) {
+    if (!g) return FC_ERR_INVALID;
+    uint64_t no = (uint64_t)g->L * (g->n + 1);
+    if (off && no) memcpy(off, g->off.p, no * 8);
+    uint64_t na = g->total_entries();
+    if (adj && na) memcpy(adj, g->adj.p, na * 4);
+    return FC_OK;
+}
+
+fc_status fc_graph_upload(fc_graph* g, void* stream) {
+    if (!g) return FC_ERR_INVALID;
+    return upload(g, (cudaStream_t)stream);
+}
+
+fc_status fc_graph_release_device(fc_graph* g) {
+    if (!g) return FC_ERR_INVALID;
+    release_device(g);
+    return FC_OK;
+}
+
+fc_status fc_graph_reset_results(fc_graph* g) {
+    if (!g) return FC_ERR_INVALID;
+    if (g->dev) {
+        g->dev->table_valid = false;
+        invalidate_densest(g->dev);
+    }
+    return FC_OK;
+}
+
+uint64_t fc_graph_device_bytes(const fc_graph* g) { return g ? device_bytes(g) : 0; }
+
+fc_status fc_coreindex(fc_graph* g, uint32_t* out, int out_on_device, void* stream) {
+    if (!g) return FC_ERR_INVALID;
+    return coreindex(g, out, out_on_device != 0, (cudaStream_t)stream);
+}
+
+fc_status fc_densest(fc_graph* g, const double* betas, uint32_t n_betas, fc_densest_result* res,
+                     void* stream) {
+    if (!g || (n_betas && (!betas || !res))) return FC_ERR_INVALID;
+    if (!g->n || !g->L) {
+        for (uint32_t b = 0; b < n_betas; b++) {
+            memset(&res[b], 0, sizeof(res[b]));
+            res[b].beta = betas[b];
+        }
+        return cuda_available() ? FC_OK : FC_ERR_NO_DEVICE;
+    }
+    return densest(g, betas, n_betas, res, (cudaStream_t)stream);
+}
+
+fc_status fc_densest_members(fc_graph* g, const fc_densest_result* res, uint32_t* nodes,
+                             uint32_t* layers, void* stream) {
+    if (!g || !res) return FC_ERR_INVALID;
+    return densest_members(g, res, nodes, layers, (cudaStream_t)stream);
+}
+
+fc_status fc_cells(fc_graph* g, double beta, fc_cell* cells_out, uint32_t cap, uint32_t* count,
+                   void* stream) {
+    if (!g) return FC_ERR_INVALID;
+    if (!g->n || !g->L) {
+        if (count) *count = 0;
+        return cuda_available() ? FC_OK : FC_ERR_NO_DEVICE;
+    }
+    return cells(g, beta, cells_out, cap, count, (cudaStream_t)stream);
+}
+
+fc_status fc_graph_stats(const fc_graph* g, fc_stats* out) {
+    if (!g || !out) return FC_ERR_INVALID;
+    *out = g->dev ? g->dev->stats : fc_stats{};
+    return FC_OK;
+}
+
+uint64_t fc_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+
+fc_status fc_batch_run(fc_graph* const* graphs, uint32_t count, double beta,
+                       uint32_t* const* tables, fc_densest_result* res,
+                       const fc_batch_options* opt, void* stream) {
+    if (count && !graphs) return FC_ERR_INVALID;
+    return batch_run(graphs, count, beta, tables, res, opt, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,534 @@
+// Densest-subgraph search over every non-empty fcgrid cell, from the core
+// table, in one pass over the edges per group of lambda columns.
+//
+// A directed entry (v -> u, layer l) lies inside C_{k,lambda} iff
+// min(core_lambda(v), core_lambda(u)) >= k.  So one histogram per lambda,
+//     H[lambda][l][key] = #{entries (v,u,l) : min(core_lambda(v), core_lambda(u)) = key},
+// gives by suffix sums over key every cell's
+//     e2_l(k,lambda) = sum over v in C_{k,lambda} of deg_C(v,l)
+// -- the `num_edge` the reference accumulates per cell (Core/FCPathLevelLeft.cpp:
+// 60-64) -- and the node histogram gives |C_{k,lambda}|.  Each cell is then
+// scored with the reference's expression (:66-90):
+//     degree_l = (float)e2_l * 1.0f / 2;  sorted descending;
+//     d_l = degree_(l) * 1.0f / |C| * 1.0 * pow(l, beta)   (FP64)
+// keeping the best l (ties to the larger l), and the cells are folded in the
+// reference's tree preorder (lambda-major, k ascending) with its float running
+// maximum (Core/FCTree.cpp:69-82, main.cpp:406).  pow(l, beta) comes from the
+// host's libm, as in the reference; every other step is IEEE FP32/FP64
+// arithmetic in the same order, so densities are bit-identical.
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <vector>
+
+#include "device.h"
+
+namespace fc {
+
+struct DensState {
+    uint32_t L = 0;
+    std::vector<uint32_t> kmax;        // per lambda (index lambda-1)
+    std::vector<uint64_t> hbase;       // per lambda: offset of H[lambda] (L*(kmax+1) words)
+    std::vector<uint64_t> nbase;       // per lambda: offset of the node histogram
+    std::vector<uint64_t> cbase;       // per lambda: first cell index
+    uint64_t hwords = 0, nwords = 0, ncells = 0;
+    uint32_t* H = nullptr;             // hwords: edge histogram -> suffix sums e2
+    uint32_t* N = nullptr;             // nwords: node histogram -> suffix sums |C|
+    uint32_t* coreT = nullptr;         // n*L node-major copy of the table
+    uint64_t* d_hbase = nullptr;       // device copies of the bases (L each)
+    uint64_t* d_nbase = nullptr;
+    uint32_t* d_kmax = nullptr;
+    fc_cell* cells = nullptr;          // ncells
+    double* powl = nullptr;            // L
+    fc_densest_result* d_res = nullptr;
+    bool hist_valid = false;
+};
+
+void free_densest_state(DeviceGraph* d) {
+    DensState* s = (DensState*)d->dens;
+    if (!s) return;
+    cudaFree(s->H);
+    cudaFree(s->N);
+    cudaFree(s->coreT);
+    cudaFree(s->d_hbase);
+    cudaFree(s->d_nbase);
+    cudaFree(s->d_kmax);
+    cudaFree(s->cells);
+    cudaFree(s->powl);
+    cudaFree(s->d_res);
+    delete s;
+    d->dens = nullptr;
+}
+
+// ---- kernels -------------------------------------------------------------
+
+__global__ void k_colmax(const uint32_t* __restrict__ table, uint32_t n, uint32_t L,
+                         uint32_t* __restrict__ kmax) {
+    // grid.y = lambda
+    const uint32_t lam = blockIdx.y;
+    const uint32_t* col = table + (uint64_t)lam * n;
+    uint32_t m = 0;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        m = max(m, col[v]);
+    m = __reduce_max_sync(0xffffffffu, m);
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(kmax + lam, m);
+}
+
+__global__ void k_transpose(const uint32_t* __restrict__ table, uint32_t n, uint32_t L,
+                            uint32_t* __restrict__ coreT) {
+    // 32x32 tiles through shared memory
+    __shared__ uint32_t tile[32][33];
+    const uint32_t v0 = blockIdx.x * 32, l0 = blockIdx.y * 32;
+    for (uint32_t r = threadIdx.y; r < 32; r += blockDim.y) {
+        uint32_t l = l0 + r, v = v0 + threadIdx.x;
+        if (l < L && v < n) tile[r][threadIdx.x] = table[(uint64_t)l * n + v];
+    }
+    __syncthreads();
+    for (uint32_t r = threadIdx.y; r < 32; r += blockDim.y) {
+        uint32_t v = v0 + r, l = l0 + threadIdx.x;
+        if (l < L && v < n) coreT[(uint64_t)v * L + l] = tile[threadIdx.x][r];
+    }
+}
+
+__global__ void k_node_hist(const uint32_t* __restrict__ table, uint32_t n,
+                            const uint64_t* __restrict__ nbase, const uint32_t* __restrict__ kmax,
+                            uint32_t* __restrict__ N) {
+    extern __shared__ uint32_t sh[];
+    const uint32_t lam = blockIdx.y;
+    const uint32_t bins = kmax[lam] + 1;
+    const bool use_sh = bins <= 12288;
+    if (use_sh)
+        for (uint32_t i = threadIdx.x; i < bins; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const uint32_t* col = table + (uint64_t)lam * n;
+    uint32_t* out = N + nbase[lam];
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        uint32_t c = col[v];
+        if (use_sh) atomicAdd(sh + c, 1u);
+        else atomicAdd(out + c, 1u);
+    }
+    __syncthreads();
+    if (use_sh)
+        for (uint32_t i = threadIdx.x; i < bins; i += blockDim.x)
+            if (sh[i]) atomicAdd(out + i, sh[i]);
+}
+
+// Edge histogram for lambda columns [lam0, lam0 + nl).  Each warp takes a
+// contiguous slice of the entry array; lanes stride through it and track the
+// source node by advancing along node_ptr.  Bins live in shared memory when
+// they fit (`sh_ok`), else in global memory.
+__global__ void k_edge_hist(const uint32_t* __restrict__ node_ptr, const uint32_t* __restrict__ adj,
+                            uint32_t n, uint32_t L, uint64_t entries, FastDiv divL,
+                            const uint32_t* __restrict__ coreT, uint32_t lam0, uint32_t nl,
+                            const uint64_t* __restrict__ hbase, const uint32_t* __restrict__ kmax,
+                            uint32_t* __restrict__ H, uint32_t sh_words, int sh_ok) {
+    extern __shared__ uint32_t sh[];
+    __shared__ uint32_t soff[64];  // per column in the group: offset into sh
+    if (threadIdx.x == 0) {
+        uint32_t o = 0;
+        for (uint32_t i = 0; i < nl; i++) {
+            soff[i] = o;
+            o += L * (kmax[lam0 + i] + 1);
+        }
+    }
+    if (sh_ok)
+        for (uint32_t i = threadIdx.x; i < sh_words; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t per = (entries + nwarps - 1) / nwarps;
+    const uint64_t e0 = gw * per, e1 = min(entries, e0 + per);
+    if (e0 < e1) {
+        // source node of this lane's first entry: last v with node_ptr[v] <= e
+        uint64_t e = e0 + lane;
+        uint32_t lo = 0, hi = n;  // node_ptr[lo] <= e < node_ptr[hi]
+        if (e < e1) {
+            while (hi - lo > 1) {
+                uint32_t mid = (lo + hi) >> 1;
+                if (node_ptr[mid] <= e) lo = mid;
+                else hi = mid;
+            }
+        }
+        uint32_t v = lo;
+        for (; e < e1; e += 32) {
+            while (node_ptr[v + 1] <= e) v++;
+            const uint32_t slot = adj[e];
+            const uint32_t u = divL.div(slot);
+            const uint32_t l = slot - u * L;
+            for (uint32_t i = 0; i < nl; i++) {
+                const uint32_t a = coreT[(uint64_t)v * L + lam0 + i];
+                if (!a) continue;
+                const uint32_t b = coreT[(uint64_t)u * L + lam0 + i];
+                const uint32_t key = min(a, b);
+                if (!key) continue;
+                const uint32_t km1 = kmax[lam0 + i] + 1;
+                if (sh_ok) atomicAdd(sh + soff[i] + l * km1 + key, 1u);
+                else atomicAdd(H + hbase[lam0 + i] + (uint64_t)l * km1 + key, 1u);
+            }
+        }
+    }
+    __syncthreads();
+    if (sh_ok) {
+        for (uint32_t i = 0; i < nl; i++) {
+            const uint32_t words = L * (kmax[lam0 + i] + 1);
+            uint32_t* g = H + hbase[lam0 + i];
+            for (uint32_t w = threadIdx.x; w < words; w += blockDim.x)
+                if (sh[soff[i] + w]) atomicAdd(g + w, sh[soff[i] + w]);
+        }
+    }
+}
+
+// Suffix sums over key, per (lambda, layer) row of H and per lambda of N.
+// uint32 arithmetic wraps exactly as the reference's `uint num_edge`.
+__global__ void k_suffix(uint32_t L, const uint64_t* __restrict__ hbase,
+                         const uint64_t* __restrict__ nbase, const uint32_t* __restrict__ kmax,
+                         uint32_t* __restrict__ H, uint32_t* __restrict__ N) {
+    const uint32_t lam = blockIdx.x;
+    const uint32_t km1 = kmax[lam] + 1;
+    for (uint32_t l = threadIdx.x; l <= L; l += blockDim.x) {
+        uint32_t* row = l < L ? H + hbase[lam] + (uint64_t)l * km1 : N + nbase[lam];
+        uint32_t acc = 0;
+        for (int64_t k = (int64_t)km1 - 1; k >= 0; k--) {
+            acc += row[k];
+            row[k] = acc;
+        }
+    }
+}
+
+// One block per cell (lambda, k), k >= 1: sort the cell's L layer counts
+// descending (bitonic sort in shared memory), evaluate every l, keep the best.
+__global__ void k_cells(uint32_t L, uint32_t P /* pow2 >= L */, const uint64_t* __restrict__ hbase,
+                        const uint64_t* __restrict__ nbase, const uint32_t* __restrict__ kmax,
+                        const uint32_t* __restrict__ H, const uint32_t* __restrict__ N,
+                        const double* __restrict__ powl, const uint32_t* __restrict__ cell_lam,
+                        const uint32_t* __restrict__ cell_k, fc_cell* __restrict__ cells) {
+    extern __shared__ uint32_t sv[];  // P values
+    __shared__ double bestd[32];
+    __shared__ uint32_t bestl[32];
+    const uint32_t ci = blockIdx.x;
+    const uint32_t lam = cell_lam[ci], k = cell_k[ci];
+    const uint32_t km1 = kmax[lam] + 1;
+    const uint32_t len = N[nbase[lam] + k];
+    for (uint32_t i = threadIdx.x; i < P; i += blockDim.x)
+        sv[i] = i < L ? H[hbase[lam] + (uint64_t)i * km1 + k] : 0u;
+    __syncthreads();
+    // bitonic sort, descending
+    for (uint32_t size = 2; size <= P; size <<= 1) {
+        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+            for (uint32_t i = threadIdx.x; i < P; i += blockDim.x) {
+                uint32_t p = i ^ stride;
+                if (p > i) {
+                    bool desc = (i & size) == 0;
+                    uint32_t a = sv[i], b = sv[p];
+                    if (desc ? (a < b) : (a > b)) {
+                        sv[i] = b;
+                        sv[p] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    double my_d = -1.0;
+    uint32_t my_l = 0;
+    for (uint32_t i = threadIdx.x; i < L; i += blockDim.x) {
+        float f = __uint2float_rn(sv[i]) * 1.0f / 2;
+        double degree = (double)f;
+        double mad = (degree * 1.0f) / (double)len * 1.0;
+        double d = mad * powl[i];
+        if (d >= my_d) {  // later i in this thread's sequence wins ties
+            my_d = d;
+            my_l = i + 1;
+        }
+    }
+    // block argmax, ties to the larger l
+    for (int o = 16; o >= 1; o >>= 1) {
+        double od = __shfl_down_sync(0xffffffffu, my_d, o);
+        uint32_t ol = __shfl_down_sync(0xffffffffu, my_l, o);
+        if (od > my_d || (od == my_d && ol > my_l)) {
+            my_d = od;
+            my_l = ol;
+        }
+    }
+    const uint32_t w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        bestd[w] = my_d;
+        bestl[w] = my_l;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double bd = -1.0;
+        uint32_t bl = 0;
+        for (uint32_t i = 0; i < (blockDim.x + 31) / 32; i++)
+            if (bestd[i] > bd || (bestd[i] == bd && bestl[i] > bl)) {
+                bd = bestd[i];
+                bl = bestl[i];
+            }
+        // the reference starts from 0.0 and keeps l on `d >= best`
+        fc_cell c;
+        c.k = k;
+        c.lmd = lam + 1;
+        c.length = len;
+        c.lstar = bl;
+        c.density = bd < 0.0 ? 0.0 : bd;
+        cells[ci] = c;
+    }
+}
+
+// The reference's preorder fold with a float running maximum.
+__global__ void k_fold(const fc_cell* __restrict__ cells, uint64_t ncells, double beta,
+                       fc_densest_result* out) {
+    if (threadIdx.x || blockIdx.x) return;
+    float maxd = 0.0f;
+    fc_densest_result r;
+    r.beta = beta;
+    r.density = 0.0;
+    r.k = r.lmd = r.length = r.lstar = 0;
+    for (uint64_t i = 0; i < ncells; i++) {
+        const fc_cell c = cells[i];
+        if (c.density >= (double)maxd) {
+            maxd = (float)c.density;
+            r.density = c.density;
+            r.k = c.k;
+            r.lmd = c.lmd;
+            r.length = c.length;
+            r.lstar = c.lstar;
+        }
+    }
+    r.max_density_f = maxd;
+    r.n_cells = (uint32_t)ncells;
+    *out = r;
+}
+
+// ---- host --------------------------------------------------------------------
+
+static int sm_count() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
+// Histograms for the resident table (beta-independent).
+static fc_status build_hist(DeviceGraph* d, cudaStream_t st) {
+    DensState* s = (DensState*)d->dens;
+    if (s && s->hist_valid) return FC_OK;
+    if (!s) {
+        s = new DensState();
+        d->dens = s;
+    }
+    const uint32_t n = d->n, L = d->L;
+    s->L = L;
+    // per-lambda maxima
+    if (!s->d_kmax) FC_CUDA_TRY(cudaMalloc(&s->d_kmax, (L + 1) * 4));
+    FC_CUDA_TRY(cudaMemsetAsync(s->d_kmax, 0, (L + 1) * 4, st));
+    dim3 g((n + 255) / 256 < 64 ? (n + 255) / 256 : 64, L);
+    if (g.x == 0) g.x = 1;
+    k_colmax<<<g, 256, 0, st>>>(d->table, n, L, s->d_kmax);
+    count_launch();
+    FC_CUDA_TRY(cudaGetLastError());
+    s->kmax.assign(L, 0);
+    FC_CUDA_TRY(cudaMemcpyAsync(s->kmax.data(), s->d_kmax, L * 4, cudaMemcpyDeviceToHost, st));
+    FC_CUDA_TRY(cudaStreamSynchronize(st));
+    d->kmax = s->kmax;
+    s->hbase.assign(L, 0);
+    s->nbase.assign(L, 0);
+    s->cbase.assign(L, 0);
+    uint64_t hw = 0, nw = 0, nc = 0;
+    for (uint32_t l = 0; l < L; l++) {
+        s->hbase[l] = hw;
+        s->nbase[l] = nw;
+        s->cbase[l] = nc;
+        hw += (uint64_t)L * (s->kmax[l] + 1);
+        nw += s->kmax[l] + 1;
+        nc += s->kmax[l];
+    }
+    // (re)allocate
+    cudaFree(s->H);
+    cudaFree(s->N);
+    cudaFree(s->cells);
+    cudaFree(s->d_hbase);
+    cudaFree(s->d_nbase);
+    s->H = s->N = nullptr;
+    s->cells = nullptr;
+    s->d_hbase = s->d_nbase = nullptr;
+    s->hwords = hw;
+    s->nwords = nw;
+    s->ncells = nc;
+    FC_CUDA_TRY(cudaMalloc(&s->H, hw * 4 + 4));
+    FC_CUDA_TRY(cudaMalloc(&s->N, nw * 4 + 4));
+    FC_CUDA_TRY(cudaMalloc(&s->cells, (nc + 1) * sizeof(fc_cell)));
+    FC_CUDA_TRY(cudaMalloc(&s->d_hbase, L * 8 + 8));
+    FC_CUDA_TRY(cudaMalloc(&s->d_nbase, L * 8 + 8));
+    if (!s->coreT) FC_CUDA_TRY(cudaMalloc(&s->coreT, (uint64_t)n * L * 4 + 4));
+    FC_CUDA_TRY(cudaMemcpyAsync(s->d_hbase, s->hbase.data(), L * 8, cudaMemcpyHostToDevice, st));
+    FC_CUDA_TRY(cudaMemcpyAsync(s->d_nbase, s->nbase.data(), L * 8, cudaMemcpyHostToDevice, st));
+    FC_CUDA_TRY(cudaMemsetAsync(s->H, 0, hw * 4 + 4, st));
+    FC_CUDA_TRY(cudaMemsetAsync(s->N, 0, nw * 4 + 4, st));
+    if (n && L) {
+        dim3 tg((n + 31) / 32, (L + 31) / 32);
+        k_transpose<<<tg, dim3(32, 8), 0, st>>>(d->table, n, L, s->coreT);
+        FC_CUDA_TRY(cudaGetLastError());
+        dim3 ng((n + 255) / 256 < 32 ? (n + 255) / 256 : 32, L);
+        k_node_hist<<<ng, 256, 12288 * 4, st>>>(d->table, n, s->d_nbase, s->d_kmax, s->N);
+        count_launch(2);
+        FC_CUDA_TRY(cudaGetLastError());
+        // lambda groups whose bins fit the shared-memory budget
+        const uint32_t SH_WORDS = 48 * 1024;  // 192 KB
+        static bool attr_set = false;
+        if (!attr_set) {
+            FC_CUDA_TRY(cudaFuncSetAttribute(k_edge_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             SH_WORDS * 4));
+            attr_set = true;
+        }
+        FastDiv divL;
+        divL.init(L);
+        const int blocks = sm_count();
+        uint32_t lam = 0;
+        while (lam < L) {
+            uint32_t words = 0, nl = 0;
+            while (lam + nl < L && nl < 64) {
+                uint32_t w = L * (s->kmax[lam + nl] + 1);
+                if (nl > 0 && words + w > SH_WORDS) break;
+                words += w;
+                nl++;
+            }
+            int sh_ok = words <= SH_WORDS;
+            size_t shb = sh_ok ? (size_t)words * 4 : 0;
+            if (d->entries) {
+                k_edge_hist<<<blocks, 1024, shb, st>>>(d->node_ptr, d->adj, n, L, d->entries, divL,
+                                                      s->coreT, lam, nl, s->d_hbase, s->d_kmax,
+                                                      s->H, words, sh_ok);
+                count_launch();
+            }
+            FC_CUDA_TRY(cudaGetLastError());
+            lam += nl;
+        }
+        k_suffix<<<L, 128, 0, st>>>(L, s->d_hbase, s->d_nbase, s->d_kmax, s->H, s->N);
+        count_launch();
+        FC_CUDA_TRY(cudaGetLastError());
+    }
+    s->hist_valid = true;
+    return FC_OK;
+}
+
+static fc_status score_cells(DeviceGraph* d, double beta, cudaStream_t st) {
+    DensState* s = (DensState*)d->dens;
+    const uint32_t L = d->L;
+    if (!s->powl) FC_CUDA_TRY(cudaMalloc(&s->powl, L * 8 + 8));
+    std::vector<double> pw(L);
+    for (uint32_t l = 0; l < L; l++) pw[l] = pow((double)(l + 1), beta);  // pow((l+1), beta)
+    FC_CUDA_TRY(cudaMemcpyAsync(s->powl, pw.data(), L * 8, cudaMemcpyHostToDevice, st));
+    if (!s->ncells) return FC_OK;
+    std::vector<uint32_t> cl(s->ncells), ck(s->ncells);
+    uint64_t i = 0;
+    for (uint32_t l = 0; l < L; l++)
+        for (uint32_t k = 1; k <= s->kmax[l]; k++, i++) {
+            cl[i] = l;
+            ck[i] = k;
+        }
+    uint32_t* dcl = nullptr;
+    FC_CUDA_TRY(cudaMallocAsync(&dcl, s->ncells * 8, st));
+    FC_CUDA_TRY(cudaMemcpyAsync(dcl, cl.data(), s->ncells * 4, cudaMemcpyHostToDevice, st));
+    FC_CUDA_TRY(cudaMemcpyAsync(dcl + s->ncells, ck.data(), s->ncells * 4, cudaMemcpyHostToDevice, st));
+    uint32_t P = 1;
+    while (P < L) P <<= 1;
+    uint32_t threads = P < 32 ? 32 : (P > 1024 ? 1024 : P);
+    size_t shb = (size_t)P * 4;
+    if (shb > 48 * 1024) FC_CUDA_TRY(cudaFuncSetAttribute(k_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shb));
+    k_cells<<<(uint32_t)s->ncells, threads, shb, st>>>(L, P, s->d_hbase, s->d_nbase, s->d_kmax, s->H,
+                                                      s->N, s->powl, dcl, dcl + s->ncells, s->cells);
+    count_launch();
+    FC_CUDA_TRY(cudaGetLastError());
+    FC_CUDA_TRY(cudaFreeAsync(dcl, st));
+    return FC_OK;
+}
+
+fc_status densest(fc_graph* g, const double* betas, uint32_t nb, fc_densest_result* res,
+                  cudaStream_t st) {
+    FC_TRY(coreindex(g, nullptr, false, st));
+    DeviceGraph* d = g->dev;
+    cudaEvent_t e0, e1;
+    FC_CUDA_TRY(cudaEventCreate(&e0));
+    FC_CUDA_TRY(cudaEventCreate(&e1));
+    FC_CUDA_TRY(cudaEventRecord(e0, st));
+    FC_TRY(build_hist(d, st));
+    DensState* s = (DensState*)d->dens;
+    if (!s->d_res) FC_CUDA_TRY(cudaMalloc(&s->d_res, sizeof(fc_densest_result)));
+    for (uint32_t b = 0; b < nb; b++) {
+        FC_TRY(score_cells(d, betas[b], st));
+        k_fold<<<1, 32, 0, st>>>(s->cells, s->ncells, betas[b], s->d_res);
+        count_launch();
+        FC_CUDA_TRY(cudaGetLastError());
+        FC_CUDA_TRY(cudaMemcpyAsync(res + b, s->d_res, sizeof(fc_densest_result),
+                                    cudaMemcpyDeviceToHost, st));
+    }
+    FC_CUDA_TRY(cudaEventRecord(e1, st));
+    FC_CUDA_TRY(cudaStreamSynchronize(st));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    d->stats.densest_ms = ms;
+    return FC_OK;
+}
+
+fc_status cells(fc_graph* g, double beta, fc_cell* out, uint32_t cap, uint32_t* count,
+                cudaStream_t st) {
+    FC_TRY(coreindex(g, nullptr, false, st));
+    DeviceGraph* d = g->dev;
+    FC_TRY(build_hist(d, st));
+    DensState* s = (DensState*)d->dens;
+    FC_TRY(score_cells(d, beta, st));
+    uint64_t nc = s->ncells;
+    if (count) *count = (uint32_t)nc;
+    uint64_t w = nc < cap ? nc : cap;
+    if (w && out) FC_CUDA_TRY(cudaMemcpyAsync(out, s->cells, w * sizeof(fc_cell), cudaMemcpyDeviceToHost, st));
+    FC_CUDA_TRY(cudaStreamSynchronize(st));
+    return FC_OK;
+}
+
+fc_status densest_members(fc_graph* g, const fc_densest_result* r, uint32_t* nodes,
+                          uint32_t* layers, cudaStream_t st) {
+    if (!r || r->k == 0) return FC_OK;
+    FC_TRY(coreindex(g, nullptr, false, st));
+    DeviceGraph* d = g->dev;
+    FC_TRY(build_hist(d, st));
+    DensState* s = (DensState*)d->dens;
+    const uint32_t n = d->n, L = d->L, lam = r->lmd - 1;
+    if (r->lmd < 1 || r->lmd > L || r->k > s->kmax[lam]) return FC_ERR_INVALID;
+    if (nodes) {
+        std::vector<uint32_t> col(n);
+        FC_CUDA_TRY(cudaMemcpyAsync(col.data(), d->table + (uint64_t)lam * n, (uint64_t)n * 4,
+                                    cudaMemcpyDeviceToHost, st));
+        FC_CUDA_TRY(cudaStreamSynchronize(st));
+        uint32_t j = 0;
+        for (uint32_t v = 0; v < n; v++)
+            if (col[v] >= r->k) nodes[j++] = v;
+    }
+    if (layers) {
+        // the cell's layer counts; the first lstar of the descending order
+        // (ties by layer index) -- for beta >= 0 lstar never splits a tie
+        const uint32_t km1 = s->kmax[lam] + 1;
+        std::vector<uint32_t> e(L);
+        for (uint32_t l = 0; l < L; l++)
+            FC_CUDA_TRY(cudaMemcpyAsync(&e[l], s->H + s->hbase[lam] + (uint64_t)l * km1 + r->k, 4,
+                                        cudaMemcpyDeviceToHost, st));
+        FC_CUDA_TRY(cudaStreamSynchronize(st));
+        std::vector<uint32_t> idx(L);
+        for (uint32_t l = 0; l < L; l++) idx[l] = l;
+        std::stable_sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return e[a] > e[b]; });
+        std::vector<uint32_t> pick(idx.begin(), idx.begin() + r->lstar);
+        std::sort(pick.begin(), pick.end());
+        for (uint32_t i = 0; i < r->lstar; i++) layers[i] = pick[i];
+    }
+    return FC_OK;
+}
+
+void invalidate_densest(DeviceGraph* d) {
+    DensState* s = (DensState*)d->dens;
+    if (s) s->hist_valid = false;
+}
+
+}  // namespace fc

@@ -1,0 +1,90 @@
+// Device-side layout shared by the kernels.
+//
+// A graph on the device is node-major:
+//   node_ptr[v] .. node_ptr[v+1]   all of v's adjacency, layer 0 first
+//   adj[e] = u * L + l              a "slot": neighbour u in layer l; it is
+//                                   also the index of deg[u][l] in an n*L
+//                                   degree table, so one 4-byte load per edge
+//                                   names both the neighbour and the counter
+//                                   to decrement
+//   deg0[v * L + l] = |N_l(v)|      the full per-layer degrees
+// Core tables are lambda-major: table[(lambda-1) * n + v].
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "fc_internal.h"
+
+namespace fc {
+
+// Division by a run-time constant d >= 1 for 32-bit x by multiply and shifts
+// (Granlund & Montgomery, "Division by invariant integers using
+// multiplication", 1994, round-up variant):
+//   l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1,
+//   q = (t + ((x - t) >> min(l,1))) >> max(l-1,0), t = umulhi(m, x).
+struct FastDiv {
+    uint32_t d, m, s1, s2;
+    void init(uint32_t dd) {
+        d = dd;
+        uint32_t l = 0;
+        while ((1ull << l) < dd) l++;
+        m = (uint32_t)((((1ull << 32) * ((1ull << l) - dd)) / dd) + 1);
+        s1 = l < 1 ? l : 1;
+        s2 = l > 1 ? l - 1 : 0;
+    }
+    __host__ __device__ __forceinline__ uint32_t div(uint32_t x) const {
+#ifdef __CUDA_ARCH__
+        uint32_t t = __umulhi(x, m);
+#else
+        uint32_t t = (uint32_t)(((uint64_t)x * m) >> 32);
+#endif
+        return (t + ((x - t) >> s1)) >> s2;
+    }
+};
+
+struct DeviceGraph {
+    int device = -1;
+    uint32_t n = 0, L = 0;
+    uint64_t entries = 0;      // directed adjacency entries over all layers
+    uint32_t max_deg = 0;      // largest single-layer degree
+    uint32_t max_row = 0;      // largest node adjacency over all layers
+    uint32_t* node_ptr = nullptr;  // n + 1
+    uint32_t* adj = nullptr;       // entries (slots)
+    uint32_t* deg0 = nullptr;      // n * L
+    // resident results
+    uint32_t* table = nullptr;     // L * n, lambda-major
+    bool table_valid = false;
+    std::vector<uint32_t> kmax;    // per lambda, max core (host copy)
+    // densest state for the resident table (histograms, cell records)
+    void* dens = nullptr;
+    // reusable scratch
+    void* ws = nullptr;
+    size_t ws_bytes = 0;
+    uint64_t bytes = 0;            // CSR + table
+    fc_stats stats{};              // diagnostics of the last computations
+};
+
+// kernels launched by this library (fc_launch_count)
+void count_launch(uint32_t k = 1);
+
+// scratch owned by a DeviceGraph, grown on demand
+fc_status ensure_ws(DeviceGraph* d, size_t bytes);
+void free_densest_state(DeviceGraph* d);
+void invalidate_densest(DeviceGraph* d);
+
+// peel.cu
+struct PeelStats {
+    uint32_t levels = 0, subrounds = 0, err = 0;
+    double ms = 0;  // CUDA-event time of the launch
+};
+fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream_t s,
+                       PeelStats* st);
+uint32_t peel_columns_per_group(const DeviceGraph* d);
+
+// last CUDA error text, for diagnostics
+const char* last_cuda_error();
+
+}  // namespace fc

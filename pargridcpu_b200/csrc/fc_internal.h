@@ -1,0 +1,102 @@
+// Internal declarations of libfirmcore: host graph, device layout, kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "firmcore.h"
+
+namespace fc {
+
+// ---------------------------------------------------------------------------
+// Host graph (the reference's MultilayerGraph after LoadFromFile/SetGraphOrder)
+//
+// Layers are stored in logical order (layer i = the reference's GetGraph(i) =
+// graph_layers[order[i]]), each as a CSR over internal ids with ascending,
+// de-duplicated neighbour rows -- the content of Graph::adj_lst_buf without the
+// inline degree word.
+// ---------------------------------------------------------------------------
+
+// Page-locked when a CUDA device is present (so uploads run at full copy
+// bandwidth), ordinary heap memory otherwise.
+template <class T>
+struct HostBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    bool pinned = false;
+    HostBuf() = default;
+    HostBuf(const HostBuf&) = delete;
+    HostBuf& operator=(const HostBuf&) = delete;
+    ~HostBuf() { reset(); }
+    bool alloc(size_t count);
+    void reset();
+    T& operator[](size_t i) { return p[i]; }
+    const T& operator[](size_t i) const { return p[i]; }
+};
+
+struct DeviceGraph;  // device-resident CSR and results (graph.cu)
+
+}  // namespace fc
+
+struct fc_graph {
+    uint32_t n = 0, L = 0;
+    std::vector<uint32_t> order;   // -o permutation (file layer index of logical layer i)
+    std::vector<uint64_t> id2vtx;  // internal id -> raw id
+    fc::HostBuf<uint64_t> off;     // L*(n+1), absolute indices into adj
+    fc::HostBuf<uint32_t> adj;     // all layers' rows, layer after layer
+    uint64_t total_entries() const { return L ? off[(uint64_t)L * (n + 1) - 1] : 0; }
+    uint64_t layer_m(uint32_t l) const {
+        const uint64_t* o = off.p + (uint64_t)l * (n + 1);
+        return o[n] - o[0];
+    }
+    fc::DeviceGraph* dev = nullptr;
+};
+
+namespace fc {
+
+// ---- loader (loader.cpp) ----------------------------------------------------
+fc_status load_dir(const std::string& dir, int order, bool write_vtx_map, fc_graph* g);
+fc_status build_from_pairs(uint32_t L, const uint64_t* m, const uint32_t* pairs, fc_graph* g);
+fc_status build_from_adjbuf(uint32_t n, uint32_t L, const uint32_t* const* bufs, const uint64_t* m,
+                            fc_graph* g);
+void apply_order(int order, fc_graph* g);
+
+// ---- device (graph.cu / peel.cu / densest.cu) --------------------------------
+bool cuda_available();
+fc_status upload(fc_graph* g, cudaStream_t s);
+void release_device(fc_graph* g);
+uint64_t device_bytes(const fc_graph* g);
+fc_status coreindex(fc_graph* g, uint32_t* out, bool out_on_device, cudaStream_t s);
+fc_status densest(fc_graph* g, const double* betas, uint32_t nb, fc_densest_result* res,
+                  cudaStream_t s);
+fc_status densest_members(fc_graph* g, const fc_densest_result* r, uint32_t* nodes,
+                          uint32_t* layers, cudaStream_t s);
+fc_status cells(fc_graph* g, double beta, fc_cell* out, uint32_t cap, uint32_t* count,
+                cudaStream_t s);
+fc_status batch_run(fc_graph* const* gs, uint32_t count, double beta, uint32_t* const* tables,
+                    fc_densest_result* res, const fc_batch_options* opt, cudaStream_t s);
+
+}  // namespace fc
+
+#define FC_CUDA_TRY(expr)                                                   \
+    do {                                                                    \
+        cudaError_t e_ = (expr);                                            \
+        if (e_ != cudaSuccess) {                                            \
+            fc::set_last_cuda_error(e_, #expr, __FILE__, __LINE__);         \
+            return e_ == cudaErrorMemoryAllocation ? FC_ERR_OOM : FC_ERR_DEVICE; \
+        }                                                                   \
+    } while (0)
+
+#define FC_TRY(expr)                      \
+    do {                                  \
+        fc_status s_ = (expr);            \
+        if (s_ != FC_OK) return s_;       \
+    } while (0)
+
+namespace fc {
+void set_last_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+}

@@ -1,0 +1,179 @@
+// Device residency: copies a host graph to the device and builds the
+// node-major, slot-encoded CSR the kernels read (layout in device.h).
+#include <cub/cub.cuh>
+
+#include <cstdio>
+#include <mutex>
+#include <string>
+
+#include "device.h"
+
+namespace fc {
+
+static thread_local std::string g_last_err;
+
+void set_last_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
+    char b[512];
+    snprintf(b, sizeof(b), "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+    g_last_err = b;
+}
+const char* last_cuda_error() { return g_last_err.c_str(); }
+
+bool cuda_available() {
+    static int have = -1;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lk(mu);
+    if (have < 0) {
+        int n = 0;
+        have = (cudaGetDeviceCount(&n) == cudaSuccess && n > 0) ? 1 : 0;
+        cudaGetLastError();
+    }
+    return have == 1;
+}
+
+// deg0[v*L + l] and the row length of every node, from per-layer offsets.
+__global__ void k_degrees(const uint64_t* __restrict__ off, uint32_t n, uint32_t L,
+                          uint32_t* __restrict__ deg0, uint32_t* __restrict__ rowlen) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        uint32_t sum = 0;
+        for (uint32_t l = 0; l < L; l++) {
+            const uint64_t* o = off + (uint64_t)l * (n + 1);
+            uint32_t d = (uint32_t)(o[v + 1] - o[v]);
+            deg0[(uint64_t)v * L + l] = d;
+            sum += d;
+        }
+        rowlen[v] = sum;
+    }
+}
+
+// One warp per node: copy its L layer rows into its node-major range as slots.
+__global__ void k_scatter(const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj_in,
+                          const uint32_t* __restrict__ node_ptr, uint32_t n, uint32_t L,
+                          uint32_t* __restrict__ adj_out) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
+        uint32_t dst = node_ptr[v];
+        for (uint32_t l = 0; l < L; l++) {
+            const uint64_t* o = off + (uint64_t)l * (n + 1);
+            uint64_t b = o[v], e = o[v + 1];
+            for (uint64_t j = b + lane; j < e; j += 32) adj_out[dst + (j - b)] = adj_in[j] * L + l;
+            dst += (uint32_t)(e - b);
+        }
+    }
+}
+
+__global__ void k_max(const uint32_t* __restrict__ a, uint64_t len, uint32_t* out) {
+    uint32_t m = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < len;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        m = max(m, a[i]);
+    m = __reduce_max_sync(0xffffffffu, m);
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+fc_status ensure_ws(DeviceGraph* d, size_t bytes) {
+    if (d->ws_bytes >= bytes) return FC_OK;
+    if (d->ws) cudaFree(d->ws);
+    d->ws = nullptr;
+    d->ws_bytes = 0;
+    size_t b = bytes + bytes / 8;
+    FC_CUDA_TRY(cudaMalloc(&d->ws, b));
+    d->ws_bytes = b;
+    return FC_OK;
+}
+
+static int num_sms() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
+fc_status upload(fc_graph* g, cudaStream_t s) {
+    if (!cuda_available()) return FC_ERR_NO_DEVICE;
+    if (g->dev) return FC_OK;
+    uint32_t n = g->n, L = g->L;
+    uint64_t entries = g->total_entries();
+    if ((uint64_t)n * L >= (1ull << 32) || entries >= (1ull << 32)) return FC_ERR_TOO_LARGE;
+    DeviceGraph* d = new DeviceGraph();
+    FC_CUDA_TRY(cudaGetDevice(&d->device));
+    d->n = n;
+    d->L = L;
+    d->entries = entries;
+    g->dev = d;
+    uint64_t noff = (uint64_t)L * (n + 1);
+    uint64_t* d_off = nullptr;
+    uint32_t* d_in = nullptr;
+    uint32_t* rowlen = nullptr;
+    uint32_t* d_max = nullptr;
+    void* tmp = nullptr;
+    size_t tmp_bytes = 0;
+    FC_CUDA_TRY(cudaMallocAsync(&d_off, noff * 8 + 8, s));
+    FC_CUDA_TRY(cudaMallocAsync(&d_in, entries * 4 + 4, s));
+    FC_CUDA_TRY(cudaMallocAsync(&rowlen, (uint64_t)n * 4 + 4, s));
+    FC_CUDA_TRY(cudaMallocAsync(&d_max, 8, s));
+    FC_CUDA_TRY(cudaMalloc(&d->node_ptr, ((uint64_t)n + 1) * 4));
+    FC_CUDA_TRY(cudaMalloc(&d->adj, entries * 4 + 4));
+    FC_CUDA_TRY(cudaMalloc(&d->deg0, (uint64_t)n * L * 4 + 4));
+    FC_CUDA_TRY(cudaMalloc(&d->table, (uint64_t)n * L * 4 + 4));
+    d->bytes = ((uint64_t)n + 1) * 4 + entries * 4 + 2ull * n * L * 4;
+    if (noff) FC_CUDA_TRY(cudaMemcpyAsync(d_off, g->off.p, noff * 8, cudaMemcpyHostToDevice, s));
+    if (entries) FC_CUDA_TRY(cudaMemcpyAsync(d_in, g->adj.p, entries * 4, cudaMemcpyHostToDevice, s));
+    FC_CUDA_TRY(cudaMemsetAsync(d_max, 0, 8, s));
+    int blocks = num_sms() * 8;
+    if (n) {
+        k_degrees<<<blocks, 256, 0, s>>>(d_off, n, L, d->deg0, rowlen);
+        FC_CUDA_TRY(cudaGetLastError());
+        FC_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, rowlen, d->node_ptr, n + 1, s));
+        FC_CUDA_TRY(cudaMallocAsync(&tmp, tmp_bytes + 16, s));
+        // rowlen has n entries; entry n of the scan input must be 0
+        FC_CUDA_TRY(cudaMemsetAsync(rowlen + n, 0, 4, s));
+        FC_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, rowlen, d->node_ptr, n + 1, s));
+        k_scatter<<<blocks, 256, 0, s>>>(d_off, d_in, d->node_ptr, n, L, d->adj);
+        FC_CUDA_TRY(cudaGetLastError());
+        k_max<<<blocks, 256, 0, s>>>(d->deg0, (uint64_t)n * L, d_max);
+        k_max<<<blocks, 256, 0, s>>>(rowlen, n, d_max + 1);
+        count_launch(4);
+        FC_CUDA_TRY(cudaGetLastError());
+    }
+    uint32_t mx[2] = {0, 0};
+    FC_CUDA_TRY(cudaMemcpyAsync(mx, d_max, 8, cudaMemcpyDeviceToHost, s));
+    if (tmp) FC_CUDA_TRY(cudaFreeAsync(tmp, s));
+    FC_CUDA_TRY(cudaFreeAsync(d_off, s));
+    FC_CUDA_TRY(cudaFreeAsync(d_in, s));
+    FC_CUDA_TRY(cudaFreeAsync(rowlen, s));
+    FC_CUDA_TRY(cudaFreeAsync(d_max, s));
+    FC_CUDA_TRY(cudaStreamSynchronize(s));
+    d->max_deg = mx[0];
+    d->max_row = mx[1];
+    return FC_OK;
+}
+
+void release_device(fc_graph* g) {
+    DeviceGraph* d = g->dev;
+    if (!d) return;
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (d->device >= 0 && d->device != cur) cudaSetDevice(d->device);
+    free_densest_state(d);
+    cudaFree(d->node_ptr);
+    cudaFree(d->adj);
+    cudaFree(d->deg0);
+    cudaFree(d->table);
+    if (d->ws) cudaFree(d->ws);
+    if (cur >= 0 && d->device != cur) cudaSetDevice(cur);
+    delete d;
+    g->dev = nullptr;
+}
+
+uint64_t device_bytes(const fc_graph* g) {
+    if (!g->dev) return 0;
+    return g->dev->bytes + g->dev->ws_bytes;
+}
+
+}  // namespace fc

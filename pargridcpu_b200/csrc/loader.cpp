@@ -1,0 +1,379 @@
+// Host loader: the reference's MultilayerGraph::LoadFromFile semantics
+// (Graph/MultilayerGraph.cpp:47-166) and Graph::BuildFromEdgeLst's CSR
+// (Graph/Graph.cpp:17-50), producing fc_graph's host CSR.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fc_internal.h"
+
+namespace fc {
+
+template <class T>
+bool HostBuf<T>::alloc(size_t count) {
+    reset();
+    size_t bytes = (count ? count : 1) * sizeof(T);
+    if (cuda_available() && cudaMallocHost((void**)&p, bytes) == cudaSuccess) {
+        pinned = true;
+    } else {
+        cudaGetLastError();
+        p = (T*)malloc(bytes);
+        pinned = false;
+    }
+    n = count;
+    return p != nullptr;
+}
+
+template <class T>
+void HostBuf<T>::reset() {
+    if (p) {
+        if (pinned) cudaFreeHost(p);
+        else free(p);
+    }
+    p = nullptr;
+    n = 0;
+    pinned = false;
+}
+
+template struct HostBuf<uint64_t>;
+template struct HostBuf<uint32_t>;
+
+namespace {
+
+// Open-addressing map raw id -> internal id; ids are handed out in order of
+// first sight (MultilayerGraph.cpp:127-143: u is looked up before v).
+struct IdMap {
+    std::vector<uint32_t> key, val;
+    std::vector<uint8_t> used;
+    uint64_t mask = 0, size = 0;
+    std::vector<uint64_t>* id2vtx;
+    explicit IdMap(std::vector<uint64_t>* out) : id2vtx(out) { rehash(1 << 16); }
+    static uint64_t h(uint32_t x) {
+        uint64_t z = (uint64_t)x * 0x9E3779B97F4A7C15ull;
+        return z ^ (z >> 29);
+    }
+    void rehash(uint64_t cap) {
+        std::vector<uint32_t> k2(cap), v2(cap);
+        std::vector<uint8_t> u2(cap, 0);
+        uint64_t m2 = cap - 1;
+        for (uint64_t i = 0; i < used.size(); i++) {
+            if (!used[i]) continue;
+            uint64_t j = h(key[i]) & m2;
+            while (u2[j]) j = (j + 1) & m2;
+            u2[j] = 1;
+            k2[j] = key[i];
+            v2[j] = val[i];
+        }
+        key.swap(k2);
+        val.swap(v2);
+        used.swap(u2);
+        mask = m2;
+    }
+    uint32_t get(uint32_t x) {
+        uint64_t j = h(x) & mask;
+        while (used[j]) {
+            if (key[j] == x) return val[j];
+            j = (j + 1) & mask;
+        }
+        uint32_t id = (uint32_t)size++;
+        used[j] = 1;
+        key[j] = x;
+        val[j] = id;
+        id2vtx->push_back(x);
+        if (size * 2 > mask) rehash((mask + 1) * 2);
+        return id;
+    }
+};
+
+bool read_file(const std::string& path, std::vector<char>& buf) {
+    FILE* f = fopen(path.c_str(), "rb");
+    if (!f) return false;
+    fseek(f, 0, SEEK_END);
+    long sz = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    buf.resize(sz > 0 ? (size_t)sz : 0);
+    size_t got = sz > 0 ? fread(buf.data(), 1, (size_t)sz, f) : 0;
+    fclose(f);
+    return got == buf.size();
+}
+
+// The layer-file loop of MultilayerGraph::LoadLayer (:122-156):
+//     while (in.peek() != EOF) { in >> u >> v; if (u != v) keep(u, v); }
+// with `uint u, v` and C++11 stream rules: an extraction that finds only
+// whitespace before the end leaves its variable unchanged and fails the
+// stream; one that finds no digit stores 0 and fails; an out-of-range value
+// stores UINT_MAX and fails; a leading '-' negates modulo 2^32; reading the
+// last digit sets end-of-file.  Once failed or at end, peek() is EOF.  A pair
+// read before either variable was ever assigned is undefined in the
+// reference and is dropped here.
+struct PairParser {
+    const char* p;
+    const char* e;
+    bool fail = false, eof = false;
+    static bool ws(char c) {
+        return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r';
+    }
+    // returns true when val was assigned
+    bool extract(uint32_t& val) {
+        if (fail || eof) {
+            fail = true;
+            return false;
+        }
+        while (p < e && ws(*p)) p++;
+        if (p >= e) {
+            eof = fail = true;
+            return false;
+        }
+        bool neg = false;
+        if (*p == '+' || *p == '-') {
+            neg = *p == '-';
+            p++;
+        }
+        const char* s = p;
+        uint64_t mag = 0;
+        bool over = false;
+        while (p < e && *p >= '0' && *p <= '9') {
+            if (!over) {
+                mag = mag * 10 + (uint64_t)(*p - '0');
+                if (mag > 0xFFFFFFFFull) over = true;
+            }
+            p++;
+        }
+        if (p >= e) eof = true;
+        if (p == s) {
+            fail = true;
+            val = 0;
+            return true;
+        }
+        if (over) {
+            fail = true;
+            val = 0xFFFFFFFFu;
+            return true;
+        }
+        val = neg ? (uint32_t)(0u - (uint32_t)mag) : (uint32_t)mag;
+        return true;
+    }
+};
+
+void parse_pairs(const std::vector<char>& text, std::vector<uint32_t>& out) {
+    PairParser ps{text.data(), text.data() + text.size()};
+    uint32_t u = 0, v = 0;
+    bool have_u = false, have_v = false;
+    out.clear();
+    out.reserve(text.size() / 6);
+    while (!(ps.fail || ps.eof || ps.p >= ps.e)) {
+        if (ps.extract(u)) have_u = true;
+        if (ps.extract(v)) have_v = true;
+        if (have_u && have_v && u != v) {
+            out.push_back(u);
+            out.push_back(v);
+        }
+    }
+}
+
+// Per-layer CSR from remapped directed pairs: rows ascending, duplicates
+// dropped (Graph.cpp:27-47).  Counting sort by source, then each row sorted.
+void build_layer(uint32_t n, const std::vector<uint32_t>& dir_pairs, std::vector<uint64_t>& off,
+                 std::vector<uint32_t>& adj) {
+    uint64_t m = dir_pairs.size() / 2;
+    std::vector<uint64_t> cnt((size_t)n + 1, 0);
+    for (uint64_t i = 0; i < m; i++) cnt[dir_pairs[2 * i] + 1]++;
+    for (uint32_t v = 0; v < n; v++) cnt[v + 1] += cnt[v];
+    std::vector<uint32_t> tgt(m);
+    std::vector<uint64_t> pos(cnt.begin(), cnt.end() - 1);
+    for (uint64_t i = 0; i < m; i++) tgt[pos[dir_pairs[2 * i]]++] = dir_pairs[2 * i + 1];
+    off.assign((size_t)n + 1, 0);
+    adj.clear();
+    adj.reserve(m);
+    for (uint32_t v = 0; v < n; v++) {
+        off[v] = adj.size();
+        uint32_t* b = tgt.data() + cnt[v];
+        uint32_t* e = tgt.data() + cnt[v + 1];
+        std::sort(b, e);
+        for (uint32_t* q = b; q < e; q++)
+            if (q == b || *q != q[-1]) adj.push_back(*q);
+    }
+    off[n] = adj.size();
+}
+
+fc_status finish(uint32_t n, uint32_t L, std::vector<std::vector<uint32_t>>& dir_pairs, fc_graph* g) {
+    g->n = n;
+    g->L = L;
+    g->order.resize(L);
+    for (uint32_t i = 0; i < L; i++) g->order[i] = i;
+    std::vector<std::vector<uint64_t>> offs(L);
+    std::vector<std::vector<uint32_t>> adjs(L);
+    uint64_t total = 0;
+    for (uint32_t l = 0; l < L; l++) {
+        build_layer(n, dir_pairs[l], offs[l], adjs[l]);
+        std::vector<uint32_t>().swap(dir_pairs[l]);
+        total += adjs[l].size();
+    }
+    if (!g->off.alloc((uint64_t)L * (n + 1)) || !g->adj.alloc(total)) return FC_ERR_OOM;
+    uint64_t base = 0;
+    for (uint32_t l = 0; l < L; l++) {
+        uint64_t* o = g->off.p + (uint64_t)l * (n + 1);
+        for (uint32_t v = 0; v <= n; v++) o[v] = base + offs[l][v];
+        if (!adjs[l].empty()) memcpy(g->adj.p + base, adjs[l].data(), adjs[l].size() * 4);
+        base += adjs[l].size();
+    }
+    return FC_OK;
+}
+
+}  // namespace
+
+fc_status build_from_pairs(uint32_t L, const uint64_t* m, const uint32_t* pairs, fc_graph* g) {
+    IdMap map(&g->id2vtx);
+    std::vector<std::vector<uint32_t>> dir(L);
+    const uint32_t* p = pairs;
+    for (uint32_t l = 0; l < L; l++) {
+        dir[l].reserve(2 * m[l] * 2);
+        for (uint64_t i = 0; i < m[l]; i++, p += 2) {
+            uint32_t u = p[0], v = p[1];
+            if (u == v) continue;  // MultilayerGraph.cpp:126
+            uint32_t a = map.get(u), b = map.get(v);
+            dir[l].push_back(a);
+            dir[l].push_back(b);
+            dir[l].push_back(b);
+            dir[l].push_back(a);
+        }
+    }
+    return finish((uint32_t)map.size, L, dir, g);
+}
+
+fc_status load_dir(const std::string& dir, int order, bool write_vtx_map, fc_graph* g) {
+    // mlg.conf: one layer file name per non-empty line (GetGraphFile, :47-63);
+    // lines are split on '\n' only, as std::getline does.
+    std::vector<char> conf;
+    if (!read_file(dir + "mlg.conf", conf)) return FC_ERR_IO;
+    std::vector<std::string> files;
+    std::string line;
+    for (size_t i = 0; i <= conf.size(); i++) {
+        if (i == conf.size() || conf[i] == '\n') {
+            if (!line.empty()) files.push_back(line);
+            line.clear();
+        } else {
+            line.push_back(conf[i]);
+        }
+    }
+    uint32_t L = (uint32_t)files.size();
+    IdMap map(&g->id2vtx);
+    std::vector<std::vector<uint32_t>> dir_pairs(L);
+    std::vector<char> text;
+    std::vector<uint32_t> raw;
+    for (uint32_t l = 0; l < L; l++) {
+        if (!read_file(dir + files[l], text)) return FC_ERR_IO;
+        parse_pairs(text, raw);
+        auto& d = dir_pairs[l];
+        d.reserve(raw.size() * 2);
+        for (size_t i = 0; i < raw.size(); i += 2) {
+            uint32_t a = map.get(raw[i]), b = map.get(raw[i + 1]);
+            d.push_back(a);
+            d.push_back(b);
+            d.push_back(b);
+            d.push_back(a);
+        }
+    }
+    if (write_vtx_map) {
+        // `u uid` per new id, in assignment order (MultilayerGraph.cpp:131,139)
+        FILE* f = fopen((dir + "__vtx_map.txt").c_str(), "wb");
+        if (!f) return FC_ERR_IO;
+        std::string out;
+        out.reserve(g->id2vtx.size() * 16);
+        char b[48];
+        for (size_t i = 0; i < g->id2vtx.size(); i++) {
+            int k = snprintf(b, sizeof(b), "%u %zu\n", (unsigned)g->id2vtx[i], i);
+            out.append(b, (size_t)k);
+        }
+        bool ok = fwrite(out.data(), 1, out.size(), f) == out.size();
+        ok = (fclose(f) == 0) && ok;
+        if (!ok) return FC_ERR_IO;
+    }
+    FC_TRY(finish((uint32_t)map.size, L, dir_pairs, g));
+    apply_order(order, g);
+    return FC_OK;
+}
+
+fc_status build_from_adjbuf(uint32_t n, uint32_t L, const uint32_t* const* bufs, const uint64_t* m,
+                            fc_graph* g) {
+    g->n = n;
+    g->L = L;
+    g->order.resize(L);
+    g->id2vtx.resize(n);
+    for (uint32_t v = 0; v < n; v++) g->id2vtx[v] = v;
+    for (uint32_t i = 0; i < L; i++) g->order[i] = i;
+    uint64_t total = 0;
+    for (uint32_t l = 0; l < L; l++) total += m[l];
+    if (!g->off.alloc((uint64_t)L * (n + 1)) || !g->adj.alloc(total)) return FC_ERR_OOM;
+    uint64_t base = 0;
+    for (uint32_t l = 0; l < L; l++) {
+        const uint32_t* b = bufs[l];
+        uint64_t* o = g->off.p + (uint64_t)l * (n + 1);
+        uint64_t r = 0, w = base;
+        for (uint32_t v = 0; v < n; v++) {
+            o[v] = w;
+            uint32_t d = b[r++];
+            if (w + d > base + m[l]) return FC_ERR_PARSE;
+            for (uint32_t j = 0; j < d; j++) {
+                uint32_t u = b[r++];
+                if (u >= n || u == v || (j && u <= g->adj[w - 1])) return FC_ERR_PARSE;
+                g->adj[w++] = u;
+            }
+        }
+        if (w != base + m[l]) return FC_ERR_PARSE;
+        o[n] = w;
+        base = w;
+    }
+    return FC_OK;
+}
+
+// SetGraphOrder (MultilayerGraph.cpp:9-45): 1/2 sort layers by
+// (float)(m>>1)/(float)n ascending/descending, 3/4 by m; the same std::sort
+// calls on the same input give the same permutation.
+void apply_order(int o, fc_graph* g) {
+    uint32_t L = g->L, n = g->n;
+    if (o == 0 || L == 0) return;
+    std::vector<uint32_t> ord(L);
+    for (uint32_t i = 0; i < L; i++) ord[i] = i;
+    std::vector<uint32_t> ms(L);
+    for (uint32_t i = 0; i < L; i++) ms[i] = (uint32_t)g->layer_m(i);
+    if (o == 1 || o == 2) {
+        std::vector<float> density(L);
+        for (uint32_t i = 0; i < L; i++) density[i] = (float)(ms[i] >> 1) / (float)n;
+        if (o == 1)
+            std::sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return density[a] < density[b]; });
+        else
+            std::sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return density[a] > density[b]; });
+    } else if (o == 3 || o == 4) {
+        if (o == 3)
+            std::sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return ms[a] < ms[b]; });
+        else
+            std::sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) { return ms[a] > ms[b]; });
+    } else {
+        return;
+    }
+    HostBuf<uint64_t> off2;
+    HostBuf<uint32_t> adj2;
+    uint64_t total = g->total_entries();
+    if (!off2.alloc((uint64_t)L * (n + 1)) || !adj2.alloc(total)) return;
+    uint64_t base = 0;
+    for (uint32_t i = 0; i < L; i++) {
+        const uint64_t* src = g->off.p + (uint64_t)ord[i] * (n + 1);
+        uint64_t* dst = off2.p + (uint64_t)i * (n + 1);
+        uint64_t len = src[n] - src[0];
+        for (uint32_t v = 0; v <= n; v++) dst[v] = base + (src[v] - src[0]);
+        if (len) memcpy(adj2.p + base, g->adj.p + src[0], len * 4);
+        base += len;
+    }
+    std::swap(g->off.p, off2.p);
+    std::swap(g->off.pinned, off2.pinned);
+    std::swap(g->adj.p, adj2.p);
+    std::swap(g->adj.pinned, adj2.pinned);
+    std::vector<uint32_t> composed(L);
+    for (uint32_t i = 0; i < L; i++) composed[i] = g->order[ord[i]];
+    g->order = composed;
+}
+
+}  // namespace fc

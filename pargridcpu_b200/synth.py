@@ -72,17 +72,28 @@ def _cl_sampler(rng, n, gamma):
     return draw
 
 
+def _unique(x):
+    """Sorted distinct values (same output as np.unique, sort-based)."""
+    x = np.sort(x)
+    if len(x) < 2:
+        return x
+    keep = np.empty(len(x), bool)
+    keep[0] = True
+    np.not_equal(x[1:], x[:-1], out=keep[1:])
+    return x[keep]
+
+
 def _fill(draw, base, target):
-    s = np.unique(base)
+    ub = _unique(base)
+    s = ub
     while len(s) < target:
         need = target - len(s)
-        s = np.unique(np.concatenate([s, draw(int(need * 1.3) + 64)]))
+        s = _unique(np.concatenate([s, draw(int(need * 1.3) + 64)]))
     if len(s) > target:
         # keep all of base, trim the fresh draws at random
-        extra = np.setdiff1d(s, base, assume_unique=True)
-        keep = np.random.default_rng(len(s)).choice(len(extra), target - len(np.unique(base)),
-                                                    replace=False)
-        s = np.sort(np.concatenate([np.unique(base), extra[keep]]))
+        extra = s[~np.isin(s, ub, assume_unique=True)]
+        keep = np.random.default_rng(len(s)).choice(len(extra), target - len(ub), replace=False)
+        s = np.sort(np.concatenate([ub, extra[keep]]))
     return s
 
 
