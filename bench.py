@@ -325,6 +325,8 @@ def run_ours(args, world, rank, local):
             "detail": {"peel_ms_per_step": statistics.mean(peel_ms),
                        "densest_ms_per_step": statistics.mean(dens_ms),
                        "levels": stats["levels"], "subrounds": stats["subrounds"],
+                       "peel_phase_ms": dict(zip(("scan", "expand", "recompute"),
+                                                 stats["phase_ms"])),
                        "densest": {k: res[k] for k in ("k", "lmd", "length", "lstar", "density",
                                                        "max_density_f")}}}
     if world == 1 and not args.no_cpu_baseline:

@@ -206,6 +206,7 @@ typedef struct fc_stats {
     uint32_t levels;         /* peel levels, summed over column groups */
     uint32_t subrounds;      /* peel sub-rounds, summed over column groups */
     uint32_t columns_per_launch;
+    double phase_ms[3];      /* peel time in level scans, expansions, recomputes */
 } fc_stats;
 
 fc_status fc_graph_stats(const fc_graph* g, fc_stats* out);

@@ -19,6 +19,7 @@ fc_status coreindex(fc_graph* g, uint32_t* out, bool out_on_device, cudaStream_t
         invalidate_densest(d);
         d->stats.peel_ms = 0;
         d->stats.peel_launches = d->stats.levels = d->stats.subrounds = 0;
+        for (int i = 0; i < 3; i++) d->stats.phase_ms[i] = 0;
         if (d->n && d->L) {
             const uint32_t per = peel_columns_per_group(d);
             d->stats.columns_per_launch = per;
@@ -30,6 +31,7 @@ fc_status coreindex(fc_graph* g, uint32_t* out, bool out_on_device, cudaStream_t
                 d->stats.peel_launches++;
                 d->stats.levels += st.levels;
                 d->stats.subrounds += st.subrounds;
+                for (int i = 0; i < 3; i++) d->stats.phase_ms[i] += st.phase_ms[i];
             }
         }
         d->table_valid = true;

@@ -79,6 +79,7 @@ void invalidate_densest(DeviceGraph* d);
 struct PeelStats {
     uint32_t levels = 0, subrounds = 0, err = 0;
     double ms = 0;  // CUDA-event time of the launch
+    double phase_ms[3] = {0, 0, 0};  // scan, expand, recompute (device timer)
 };
 fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream_t s,
                        PeelStats* st);

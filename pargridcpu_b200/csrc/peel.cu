@@ -23,6 +23,7 @@
 // error and the kernel winds down; level and sub-round counts are bounded by
 // n*columns and the largest degree.
 #include <cooperative_groups.h>
+#include <cooperative_groups/scan.h>
 
 #include <cstdio>
 #include <cstdlib>
@@ -39,9 +40,15 @@ enum : uint32_t { ERR_NONE = 0, ERR_BARRIER = 1, ERR_LIMIT = 2 };
 struct PeelCtl {
     uint32_t bar_count, bar_gen, err, phase;
     uint32_t level, front_cur, alive_cur, dirty_cnt;
-    uint32_t front_cnt[2], hub_cnt[2], alive_cnt[2];
+    uint32_t front_cnt[2], chunk_cnt[2], alive_cnt[2];
     uint32_t next_min, levels, subrounds, pad;
+    uint64_t t_last;      // globaltimer at the last barrier
+    uint64_t ph_ns[4];    // time spent per phase kind (scan/init, expand, recompute)
 };
+
+// rows longer than SMALL_ROW entries are expanded as CHUNK-entry work items
+constexpr uint32_t SMALL_ROW = 32;
+constexpr uint32_t CHUNK = 128;
 
 struct PeelJob {
     uint32_t n, L, col0, ncols;
@@ -53,12 +60,11 @@ struct PeelJob {
     uint32_t* deg;       // ncols * n * L
     uint32_t* t;         // table + col0 * n: ncols * n
     uint32_t* alive[2];  // each ncols * n
-    uint32_t* front[2];
-    uint32_t* hubs[2];
+    uint32_t* front[2];  // rows of at most SMALL_ROW entries
+    uint64_t* chunks[2]; // (x | chunk << 32) items of longer rows
     uint32_t* dirty;
     uint32_t* dflag;     // ncols * n
     PeelCtl* ctl;
-    uint32_t hub_threshold;
     uint32_t max_level;
     uint32_t max_subrounds;
     uint32_t upper_bits;  // bits of the largest layer degree
@@ -106,10 +112,16 @@ __device__ void leader_step(volatile PeelCtl* c, const PeelJob& j) {
             c->phase = PH_DONE;
         }
     };
+    {
+        uint64_t now = global_ns();
+        uint32_t kind = c->phase == PH_EXPAND ? 1 : (c->phase == PH_RECOMPUTE ? 2 : 0);
+        if (c->t_last) c->ph_ns[kind] += now - c->t_last;
+        c->t_last = now;
+    }
     switch (c->phase) {
         case PH_SCAN:  // also the state after INIT
             c->alive_cur ^= 1;
-            if (c->front_cnt[c->front_cur] + c->hub_cnt[c->front_cur] > 0) {
+            if (c->front_cnt[c->front_cur] + c->chunk_cnt[c->front_cur] > 0) {
                 c->phase = PH_EXPAND;
                 c->dirty_cnt = 0;
             } else {
@@ -119,7 +131,7 @@ __device__ void leader_step(volatile PeelCtl* c, const PeelJob& j) {
         case PH_EXPAND:
             c->phase = PH_RECOMPUTE;
             c->front_cnt[c->front_cur ^ 1] = 0;
-            c->hub_cnt[c->front_cur ^ 1] = 0;
+            c->chunk_cnt[c->front_cur ^ 1] = 0;
             break;
         case PH_RECOMPUTE:
             c->dirty_cnt = 0;
@@ -128,7 +140,7 @@ __device__ void leader_step(volatile PeelCtl* c, const PeelJob& j) {
             if (c->subrounds > j.max_subrounds) {
                 c->err = ERR_LIMIT;
                 c->phase = PH_DONE;
-            } else if (c->front_cnt[c->front_cur] + c->hub_cnt[c->front_cur] > 0) {
+            } else if (c->front_cnt[c->front_cur] + c->chunk_cnt[c->front_cur] > 0) {
                 c->phase = PH_EXPAND;
             } else {
                 end_level();
@@ -226,21 +238,43 @@ __device__ __forceinline__ uint32_t row_len(const PeelJob& j, uint32_t v) {
     return __ldg(j.node_ptr + v + 1) - __ldg(j.node_ptr + v);
 }
 
+// A removed node joins the next expansion: short rows as one item, longer
+// rows as ceil(len / CHUNK) chunk items so that no warp walks a long row alone.
 __device__ __forceinline__ void push_frontier(const PeelJob& j, uint32_t f, uint32_t x) {
     uint32_t v = x - j.divN.div(x) * j.n;
-    if (row_len(j, v) > j.hub_threshold) push(j.hubs[f], &j.ctl->hub_cnt[f], x);
-    else push(j.front[f], &j.ctl->front_cnt[f], x);
+    uint32_t len = row_len(j, v);
+    if (len <= SMALL_ROW) {
+        push(j.front[f], &j.ctl->front_cnt[f], x);
+        return;
+    }
+    uint32_t nch = (len + CHUNK - 1) / CHUNK;
+    cg::coalesced_group g = cg::coalesced_threads();
+    uint32_t incl = cg::inclusive_scan(g, nch);
+    uint32_t base = 0;
+    if (g.thread_rank() == g.size() - 1) base = atomicAdd(&j.ctl->chunk_cnt[f], incl);
+    base = g.shfl(base, g.size() - 1);
+    uint64_t* out = j.chunks[f] + base + (incl - nch);
+    for (uint32_t c = 0; c < nch; c++) out[c] = (uint64_t)x | ((uint64_t)c << 32);
 }
 
-// One removed neighbour slot: decrement and trigger.
-__device__ __forceinline__ void visit(const PeelJob& j, uint32_t c, uint32_t slot, uint32_t k) {
-    uint32_t u = j.divL.div(slot);
-    uint32_t y = c * j.n + u;
-    uint32_t tu = ld_l2(j.t + y);
-    if (tu > k) {
-        uint32_t old = atomicSub(j.deg + (uint64_t)c * j.nL + slot, 1u);
-        if (old == tu) {
-            if (atomicExch(j.dflag + y, 1u) == 0u) push(j.dirty, &j.ctl->dirty_cnt, y);
+// Up to four removed-neighbour slots per lane at once (loads first, then the
+// atomics), so each lane keeps several memory operations in flight: decrement
+// deg[u][l] and mark u dirty when the decrement took it from exactly t[u].
+__device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&col)[4],
+                                       const uint32_t (&slot)[4], const bool (&ok)[4], uint32_t k) {
+    uint32_t y[4], tu[4], old[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        y[i] = col[i] * j.n + j.divL.div(slot[i]);
+        tu[i] = ok[i] ? ld_l2(j.t + y[i]) : 0u;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+        old[i] = (ok[i] && tu[i] > k) ? atomicSub(j.deg + (uint64_t)col[i] * j.nL + slot[i], 1u) : 0u;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        if (ok[i] && tu[i] > k && old[i] == tu[i]) {
+            if (atomicExch(j.dflag + y[i], 1u) == 0u) push(j.dirty, &j.ctl->dirty_cnt, y[i]);
         }
     }
 }
@@ -300,14 +334,36 @@ __device__ void phase_expand(const PeelJob& j) {
     const PeelCtl* c = j.ctl;
     const uint32_t f = ld_l2(&c->front_cur);
     const uint32_t fsize = ld_l2(&c->front_cnt[f]);
-    const uint32_t hsize = ld_l2(&c->hub_cnt[f]);
+    const uint32_t csize = ld_l2(&c->chunk_cnt[f]);
     const uint32_t k = ld_l2(&c->level);
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
     const uint32_t* F = j.front[f];
-    // small rows: 32 frontier nodes per warp, their adjacency flattened over
-    // the lanes (owner found by binary search over the exclusive scan)
+    // long rows: CHUNK-entry items, one per warp, four slots per lane
+    for (uint32_t ci = gw; ci < csize; ci += nw) {
+        const uint64_t it = __ldcg(reinterpret_cast<const unsigned long long*>(j.chunks[f]) + ci);
+        const uint32_t x = (uint32_t)it, ch = (uint32_t)(it >> 32);
+        const uint32_t col = j.divN.div(x);
+        const uint32_t v = x - col * j.n;
+        const uint32_t b = __ldg(j.node_ptr + v) + ch * CHUNK;
+        const uint32_t e = min(__ldg(j.node_ptr + v + 1), b + CHUNK);
+        for (uint32_t q0 = b; q0 < e; q0 += 128) {
+            uint32_t cols[4], slot[4];
+            bool ok[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                uint32_t q = q0 + lane + 32 * i;
+                ok[i] = q < e;
+                slot[i] = ok[i] ? __ldg(j.adj + q) : 0u;
+                cols[i] = col;
+            }
+            visit4(j, cols, slot, ok, k);
+        }
+    }
+    // short rows: 32 frontier nodes per warp, their adjacency (at most 1024
+    // entries) flattened over the lanes; the owner of entry q is found by
+    // binary search over the warp's exclusive scan of row lengths
     for (uint32_t base = gw * 32; base < fsize; base += nw * 32) {
         uint32_t i = base + lane;
         uint32_t x = i < fsize ? ld_l2(F + i) : 0;
@@ -326,33 +382,26 @@ __device__ void phase_expand(const PeelJob& j) {
         }
         uint32_t excl = incl - len;
         uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-        for (uint32_t jb = 0; jb < total; jb += 32) {
-            uint32_t q = jb + lane;
-            uint32_t own = 0;
+        for (uint32_t jb = 0; jb < total; jb += 128) {
+            uint32_t cols[4], slot[4];
+            bool ok[4];
 #pragma unroll
-            for (int step = 16; step >= 1; step >>= 1) {
-                uint32_t cand = own + step;
-                uint32_t ex = __shfl_sync(0xffffffffu, excl, cand & 31);
-                if (cand < 32 && ex <= q) own = cand;
+            for (int i = 0; i < 4; i++) {
+                const uint32_t q = jb + 32 * i + lane;
+                uint32_t own = 0;
+#pragma unroll
+                for (int step = 16; step >= 1; step >>= 1) {
+                    uint32_t cand = own + step;
+                    uint32_t ex = __shfl_sync(0xffffffffu, excl, cand & 31);
+                    if (cand < 32 && ex <= q) own = cand;
+                }
+                const uint32_t ob = __shfl_sync(0xffffffffu, b, own);
+                const uint32_t oe = __shfl_sync(0xffffffffu, excl, own);
+                cols[i] = __shfl_sync(0xffffffffu, col, own);
+                ok[i] = q < total;
+                slot[i] = ok[i] ? __ldg(j.adj + ob + (q - oe)) : 0u;
             }
-            uint32_t ob = __shfl_sync(0xffffffffu, b, own);
-            uint32_t oe = __shfl_sync(0xffffffffu, excl, own);
-            uint32_t oc = __shfl_sync(0xffffffffu, col, own);
-            if (q < total) visit(j, oc, __ldg(j.adj + ob + (q - oe)), k);
-        }
-    }
-    // hub rows: every warp takes its share of each hub's chunks
-    constexpr uint32_t CH = 512;
-    for (uint32_t h = 0; h < hsize; h++) {
-        uint32_t x = ld_l2(j.hubs[f] + h);
-        uint32_t col = j.divN.div(x);
-        uint32_t v = x - col * j.n;
-        uint32_t b = __ldg(j.node_ptr + v);
-        uint32_t e = __ldg(j.node_ptr + v + 1);
-        uint32_t nch = (e - b + CH - 1) / CH;
-        for (uint32_t ch = gw; ch < nch; ch += nw) {
-            uint32_t cb = b + ch * CH, ce = min(e, cb + CH);
-            for (uint32_t q = cb + lane; q < ce; q += 32) visit(j, col, __ldg(j.adj + q), k);
+            visit4(j, cols, slot, ok, k);
         }
     }
 }
@@ -471,11 +520,18 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
     const uint32_t n = d->n, L = d->L;
     const uint64_t nx = (uint64_t)ncols * n;
     const uint64_t nL = (uint64_t)n * L;
-    // workspace: deg | alive0 alive1 front0 front1 hub0 hub1 dirty dflag | ctl
-    size_t words = (size_t)(ncols * nL) + 8 * nx + 256;
+    // workspace: chunk0 chunk1 (uint64) | deg | alive0 alive1 front0 front1
+    // dirty dflag | ctl.  A sub-round's chunk items number at most one per
+    // removed node plus entries / CHUNK per column.
+    const uint64_t nchunk = nx + ((uint64_t)ncols * d->entries + CHUNK - 1) / CHUNK + 1;
+    size_t words = 4 * nchunk + (size_t)(ncols * nL) + 6 * nx + 256;
     FC_TRY(ensure_ws(d, words * 4));
     uint32_t* w = (uint32_t*)d->ws;
     PeelJob j;
+    j.chunks[0] = (uint64_t*)w;
+    w += 2 * nchunk;
+    j.chunks[1] = (uint64_t*)w;
+    w += 2 * nchunk;
     j.n = n;
     j.L = L;
     j.col0 = col0;
@@ -493,12 +549,9 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
     j.alive[1] = w; w += nx;
     j.front[0] = w; w += nx;
     j.front[1] = w; w += nx;
-    j.hubs[0] = w; w += nx;
-    j.hubs[1] = w; w += nx;
     j.dirty = w; w += nx;
     j.dflag = w; w += nx;
     j.ctl = (PeelCtl*)(((uintptr_t)w + 255) & ~(uintptr_t)255);
-    j.hub_threshold = env_u32("FC_HUB_THRESHOLD", 2048);
     j.max_level = d->max_deg + 1;
     j.max_subrounds = (uint32_t)std::min<uint64_t>(0xFFFFFFF0ull, nx + d->max_deg + 16);
     uint32_t bits = 0;
@@ -536,6 +589,7 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
         st->levels = out.levels;
         st->subrounds = out.subrounds;
         st->err = out.err;
+        for (int i = 0; i < 3; i++) st->phase_ms[i] = out.ph_ns[i] * 1e-6;
     }
     if (out.err) return FC_ERR_ITER_LIMIT;
     return FC_OK;

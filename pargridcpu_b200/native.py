@@ -59,10 +59,12 @@ class BatchOptions(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("peel_ms", C.c_double), ("densest_ms", C.c_double),
                 ("peel_launches", C.c_uint32), ("levels", C.c_uint32), ("subrounds", C.c_uint32),
-                ("columns_per_launch", C.c_uint32)]
+                ("columns_per_launch", C.c_uint32), ("phase_ms", C.c_double * 3)]
 
     def as_dict(self):
-        return {f: getattr(self, f) for f, _ in self._fields_}
+        d = {f: getattr(self, f) for f, _ in self._fields_}
+        d["phase_ms"] = list(self.phase_ms)
+        return d
 
 
 class ServerOptions(C.Structure):
