@@ -41,8 +41,23 @@ struct DensState {
     fc_cell* cells = nullptr;          // ncells
     double* powl = nullptr;            // L
     fc_densest_result* d_res = nullptr;
+    uint32_t* cell_lk = nullptr;       // 2 * ncells: lambda index, then k, per cell
+    std::vector<uint32_t> cell_host;
+    uint64_t H_cap = 0, N_cap = 0, cells_cap = 0, cell_lk_cap = 0, hbase_cap = 0, nbase_cap = 0;
     bool hist_valid = false;
 };
+
+template <class T>
+static fc_status grow(T*& p, uint64_t& cap, uint64_t need) {
+    if (p && cap >= need) return FC_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    uint64_t c = need + need / 4 + 16;
+    FC_CUDA_TRY(cudaMalloc(&p, c * sizeof(T)));
+    cap = c;
+    return FC_OK;
+}
 
 void free_densest_state(DeviceGraph* d) {
     DensState* s = (DensState*)d->dens;
@@ -56,6 +71,7 @@ void free_densest_state(DeviceGraph* d) {
     cudaFree(s->cells);
     cudaFree(s->powl);
     cudaFree(s->d_res);
+    cudaFree(s->cell_lk);
     delete s;
     d->dens = nullptr;
 }
@@ -344,26 +360,32 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st) {
         nw += s->kmax[l] + 1;
         nc += s->kmax[l];
     }
-    // (re)allocate
-    cudaFree(s->H);
-    cudaFree(s->N);
-    cudaFree(s->cells);
-    cudaFree(s->d_hbase);
-    cudaFree(s->d_nbase);
-    s->H = s->N = nullptr;
-    s->cells = nullptr;
-    s->d_hbase = s->d_nbase = nullptr;
+    // grow-only buffers: a recomputation of the same graph allocates nothing
     s->hwords = hw;
     s->nwords = nw;
     s->ncells = nc;
-    FC_CUDA_TRY(cudaMalloc(&s->H, hw * 4 + 4));
-    FC_CUDA_TRY(cudaMalloc(&s->N, nw * 4 + 4));
-    FC_CUDA_TRY(cudaMalloc(&s->cells, (nc + 1) * sizeof(fc_cell)));
-    FC_CUDA_TRY(cudaMalloc(&s->d_hbase, L * 8 + 8));
-    FC_CUDA_TRY(cudaMalloc(&s->d_nbase, L * 8 + 8));
+    FC_TRY(grow(s->H, s->H_cap, hw + 1));
+    FC_TRY(grow(s->N, s->N_cap, nw + 1));
+    FC_TRY(grow(s->cells, s->cells_cap, nc + 1));
+    FC_TRY(grow(s->cell_lk, s->cell_lk_cap, 2 * nc + 2));
+    FC_TRY(grow(s->d_hbase, s->hbase_cap, L + 1));
+    FC_TRY(grow(s->d_nbase, s->nbase_cap, L + 1));
     if (!s->coreT) FC_CUDA_TRY(cudaMalloc(&s->coreT, (uint64_t)n * L * 4 + 4));
     FC_CUDA_TRY(cudaMemcpyAsync(s->d_hbase, s->hbase.data(), L * 8, cudaMemcpyHostToDevice, st));
     FC_CUDA_TRY(cudaMemcpyAsync(s->d_nbase, s->nbase.data(), L * 8, cudaMemcpyHostToDevice, st));
+    // cell list (lambda index, k) in the reference's order, for k_cells
+    s->cell_host.resize(2 * nc + 2);
+    {
+        uint64_t i = 0;
+        for (uint32_t l = 0; l < L; l++)
+            for (uint32_t k = 1; k <= s->kmax[l]; k++, i++) {
+                s->cell_host[i] = l;
+                s->cell_host[nc + i] = k;
+            }
+    }
+    if (nc)
+        FC_CUDA_TRY(cudaMemcpyAsync(s->cell_lk, s->cell_host.data(), 2 * nc * 4,
+                                    cudaMemcpyHostToDevice, st));
     FC_CUDA_TRY(cudaMemsetAsync(s->H, 0, hw * 4 + 4, st));
     FC_CUDA_TRY(cudaMemsetAsync(s->N, 0, nw * 4 + 4, st));
     if (n && L) {
@@ -421,27 +443,16 @@ static fc_status score_cells(DeviceGraph* d, double beta, cudaStream_t st) {
     for (uint32_t l = 0; l < L; l++) pw[l] = pow((double)(l + 1), beta);  // pow((l+1), beta)
     FC_CUDA_TRY(cudaMemcpyAsync(s->powl, pw.data(), L * 8, cudaMemcpyHostToDevice, st));
     if (!s->ncells) return FC_OK;
-    std::vector<uint32_t> cl(s->ncells), ck(s->ncells);
-    uint64_t i = 0;
-    for (uint32_t l = 0; l < L; l++)
-        for (uint32_t k = 1; k <= s->kmax[l]; k++, i++) {
-            cl[i] = l;
-            ck[i] = k;
-        }
-    uint32_t* dcl = nullptr;
-    FC_CUDA_TRY(cudaMallocAsync(&dcl, s->ncells * 8, st));
-    FC_CUDA_TRY(cudaMemcpyAsync(dcl, cl.data(), s->ncells * 4, cudaMemcpyHostToDevice, st));
-    FC_CUDA_TRY(cudaMemcpyAsync(dcl + s->ncells, ck.data(), s->ncells * 4, cudaMemcpyHostToDevice, st));
     uint32_t P = 1;
     while (P < L) P <<= 1;
     uint32_t threads = P < 32 ? 32 : (P > 1024 ? 1024 : P);
     size_t shb = (size_t)P * 4;
     if (shb > 48 * 1024) FC_CUDA_TRY(cudaFuncSetAttribute(k_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shb));
     k_cells<<<(uint32_t)s->ncells, threads, shb, st>>>(L, P, s->d_hbase, s->d_nbase, s->d_kmax, s->H,
-                                                      s->N, s->powl, dcl, dcl + s->ncells, s->cells);
+                                                      s->N, s->powl, s->cell_lk,
+                                                      s->cell_lk + s->ncells, s->cells);
     count_launch();
     FC_CUDA_TRY(cudaGetLastError());
-    FC_CUDA_TRY(cudaFreeAsync(dcl, st));
     return FC_OK;
 }
 

@@ -1,27 +1,32 @@
 // The fcgrid peel: core_lambda(v) for a group of lambda columns of one graph,
 // in one persistent cooperative kernel with the level loop inside.
 //
-// Per column lambda (all columns of the group advance together, level by
-// level) the kernel runs the bucket peel of the reference's get_index2
-// (CoreIndexParallel/CoreIndex.cpp:62-109) level-synchronously:
+// x = (column c, node v) ranges over the group's columns, lambda = col0+c+1.
+// All columns advance together, level by level, K = 0, 1, 2, ...:
 //
-//   t[x]    x = (column, node).  While the node is alive, t is its exact
-//           Top-lambda -- the lambda-th largest of its L layer degrees inside
-//           the alive set; once removed, t is its core index.
-//   level k: the frontier is every alive x with t[x] == k.  Removing x
-//           decrements deg[u][l] for each alive neighbour slot (u,l); a
-//           decrement that takes deg from exactly t[u] to t[u]-1 is the only
-//           way Top-lambda can fall (the lazy trigger of CoreIndex.cpp:92), so
-//           u is marked dirty; dirty nodes get Top-lambda recomputed, and
-//           those now <= k join the next frontier of the same level.
-//   The sub-round EXPAND -> RECOMPUTE repeats until the frontier is empty,
-//   then the next level is the smallest t still alive.
+//   SCAN(K)   every alive x counts its layers with degree >= K+1 inside the
+//             alive set, cnt[x].  cnt < lambda means Top-lambda(x) <= K: x is
+//             removed at level K (core = K).  The others keep cnt.
+//   DRAIN(K)  removed nodes are expanded from a device work queue: each
+//             adjacency slot (u,l) of a removed x decrements deg[u][l] of an
+//             alive u; a decrement from exactly K+1 to K lowers cnt[u], and the
+//             decrement that takes cnt[u] from lambda to lambda-1 removes u at
+//             level K too -- ParGrid's own trigger (CoreParallel/
+//             FCSyncLeft.cpp:99-103).  Each of those crossings happens exactly
+//             once, so every node is queued once.  Removals cascade through
+//             the queue without any barrier; the level ends when no queued item
+//             is left unprocessed (a pending-items counter reaches zero).
 //
-// Phases are separated by a grid barrier whose last arriving block runs the
-// small serial "leader" step (counter resets, level changes).  Every barrier
-// wait is bounded: a block that waits longer than the timeout records an
-// error and the kernel winds down; level and sub-round counts are bounded by
-// n*columns and the largest degree.
+// This computes the same table as the reference's get_index2 bucket peel
+// (CoreIndexParallel/CoreIndex.cpp:62-109) and ParGrid's per-cell PeelSync:
+// core_lambda is the unique fixpoint, whatever the removal order.
+//
+// Long rows (more than SMALL_ROW entries) are queued as CHUNK-entry items so
+// that hubs spread over many warps.  SCAN and DRAIN are separated by a grid
+// barrier whose last arriving block runs the serial "leader" step (level
+// change, counter resets).  Every wait -- barrier or queue -- is bounded by a
+// timeout after which the kernel records an error and winds down; the level
+// count is bounded by the largest degree.
 #include <cooperative_groups.h>
 #include <cooperative_groups/scan.h>
 
@@ -34,16 +39,20 @@ namespace cg = cooperative_groups;
 
 namespace fc {
 
-enum : uint32_t { PH_EXPAND = 1, PH_RECOMPUTE = 2, PH_SCAN = 3, PH_DONE = 4 };
-enum : uint32_t { ERR_NONE = 0, ERR_BARRIER = 1, ERR_LIMIT = 2 };
+enum : uint32_t { PH_SCAN = 1, PH_DRAIN = 2, PH_DONE = 3 };
+enum : uint32_t { ERR_NONE = 0, ERR_BARRIER = 1, ERR_LIMIT = 2, ERR_QUEUE = 3 };
+constexpr uint32_t UNSET = 0xFFFFFFFFu;
+constexpr unsigned long long EMPTY = ~0ull;
 
 struct PeelCtl {
     uint32_t bar_count, bar_gen, err, phase;
-    uint32_t level, front_cur, alive_cur, dirty_cnt;
-    uint32_t front_cnt[2], chunk_cnt[2], alive_cnt[2];
-    uint32_t next_min, levels, subrounds, pad;
+    uint32_t level, alive_cur, q_cur, prev_tail;
+    uint32_t alive_cnt[2];
+    uint32_t q_tail[2], q_head[2];
+    uint32_t pending;     // queued items not yet processed (current level)
+    uint32_t levels, items, pad;
     uint64_t t_last;      // globaltimer at the last barrier
-    uint64_t ph_ns[4];    // time spent per phase kind (scan/init, expand, recompute)
+    uint64_t ph_ns[4];    // time per phase kind: scan, drain
 };
 
 // rows longer than SMALL_ROW entries are expanded as CHUNK-entry work items
@@ -57,17 +66,14 @@ struct PeelJob {
     const uint32_t* node_ptr;
     const uint32_t* adj;
     const uint32_t* deg0;
-    uint32_t* deg;       // ncols * n * L
-    uint32_t* t;         // table + col0 * n: ncols * n
-    uint32_t* alive[2];  // each ncols * n
-    uint32_t* front[2];  // rows of at most SMALL_ROW entries
-    uint64_t* chunks[2]; // (x | chunk << 32) items of longer rows
-    uint32_t* dirty;
-    uint32_t* dflag;     // ncols * n
+    uint32_t* deg;                 // ncols * n * L, degrees inside the alive set
+    uint32_t* t;                   // table + col0 * n: UNSET while alive, then the core
+    uint32_t* cnt;                 // ncols * n
+    uint32_t* alive[2];            // each ncols * n
+    unsigned long long* queue[2];  // work items (x | chunk << 32), EMPTY when unwritten
+    uint32_t qcap;
     PeelCtl* ctl;
     uint32_t max_level;
-    uint32_t max_subrounds;
-    uint32_t upper_bits;  // bits of the largest layer degree
     uint64_t timeout_ns;
 };
 
@@ -86,6 +92,11 @@ __device__ __forceinline__ uint32_t atom_add_acq_rel(uint32_t* p, uint32_t v) {
     asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
     return old;
 }
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
 __device__ __forceinline__ uint64_t global_ns() {
     uint64_t t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -97,54 +108,39 @@ __device__ __forceinline__ uint32_t ld_l2(const uint32_t* p) { return __ldcg(p);
 // ---- leader step: phase transitions (one thread, all blocks parked) -------
 
 __device__ void leader_step(volatile PeelCtl* c, const PeelJob& j) {
-    auto end_level = [&]() {
-        if (c->next_min == 0xFFFFFFFFu) {
-            c->phase = PH_DONE;
-            return;
-        }
-        c->level = c->next_min;
-        c->next_min = 0xFFFFFFFFu;
+    {
+        uint64_t now = global_ns();
+        uint32_t kind = c->phase == PH_DRAIN ? 1 : 0;
+        if (c->t_last) c->ph_ns[kind] += now - c->t_last;
+        c->t_last = now;
+    }
+    auto next_level = [&]() {
+        // the queue of this level is done: the other one becomes current
+        c->prev_tail = c->q_tail[c->q_cur];
+        c->q_cur ^= 1;
+        c->q_tail[c->q_cur] = 0;
+        c->q_head[c->q_cur] = 0;
+        c->pending = 0;
+        c->level = c->level + 1;
+        c->levels = c->levels + 1;
         c->alive_cnt[c->alive_cur ^ 1] = 0;
-        c->levels++;
         c->phase = PH_SCAN;
         if (c->level > j.max_level) {
             c->err = ERR_LIMIT;
             c->phase = PH_DONE;
         }
     };
-    {
-        uint64_t now = global_ns();
-        uint32_t kind = c->phase == PH_EXPAND ? 1 : (c->phase == PH_RECOMPUTE ? 2 : 0);
-        if (c->t_last) c->ph_ns[kind] += now - c->t_last;
-        c->t_last = now;
-    }
     switch (c->phase) {
-        case PH_SCAN:  // also the state after INIT
+        case PH_SCAN:  // also the state after INIT + the first scan
             c->alive_cur ^= 1;
-            if (c->front_cnt[c->front_cur] + c->chunk_cnt[c->front_cur] > 0) {
-                c->phase = PH_EXPAND;
-                c->dirty_cnt = 0;
-            } else {
-                end_level();
-            }
+            if (c->q_tail[c->q_cur] > 0) c->phase = PH_DRAIN;
+            else if (c->alive_cnt[c->alive_cur] == 0) c->phase = PH_DONE;
+            else next_level();
             break;
-        case PH_EXPAND:
-            c->phase = PH_RECOMPUTE;
-            c->front_cnt[c->front_cur ^ 1] = 0;
-            c->chunk_cnt[c->front_cur ^ 1] = 0;
-            break;
-        case PH_RECOMPUTE:
-            c->dirty_cnt = 0;
-            c->front_cur ^= 1;
-            c->subrounds++;
-            if (c->subrounds > j.max_subrounds) {
-                c->err = ERR_LIMIT;
-                c->phase = PH_DONE;
-            } else if (c->front_cnt[c->front_cur] + c->chunk_cnt[c->front_cur] > 0) {
-                c->phase = PH_EXPAND;
-            } else {
-                end_level();
-            }
+        case PH_DRAIN:
+            c->items = c->items + c->q_tail[c->q_cur];
+            if (c->alive_cnt[c->alive_cur] == 0) c->phase = PH_DONE;
+            else next_level();
             break;
         default:
             c->phase = PH_DONE;
@@ -172,7 +168,7 @@ __device__ bool grid_barrier(const PeelJob& j) {
             uint32_t ns = 32;
             while (ld_acquire(&c->bar_gen) == gen) {
                 __nanosleep(ns);
-                if (ns < 512) ns <<= 1;
+                if (ns < 256) ns <<= 1;
                 if (global_ns() - t0 > j.timeout_ns) {
                     atomicExch(&c->err, ERR_BARRIER);
                     break;
@@ -196,101 +192,118 @@ __device__ __forceinline__ void push(uint32_t* list, uint32_t* cnt, uint32_t val
     list[base + g.thread_rank()] = val;
 }
 
-// Lambda-th largest of L values v[0..L) by a group of G lanes (G a power of
-// two; all 32 lanes of the warp call this together, each group with its own
-// row and lambda).  Radix select from bit `bits-1` down: the answer is the
-// largest x with #{v >= x} >= lambda.  `bits` must be warp-uniform and cover
-// the answer.  Rows with lmd == 0 are idle lanes (result unused).
-template <int G>
-__device__ __forceinline__ uint32_t group_topl(const uint32_t* row, uint32_t L, uint32_t lmd,
-                                               uint32_t bits, bool live_row, bool l2) {
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t gl = lane & (G - 1);
-    constexpr int MAXV = 16;
-    uint32_t vals[MAXV];
-    const uint32_t nv = (L + G - 1) / G;
-    const bool inreg = nv <= MAXV;
-    if (inreg) {
-#pragma unroll
-        for (int i = 0; i < MAXV; i++) {
-            uint32_t li = gl + (uint32_t)i * G;
-            vals[i] = (live_row && (uint32_t)i < nv && li < L) ? (l2 ? ld_l2(row + li) : row[li]) : 0u;
-        }
-    }
-    uint32_t res = 0;
-    for (int b = (int)bits - 1; b >= 0; b--) {
-        uint32_t cand = res | (1u << b);
-        uint32_t cnt = 0;
-        if (inreg) {
-#pragma unroll
-            for (int i = 0; i < MAXV; i++) cnt += vals[i] >= cand;
-        } else if (live_row) {
-            for (uint32_t li = gl; li < L; li += G) cnt += (l2 ? ld_l2(row + li) : row[li]) >= cand;
-        }
-#pragma unroll
-        for (int off = G / 2; off >= 1; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
-        if (cnt >= lmd) res = cand;
-    }
-    return res;
-}
-
 __device__ __forceinline__ uint32_t row_len(const PeelJob& j, uint32_t v) {
     return __ldg(j.node_ptr + v + 1) - __ldg(j.node_ptr + v);
 }
 
-// A removed node joins the next expansion: short rows as one item, longer
-// rows as ceil(len / CHUNK) chunk items so that no warp walks a long row alone.
-__device__ __forceinline__ void push_frontier(const PeelJob& j, uint32_t f, uint32_t x) {
-    uint32_t v = x - j.divN.div(x) * j.n;
-    uint32_t len = row_len(j, v);
-    if (len <= SMALL_ROW) {
-        push(j.front[f], &j.ctl->front_cnt[f], x);
-        return;
-    }
-    uint32_t nch = (len + CHUNK - 1) / CHUNK;
+// Queue the work items of a removed x (called by the lanes that removed a
+// node, together): one item for a short row, ceil(len / CHUNK) chunk items
+// for a long one.  `pending` is raised before the items become visible, so
+// it cannot reach zero while they wait.
+__device__ __forceinline__ void enqueue(const PeelJob& j, uint32_t q, uint32_t x) {
+    const uint32_t v = x - j.divN.div(x) * j.n;
+    const uint32_t len = row_len(j, v);
+    const uint32_t nit = len <= SMALL_ROW ? 1u : (len + CHUNK - 1) / CHUNK;
     cg::coalesced_group g = cg::coalesced_threads();
-    uint32_t incl = cg::inclusive_scan(g, nch);
+    const uint32_t incl = cg::inclusive_scan(g, nit);
     uint32_t base = 0;
-    if (g.thread_rank() == g.size() - 1) base = atomicAdd(&j.ctl->chunk_cnt[f], incl);
-    base = g.shfl(base, g.size() - 1);
-    uint64_t* out = j.chunks[f] + base + (incl - nch);
-    for (uint32_t c = 0; c < nch; c++) out[c] = (uint64_t)x | ((uint64_t)c << 32);
-}
-
-// Up to four removed-neighbour slots per lane at once (loads first, then the
-// atomics), so each lane keeps several memory operations in flight: decrement
-// deg[u][l] and mark u dirty when the decrement took it from exactly t[u].
-__device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&col)[4],
-                                       const uint32_t (&slot)[4], const bool (&ok)[4], uint32_t k) {
-    uint32_t y[4], tu[4], old[4];
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        y[i] = col[i] * j.n + j.divL.div(slot[i]);
-        tu[i] = ok[i] ? ld_l2(j.t + y[i]) : 0u;
+    if (g.thread_rank() == g.size() - 1) {
+        atomicAdd(&j.ctl->pending, incl);
+        base = atomicAdd(&j.ctl->q_tail[q], incl);
     }
-#pragma unroll
-    for (int i = 0; i < 4; i++)
-        old[i] = (ok[i] && tu[i] > k) ? atomicSub(j.deg + (uint64_t)col[i] * j.nL + slot[i], 1u) : 0u;
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        if (ok[i] && tu[i] > k && old[i] == tu[i]) {
-            if (atomicExch(j.dflag + y[i], 1u) == 0u) push(j.dirty, &j.ctl->dirty_cnt, y[i]);
+    base = g.shfl(base, g.size() - 1);
+    __threadfence();
+    const uint32_t first = base + incl - nit;
+    for (uint32_t c = 0; c < nit; c++) {
+        const uint32_t idx = first + c;
+        if (idx < j.qcap) {
+            const unsigned long long it = (unsigned long long)x | ((unsigned long long)c << 32);
+            asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(j.queue[q] + idx), "l"(it)
+                         : "memory");
+        } else {
+            atomicExch(&j.ctl->err, ERR_QUEUE);
         }
     }
 }
 
-// Block-wide minimum into *dst (one atomic per block).
-__device__ __forceinline__ void block_min_to(uint32_t v, uint32_t* dst) {
-    __shared__ uint32_t smin;
-    if (threadIdx.x == 0) smin = 0xFFFFFFFFu;
-    __syncthreads();
-    v = __reduce_min_sync(0xffffffffu, v);
-    if ((threadIdx.x & 31) == 0 && v != 0xFFFFFFFFu) atomicMin(&smin, v);
-    __syncthreads();
-    if (threadIdx.x == 0 && smin != 0xFFFFFFFFu) atomicMin(dst, smin);
+// Count of the L values row[0..L) that are >= thr, by a group of G lanes (G a
+// power of two; all 32 lanes of the warp call this together).  Every lane of
+// a group returns the group's count.
+template <int G>
+__device__ __forceinline__ uint32_t group_count_ge(const uint32_t* row, uint32_t L, uint32_t thr,
+                                                   bool live) {
+    const uint32_t gl = (threadIdx.x & 31) & (G - 1);
+    uint32_t cnt = 0;
+    if (live)
+        for (uint32_t li = gl; li < L; li += G) cnt += ld_l2(row + li) >= thr;
+#pragma unroll
+    for (int off = G / 2; off >= 1; off >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, off);
+    return cnt;
+}
+
+// One removed-neighbour slot per entry, up to four per lane at once (loads
+// first, then the atomics) so each lane keeps several memory operations in
+// flight.
+__device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&col)[4],
+                                       const uint32_t (&slot)[4], const bool (&ok)[4], uint32_t k,
+                                       uint32_t q) {
+    uint32_t y[4], cy[4], old[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        y[i] = col[i] * j.n + j.divL.div(slot[i]);
+        cy[i] = ok[i] ? ld_l2(j.cnt + y[i]) : 0u;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const uint32_t lmd = j.col0 + col[i] + 1;
+        old[i] = (ok[i] && cy[i] >= lmd) ? atomicSub(j.deg + (uint64_t)col[i] * j.nL + slot[i], 1u)
+                                         : 0u;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const uint32_t lmd = j.col0 + col[i] + 1;
+        if (ok[i] && cy[i] >= lmd && old[i] == k + 1) {
+            if (atomicSub(j.cnt + y[i], 1u) == lmd) {
+                j.t[y[i]] = k;
+                enqueue(j, q, y[i]);
+            }
+        }
+    }
 }
 
 // ---- phases ---------------------------------------------------------------
+
+// SCAN(K) over `cnt_nodes` alive entries taken from `src` (or 0..nx-1 when
+// src is null, the first level): removed nodes get t = K and are queued,
+// the rest keep their count and move to `out`.
+template <int G>
+__device__ void scan_nodes(const PeelJob& j, const uint32_t* src, uint32_t cnt_nodes, uint32_t k,
+                           uint32_t q, uint32_t* out, uint32_t* out_cnt) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t per_warp = 32 / G;
+    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t base = gw * per_warp; base < cnt_nodes; base += nw * per_warp) {
+        const uint32_t idx = base + lane / G;
+        bool live = idx < cnt_nodes;
+        const uint32_t x = live ? (src ? ld_l2(src + idx) : idx) : 0;
+        if (live && src && ld_l2(j.t + x) != UNSET) live = false;  // removed last level
+        const uint32_t c = j.divN.div(x);
+        const uint32_t v = x - c * j.n;
+        const uint32_t cnt = group_count_ge<G>(j.deg + (uint64_t)c * j.nL + (uint64_t)v * j.L, j.L,
+                                               k + 1, live);
+        if (live && (lane & (G - 1)) == 0) {
+            j.cnt[x] = cnt;
+            if (cnt < j.col0 + c + 1) {
+                j.t[x] = k;
+                enqueue(j, q, x);
+            } else {
+                if (!src) j.t[x] = UNSET;
+                push(out, out_cnt, x);
+            }
+        }
+    }
+}
 
 template <int G>
 __device__ void phase_init(const PeelJob& j) {
@@ -300,178 +313,164 @@ __device__ void phase_init(const PeelJob& j) {
         const uint32_t d0 = __ldg(j.deg0 + i);
         for (uint32_t c = 0; c < j.ncols; c++) j.deg[(uint64_t)c * j.nL + i] = d0;
     }
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < (uint64_t)j.ncols * j.n;
-         i += stride)
-        j.dflag[i] = 0;
-    // Top-lambda of every (column, node); level 0 split into frontier / alive
+    __threadfence();
+    // the degree copies are read back by other warps of this same phase only
+    // for their own rows, which each group copies itself below
     const uint32_t lane = threadIdx.x & 31;
-    const uint32_t per_warp = 32 / G;
-    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t nx = j.ncols * j.n;
-    uint32_t lmin = 0xFFFFFFFFu;
-    for (uint32_t base = gw * per_warp; base < nx; base += nw * per_warp) {
-        uint32_t x = base + lane / G;
-        bool live = x < nx;
-        uint32_t c = live ? j.divN.div(x) : 0;
-        uint32_t v = x - c * j.n;
-        uint32_t lmd = j.col0 + c + 1;
-        uint32_t tv = group_topl<G>(j.deg0 + (uint64_t)v * j.L, j.L, live ? lmd : 0, j.upper_bits,
-                                    live, false);
-        if (live && (lane & (G - 1)) == 0) {
-            j.t[x] = tv;
-            if (tv == 0) push_frontier(j, 0, x);
-            else {
-                push(j.alive[1], &j.ctl->alive_cnt[1], x);
-                lmin = min(lmin, tv);
-            }
-        }
-    }
-    block_min_to(lmin, &j.ctl->next_min);
-}
-
-__device__ void phase_expand(const PeelJob& j) {
-    const PeelCtl* c = j.ctl;
-    const uint32_t f = ld_l2(&c->front_cur);
-    const uint32_t fsize = ld_l2(&c->front_cnt[f]);
-    const uint32_t csize = ld_l2(&c->chunk_cnt[f]);
-    const uint32_t k = ld_l2(&c->level);
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t* F = j.front[f];
-    // long rows: CHUNK-entry items, one per warp, four slots per lane
-    for (uint32_t ci = gw; ci < csize; ci += nw) {
-        const uint64_t it = __ldcg(reinterpret_cast<const unsigned long long*>(j.chunks[f]) + ci);
-        const uint32_t x = (uint32_t)it, ch = (uint32_t)(it >> 32);
-        const uint32_t col = j.divN.div(x);
-        const uint32_t v = x - col * j.n;
-        const uint32_t b = __ldg(j.node_ptr + v) + ch * CHUNK;
-        const uint32_t e = min(__ldg(j.node_ptr + v + 1), b + CHUNK);
-        for (uint32_t q0 = b; q0 < e; q0 += 128) {
-            uint32_t cols[4], slot[4];
-            bool ok[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                uint32_t q = q0 + lane + 32 * i;
-                ok[i] = q < e;
-                slot[i] = ok[i] ? __ldg(j.adj + q) : 0u;
-                cols[i] = col;
-            }
-            visit4(j, cols, slot, ok, k);
-        }
-    }
-    // short rows: 32 frontier nodes per warp, their adjacency (at most 1024
-    // entries) flattened over the lanes; the owner of entry q is found by
-    // binary search over the warp's exclusive scan of row lengths
-    for (uint32_t base = gw * 32; base < fsize; base += nw * 32) {
-        uint32_t i = base + lane;
-        uint32_t x = i < fsize ? ld_l2(F + i) : 0;
-        uint32_t col = j.divN.div(x);
-        uint32_t v = x - col * j.n;
-        uint32_t b = 0, len = 0;
-        if (i < fsize) {
-            b = __ldg(j.node_ptr + v);
-            len = __ldg(j.node_ptr + v + 1) - b;
-        }
-        uint32_t incl = len;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= (uint32_t)o) incl += y;
-        }
-        uint32_t excl = incl - len;
-        uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-        for (uint32_t jb = 0; jb < total; jb += 128) {
-            uint32_t cols[4], slot[4];
-            bool ok[4];
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                const uint32_t q = jb + 32 * i + lane;
-                uint32_t own = 0;
-#pragma unroll
-                for (int step = 16; step >= 1; step >>= 1) {
-                    uint32_t cand = own + step;
-                    uint32_t ex = __shfl_sync(0xffffffffu, excl, cand & 31);
-                    if (cand < 32 && ex <= q) own = cand;
-                }
-                const uint32_t ob = __shfl_sync(0xffffffffu, b, own);
-                const uint32_t oe = __shfl_sync(0xffffffffu, excl, own);
-                cols[i] = __shfl_sync(0xffffffffu, col, own);
-                ok[i] = q < total;
-                slot[i] = ok[i] ? __ldg(j.adj + ob + (q - oe)) : 0u;
-            }
-            visit4(j, cols, slot, ok, k);
-        }
-    }
+    (void)lane;
 }
 
 template <int G>
-__device__ void phase_recompute(const PeelJob& j) {
+__device__ void phase_scan(const PeelJob& j, bool first) {
     const PeelCtl* c = j.ctl;
-    const uint32_t dsize = ld_l2(&c->dirty_cnt);
     const uint32_t k = ld_l2(&c->level);
-    const uint32_t fout = ld_l2(&c->front_cur) ^ 1;
+    const uint32_t q = ld_l2(&c->q_cur);
+    const uint32_t prev = ld_l2(&c->prev_tail);
+    // the other queue held the previous level's items: blank them for reuse
+    unsigned long long* other = j.queue[q ^ 1];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < prev && i < j.qcap;
+         i += gridDim.x * blockDim.x)
+        other[i] = EMPTY;
+    if (first) {
+        scan_nodes<G>(j, nullptr, j.ncols * j.n, k, q, j.alive[1], &j.ctl->alive_cnt[1]);
+    } else {
+        const uint32_t a = ld_l2(&c->alive_cur);
+        scan_nodes<G>(j, j.alive[a], ld_l2(&c->alive_cnt[a]), k, q, j.alive[a ^ 1],
+                      &j.ctl->alive_cnt[a ^ 1]);
+    }
+}
+
+// DRAIN(K): each warp claims 32 queue slots at a time (one per lane) and
+// processes the items that are ready; it stops once no queued item is left
+// unprocessed.
+__device__ void phase_drain(const PeelJob& j) {
+    PeelCtl* c = j.ctl;
+    const uint32_t k = ld_l2(&c->level);
+    const uint32_t q = ld_l2(&c->q_cur);
+    const unsigned long long* Q = j.queue[q];
     const uint32_t lane = threadIdx.x & 31;
-    const uint32_t per_warp = 32 / G;
-    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    uint32_t lmin = 0xFFFFFFFFu;
-    for (uint32_t base = gw * per_warp; base < dsize; base += nw * per_warp) {
-        uint32_t idx = base + lane / G;
-        bool live = idx < dsize;
-        uint32_t y = live ? ld_l2(j.dirty + idx) : 0;
-        uint32_t col = j.divN.div(y);
-        uint32_t u = y - col * j.n;
-        uint32_t upper = live ? ld_l2(j.t + y) : 0;
-        uint32_t bits = upper ? 32 - __clz(upper) : 0;
-        bits = __reduce_max_sync(0xffffffffu, bits);
-        uint32_t nt = group_topl<G>(j.deg + (uint64_t)col * j.nL + (uint64_t)u * j.L, j.L,
-                                    live ? j.col0 + col + 1 : 0, bits, live, true);
-        if (live && (lane & (G - 1)) == 0) {
-            j.dflag[y] = 0;
-            if (nt <= k) {
-                j.t[y] = k;
-                push_frontier(j, fout, y);
+    uint64_t t0 = global_ns();  // last progress of this warp
+    bool finished = false;
+    while (!finished) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&c->q_head[q], 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        const uint32_t idx = base + lane;
+        bool outstanding = true;
+        uint32_t ns = 64;
+        while (__any_sync(0xffffffffu, outstanding)) {
+            unsigned long long it = EMPTY;
+            if (outstanding && idx < j.qcap) it = ld_relaxed64(Q + idx);
+            const bool ready = outstanding && it != EMPTY;
+            const uint32_t rmask = __ballot_sync(0xffffffffu, ready);
+            if (rmask) {
+                ns = 64;
+                const uint32_t x = (uint32_t)it, ch = (uint32_t)(it >> 32);
+                const uint32_t col = j.divN.div(x);
+                const uint32_t v = x - col * j.n;
+                uint32_t b = 0, e = 0;
+                if (ready) {
+                    b = __ldg(j.node_ptr + v);
+                    e = __ldg(j.node_ptr + v + 1);
+                }
+                const bool is_chunk = ready && (e - b) > SMALL_ROW;
+                // short rows of the ready lanes, flattened over the warp
+                const uint32_t len = (ready && !is_chunk) ? e - b : 0u;
+                uint32_t incl = len;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= (uint32_t)o) incl += y;
+                }
+                const uint32_t excl = incl - len;
+                const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+                for (uint32_t jb = 0; jb < total; jb += 128) {
+                    uint32_t cols[4], slot[4];
+                    bool ok[4];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const uint32_t qq = jb + 32 * i + lane;
+                        uint32_t own = 0;
+#pragma unroll
+                        for (int step = 16; step >= 1; step >>= 1) {
+                            uint32_t cand = own + step;
+                            uint32_t ex = __shfl_sync(0xffffffffu, excl, cand & 31);
+                            if (cand < 32 && ex <= qq) own = cand;
+                        }
+                        const uint32_t ob = __shfl_sync(0xffffffffu, b, own);
+                        const uint32_t oe = __shfl_sync(0xffffffffu, excl, own);
+                        cols[i] = __shfl_sync(0xffffffffu, col, own);
+                        ok[i] = qq < total;
+                        slot[i] = ok[i] ? __ldg(j.adj + ob + (qq - oe)) : 0u;
+                    }
+                    visit4(j, cols, slot, ok, k, q);
+                }
+                // chunk items, one at a time across the whole warp
+                uint32_t cm = __ballot_sync(0xffffffffu, is_chunk);
+                while (cm) {
+                    const uint32_t src = __ffs(cm) - 1;
+                    cm &= cm - 1;
+                    const uint32_t sb = __shfl_sync(0xffffffffu, b, src);
+                    const uint32_t se = __shfl_sync(0xffffffffu, e, src);
+                    const uint32_t sc = __shfl_sync(0xffffffffu, col, src);
+                    const uint32_t sch = __shfl_sync(0xffffffffu, ch, src);
+                    const uint32_t cb = sb + sch * CHUNK;
+                    const uint32_t ce = min(se, cb + CHUNK);
+                    for (uint32_t q0 = cb; q0 < ce; q0 += 128) {
+                        uint32_t cols[4], slot[4];
+                        bool ok[4];
+#pragma unroll
+                        for (int i = 0; i < 4; i++) {
+                            const uint32_t p = q0 + lane + 32 * i;
+                            ok[i] = p < ce;
+                            slot[i] = ok[i] ? __ldg(j.adj + p) : 0u;
+                            cols[i] = sc;
+                        }
+                        visit4(j, cols, slot, ok, k, q);
+                    }
+                }
+                if (ready) outstanding = false;
+                // every lane's enqueues raised `pending` before this point
+                // (ordered by the warp barrier), so the decrement cannot let
+                // it reach zero while their items wait
+                __syncwarp();
+                if (lane == 0) {
+                    __threadfence();
+                    atomicSub(&c->pending, (uint32_t)__popc(rmask));
+                }
+                t0 = global_ns();
             } else {
-                j.t[y] = nt;
-                lmin = min(lmin, nt);
+                // nothing ready: done when no queued item is left anywhere
+                if (ld_acquire(&c->pending) == 0) {
+                    finished = true;
+                    break;
+                }
+                __nanosleep(ns);
+                if (ns < 1024) ns <<= 1;
+                if (global_ns() - t0 > j.timeout_ns) {
+                    if (lane == 0) atomicExch(&c->err, ERR_BARRIER);
+                    finished = true;
+                    break;
+                }
+                if (ld_acquire(&c->err) != ERR_NONE) {
+                    finished = true;
+                    break;
+                }
             }
         }
     }
-    block_min_to(lmin, &j.ctl->next_min);
-}
-
-__device__ void phase_scan(const PeelJob& j) {
-    const PeelCtl* c = j.ctl;
-    const uint32_t a = ld_l2(&c->alive_cur);
-    const uint32_t asize = ld_l2(&c->alive_cnt[a]);
-    const uint32_t k = ld_l2(&c->level);
-    const uint32_t f = ld_l2(&c->front_cur);
-    const uint32_t* A = j.alive[a];
-    uint32_t* out = j.alive[a ^ 1];
-    uint32_t lmin = 0xFFFFFFFFu;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < asize; i += gridDim.x * blockDim.x) {
-        uint32_t x = ld_l2(A + i);
-        uint32_t tx = ld_l2(j.t + x);
-        if (tx == k) push_frontier(j, f, x);
-        else if (tx > k) {
-            push(out, &j.ctl->alive_cnt[a ^ 1], x);
-            lmin = min(lmin, tx);
-        }
-    }
-    block_min_to(lmin, &j.ctl->next_min);
 }
 
 template <int G>
 __global__ void __launch_bounds__(512) k_peel(PeelJob j) {
     phase_init<G>(j);
     if (!grid_barrier(j)) return;
+    phase_scan<G>(j, true);
+    if (!grid_barrier(j)) return;
     for (;;) {
         const uint32_t ph = ld_l2(&j.ctl->phase);
-        if (ph == PH_EXPAND) phase_expand(j);
-        else if (ph == PH_RECOMPUTE) phase_recompute<G>(j);
-        else if (ph == PH_SCAN) phase_scan(j);
+        if (ph == PH_DRAIN) phase_drain(j);
+        else if (ph == PH_SCAN) phase_scan<G>(j, false);
         else return;
         if (!grid_barrier(j)) return;
     }
@@ -486,8 +485,8 @@ static uint32_t env_u32(const char* name, uint32_t dflt) {
 
 uint32_t peel_columns_per_group(const DeviceGraph* d) {
     // every column needs an n*L degree table plus ~8 words per node; keep the
-    // group's working set within a budget (FC_PEEL_GROUP_BYTES, default 4 GiB)
-    uint64_t per_col = ((uint64_t)d->n * d->L + 8ull * d->n) * 4;
+    // group's working set within a budget (FC_PEEL_GROUP_MB, default 4 GiB)
+    uint64_t per_col = ((uint64_t)d->n * d->L + 8ull * d->n) * 4 + d->entries / 8;
     uint64_t budget = (uint64_t)env_u32("FC_PEEL_GROUP_MB", 4096) << 20;
     uint64_t cols = per_col ? budget / per_col : d->L;
     uint32_t want = env_u32("FC_PEEL_GROUP_COLS", 0);
@@ -520,18 +519,20 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
     const uint32_t n = d->n, L = d->L;
     const uint64_t nx = (uint64_t)ncols * n;
     const uint64_t nL = (uint64_t)n * L;
-    // workspace: chunk0 chunk1 (uint64) | deg | alive0 alive1 front0 front1
-    // dirty dflag | ctl.  A sub-round's chunk items number at most one per
-    // removed node plus entries / CHUNK per column.
-    const uint64_t nchunk = nx + ((uint64_t)ncols * d->entries + CHUNK - 1) / CHUNK + 1;
-    size_t words = 4 * nchunk + (size_t)(ncols * nL) + 6 * nx + 256;
+    // workspace: queue0 queue1 (uint64) | deg | cnt alive0 alive1 | ctl.
+    // A level queues each removed node once, long rows as entries/CHUNK + 1
+    // items, so a queue holds at most nx + ncols * entries / CHUNK items.
+    const uint64_t qcap = nx + ((uint64_t)ncols * d->entries + CHUNK - 1) / CHUNK + 64;
+    if (qcap >= (1ull << 32)) return FC_ERR_TOO_LARGE;
+    size_t words = 4 * qcap + (size_t)(ncols * nL) + 3 * nx + 256;
     FC_TRY(ensure_ws(d, words * 4));
     uint32_t* w = (uint32_t*)d->ws;
     PeelJob j;
-    j.chunks[0] = (uint64_t*)w;
-    w += 2 * nchunk;
-    j.chunks[1] = (uint64_t*)w;
-    w += 2 * nchunk;
+    j.queue[0] = (unsigned long long*)w;
+    w += 2 * qcap;
+    j.queue[1] = (unsigned long long*)w;
+    w += 2 * qcap;
+    j.qcap = (uint32_t)qcap;
     j.n = n;
     j.L = L;
     j.col0 = col0;
@@ -545,23 +546,17 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
     j.deg = w;
     w += ncols * nL;
     j.t = d->table + (uint64_t)col0 * n;
+    j.cnt = w; w += nx;
     j.alive[0] = w; w += nx;
     j.alive[1] = w; w += nx;
-    j.front[0] = w; w += nx;
-    j.front[1] = w; w += nx;
-    j.dirty = w; w += nx;
-    j.dflag = w; w += nx;
     j.ctl = (PeelCtl*)(((uintptr_t)w + 255) & ~(uintptr_t)255);
     j.max_level = d->max_deg + 1;
-    j.max_subrounds = (uint32_t)std::min<uint64_t>(0xFFFFFFF0ull, nx + d->max_deg + 16);
-    uint32_t bits = 0;
-    while (bits < 32 && (d->max_deg >> bits)) bits++;
-    j.upper_bits = bits;
     j.timeout_ns = (uint64_t)env_u32("FC_BARRIER_TIMEOUT_MS", 4000) * 1000000ull;
     PeelCtl init{};
-    init.phase = PH_SCAN;  // INIT behaves as a scan into alive[1]
+    init.phase = PH_SCAN;  // INIT + the first scan write alive[1]
     init.alive_cur = 0;
-    init.next_min = 0xFFFFFFFFu;
+    init.q_cur = 0;
+    FC_CUDA_TRY(cudaMemsetAsync(j.queue[0], 0xFF, 2 * qcap * 8, s));
     FC_CUDA_TRY(cudaMemcpyAsync(j.ctl, &init, sizeof(init), cudaMemcpyHostToDevice, s));
     cudaEvent_t e0, e1;
     FC_CUDA_TRY(cudaEventCreate(&e0));
@@ -587,9 +582,11 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
     if (st) {
         st->ms = ms;
         st->levels = out.levels;
-        st->subrounds = out.subrounds;
+        st->subrounds = out.items;
         st->err = out.err;
-        for (int i = 0; i < 3; i++) st->phase_ms[i] = out.ph_ns[i] * 1e-6;
+        st->phase_ms[0] = out.ph_ns[0] * 1e-6;
+        st->phase_ms[1] = out.ph_ns[1] * 1e-6;
+        st->phase_ms[2] = 0;
     }
     if (out.err) return FC_ERR_ITER_LIMIT;
     return FC_OK;
