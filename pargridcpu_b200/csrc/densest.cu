@@ -348,6 +348,8 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st) {
     FC_CUDA_TRY(cudaMemcpyAsync(s->kmax.data(), s->d_kmax, L * 4, cudaMemcpyDeviceToHost, st));
     FC_CUDA_TRY(cudaStreamSynchronize(st));
     d->kmax = s->kmax;
+    for (uint32_t l = 0; l < L; l++)
+        if (s->kmax[l] > d->max_deg) return FC_ERR_DEVICE;  // not a valid core table
     s->hbase.assign(L, 0);
     s->nbase.assign(L, 0);
     s->cbase.assign(L, 0);

@@ -39,7 +39,7 @@ namespace cg = cooperative_groups;
 
 namespace fc {
 
-enum : uint32_t { PH_SCAN = 1, PH_DRAIN = 2, PH_DONE = 3 };
+enum : uint32_t { PH_SCAN = 1, PH_DRAIN = 2, PH_DONE = 3, PH_INIT = 4 };
 enum : uint32_t { ERR_NONE = 0, ERR_BARRIER = 1, ERR_LIMIT = 2, ERR_QUEUE = 3 };
 constexpr uint32_t UNSET = 0xFFFFFFFFu;
 constexpr unsigned long long EMPTY = ~0ull;
@@ -131,7 +131,10 @@ __device__ void leader_step(volatile PeelCtl* c, const PeelJob& j) {
         }
     };
     switch (c->phase) {
-        case PH_SCAN:  // also the state after INIT + the first scan
+        case PH_INIT:  // degree tables copied: the first scan follows
+            c->phase = PH_SCAN;
+            break;
+        case PH_SCAN:  // the first scan wrote alive[1]
             c->alive_cur ^= 1;
             if (c->q_tail[c->q_cur] > 0) c->phase = PH_DRAIN;
             else if (c->alive_cnt[c->alive_cur] == 0) c->phase = PH_DONE;
@@ -553,7 +556,7 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
     j.max_level = d->max_deg + 1;
     j.timeout_ns = (uint64_t)env_u32("FC_BARRIER_TIMEOUT_MS", 4000) * 1000000ull;
     PeelCtl init{};
-    init.phase = PH_SCAN;  // INIT + the first scan write alive[1]
+    init.phase = PH_INIT;
     init.alive_cur = 0;
     init.q_cur = 0;
     FC_CUDA_TRY(cudaMemsetAsync(j.queue[0], 0xFF, 2 * qcap * 8, s));
