@@ -15,6 +15,7 @@ void count_launch(uint32_t k) { g_launches.fetch_add(k, std::memory_order_relaxe
 fc_status coreindex(fc_graph* g, uint32_t* out, bool out_on_device, cudaStream_t s) {
     FC_TRY(upload(g, s));
     DeviceGraph* d = g->dev;
+    d->home = s;
     if (!d->table_valid) {
         invalidate_densest(d);
         d->stats.peel_ms = 0;

@@ -48,13 +48,13 @@ struct DensState {
 };
 
 template <class T>
-static fc_status grow(T*& p, uint64_t& cap, uint64_t need) {
+static fc_status grow(T*& p, uint64_t& cap, uint64_t need, cudaStream_t st) {
     if (p && cap >= need) return FC_OK;
-    if (p) cudaFree(p);
+    dev_free(p, st);
     p = nullptr;
     cap = 0;
     uint64_t c = need + need / 4 + 16;
-    FC_CUDA_TRY(cudaMalloc(&p, c * sizeof(T)));
+    FC_TRY(dev_alloc((void**)&p, c * sizeof(T), st));
     cap = c;
     return FC_OK;
 }
@@ -62,16 +62,11 @@ static fc_status grow(T*& p, uint64_t& cap, uint64_t need) {
 void free_densest_state(DeviceGraph* d) {
     DensState* s = (DensState*)d->dens;
     if (!s) return;
-    cudaFree(s->H);
-    cudaFree(s->N);
-    cudaFree(s->coreT);
-    cudaFree(s->d_hbase);
-    cudaFree(s->d_nbase);
-    cudaFree(s->d_kmax);
-    cudaFree(s->cells);
-    cudaFree(s->powl);
-    cudaFree(s->d_res);
-    cudaFree(s->cell_lk);
+    // called with the graph's work finished (release_device synchronizes)
+    for (void* p : {(void*)s->H, (void*)s->N, (void*)s->coreT, (void*)s->d_hbase,
+                    (void*)s->d_nbase, (void*)s->d_kmax, (void*)s->cells, (void*)s->powl,
+                    (void*)s->d_res, (void*)s->cell_lk})
+        dev_free(p, 0);
     delete s;
     d->dens = nullptr;
 }
@@ -337,7 +332,7 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st) {
     const uint32_t n = d->n, L = d->L;
     s->L = L;
     // per-lambda maxima
-    if (!s->d_kmax) FC_CUDA_TRY(cudaMalloc(&s->d_kmax, (L + 1) * 4));
+    if (!s->d_kmax) FC_TRY(dev_alloc((void**)&s->d_kmax, (L + 1) * 4, st));
     FC_CUDA_TRY(cudaMemsetAsync(s->d_kmax, 0, (L + 1) * 4, st));
     dim3 g((n + 255) / 256 < 64 ? (n + 255) / 256 : 64, L);
     if (g.x == 0) g.x = 1;
@@ -366,13 +361,13 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st) {
     s->hwords = hw;
     s->nwords = nw;
     s->ncells = nc;
-    FC_TRY(grow(s->H, s->H_cap, hw + 1));
-    FC_TRY(grow(s->N, s->N_cap, nw + 1));
-    FC_TRY(grow(s->cells, s->cells_cap, nc + 1));
-    FC_TRY(grow(s->cell_lk, s->cell_lk_cap, 2 * nc + 2));
-    FC_TRY(grow(s->d_hbase, s->hbase_cap, L + 1));
-    FC_TRY(grow(s->d_nbase, s->nbase_cap, L + 1));
-    if (!s->coreT) FC_CUDA_TRY(cudaMalloc(&s->coreT, (uint64_t)n * L * 4 + 4));
+    FC_TRY(grow(s->H, s->H_cap, hw + 1, st));
+    FC_TRY(grow(s->N, s->N_cap, nw + 1, st));
+    FC_TRY(grow(s->cells, s->cells_cap, nc + 1, st));
+    FC_TRY(grow(s->cell_lk, s->cell_lk_cap, 2 * nc + 2, st));
+    FC_TRY(grow(s->d_hbase, s->hbase_cap, L + 1, st));
+    FC_TRY(grow(s->d_nbase, s->nbase_cap, L + 1, st));
+    if (!s->coreT) FC_TRY(dev_alloc((void**)&s->coreT, (uint64_t)n * L * 4 + 4, st));
     FC_CUDA_TRY(cudaMemcpyAsync(s->d_hbase, s->hbase.data(), L * 8, cudaMemcpyHostToDevice, st));
     FC_CUDA_TRY(cudaMemcpyAsync(s->d_nbase, s->nbase.data(), L * 8, cudaMemcpyHostToDevice, st));
     // cell list (lambda index, k) in the reference's order, for k_cells
@@ -440,7 +435,7 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st) {
 static fc_status score_cells(DeviceGraph* d, double beta, cudaStream_t st) {
     DensState* s = (DensState*)d->dens;
     const uint32_t L = d->L;
-    if (!s->powl) FC_CUDA_TRY(cudaMalloc(&s->powl, L * 8 + 8));
+    if (!s->powl) FC_TRY(dev_alloc((void**)&s->powl, L * 8 + 8, st));
     std::vector<double> pw(L);
     for (uint32_t l = 0; l < L; l++) pw[l] = pow((double)(l + 1), beta);  // pow((l+1), beta)
     FC_CUDA_TRY(cudaMemcpyAsync(s->powl, pw.data(), L * 8, cudaMemcpyHostToDevice, st));
@@ -468,7 +463,7 @@ fc_status densest(fc_graph* g, const double* betas, uint32_t nb, fc_densest_resu
     FC_CUDA_TRY(cudaEventRecord(e0, st));
     FC_TRY(build_hist(d, st));
     DensState* s = (DensState*)d->dens;
-    if (!s->d_res) FC_CUDA_TRY(cudaMalloc(&s->d_res, sizeof(fc_densest_result)));
+    if (!s->d_res) FC_TRY(dev_alloc((void**)&s->d_res, sizeof(fc_densest_result), st));
     for (uint32_t b = 0; b < nb; b++) {
         FC_TRY(score_cells(d, betas[b], st));
         k_fold<<<1, 32, 0, st>>>(s->cells, s->ncells, betas[b], s->d_res);

@@ -65,13 +65,20 @@ struct DeviceGraph {
     size_t ws_bytes = 0;
     uint64_t bytes = 0;            // CSR + table
     fc_stats stats{};              // diagnostics of the last computations
+    cudaStream_t home = nullptr;   // stream of the last call (device frees are ordered on it)
 };
+
+// Device memory from the device's stream-ordered pool, which keeps freed
+// memory for reuse (release threshold raised once per device), so that
+// dropping and re-uploading a graph does not return to the driver.
+fc_status dev_alloc(void** p, size_t bytes, cudaStream_t s);
+void dev_free(void* p, cudaStream_t s);
 
 // kernels launched by this library (fc_launch_count)
 void count_launch(uint32_t k = 1);
 
 // scratch owned by a DeviceGraph, grown on demand
-fc_status ensure_ws(DeviceGraph* d, size_t bytes);
+fc_status ensure_ws(DeviceGraph* d, size_t bytes, cudaStream_t s);
 void free_densest_state(DeviceGraph* d);
 void invalidate_densest(DeviceGraph* d);
 

@@ -72,13 +72,38 @@ __global__ void k_max(const uint32_t* __restrict__ a, uint64_t len, uint32_t* ou
     if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
-fc_status ensure_ws(DeviceGraph* d, size_t bytes) {
+fc_status dev_alloc(void** p, size_t bytes, cudaStream_t s) {
+    static std::mutex mu;
+    static bool pool_set[64] = {};
+    int dev = 0;
+    FC_CUDA_TRY(cudaGetDevice(&dev));
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (dev < 64 && !pool_set[dev]) {
+            cudaMemPool_t pool;
+            if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+                uint64_t keep = ~0ull;
+                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            }
+            cudaGetLastError();
+            pool_set[dev] = true;
+        }
+    }
+    FC_CUDA_TRY(cudaMallocAsync(p, bytes ? bytes : 16, s));
+    return FC_OK;
+}
+
+void dev_free(void* p, cudaStream_t s) {
+    if (p) cudaFreeAsync(p, s);
+}
+
+fc_status ensure_ws(DeviceGraph* d, size_t bytes, cudaStream_t s) {
     if (d->ws_bytes >= bytes) return FC_OK;
-    if (d->ws) cudaFree(d->ws);
+    dev_free(d->ws, s);
     d->ws = nullptr;
     d->ws_bytes = 0;
     size_t b = bytes + bytes / 8;
-    FC_CUDA_TRY(cudaMalloc(&d->ws, b));
+    FC_TRY(dev_alloc(&d->ws, b, s));
     d->ws_bytes = b;
     return FC_OK;
 }
@@ -105,6 +130,7 @@ fc_status upload(fc_graph* g, cudaStream_t s) {
     d->n = n;
     d->L = L;
     d->entries = entries;
+    d->home = s;
     g->dev = d;
     uint64_t noff = (uint64_t)L * (n + 1);
     uint64_t* d_off = nullptr;
@@ -117,10 +143,10 @@ fc_status upload(fc_graph* g, cudaStream_t s) {
     FC_CUDA_TRY(cudaMallocAsync(&d_in, entries * 4 + 4, s));
     FC_CUDA_TRY(cudaMallocAsync(&rowlen, (uint64_t)n * 4 + 4, s));
     FC_CUDA_TRY(cudaMallocAsync(&d_max, 8, s));
-    FC_CUDA_TRY(cudaMalloc(&d->node_ptr, ((uint64_t)n + 1) * 4));
-    FC_CUDA_TRY(cudaMalloc(&d->adj, entries * 4 + 4));
-    FC_CUDA_TRY(cudaMalloc(&d->deg0, (uint64_t)n * L * 4 + 4));
-    FC_CUDA_TRY(cudaMalloc(&d->table, (uint64_t)n * L * 4 + 4));
+    FC_TRY(dev_alloc((void**)&d->node_ptr, ((uint64_t)n + 1) * 4, s));
+    FC_TRY(dev_alloc((void**)&d->adj, entries * 4 + 4, s));
+    FC_TRY(dev_alloc((void**)&d->deg0, (uint64_t)n * L * 4 + 4, s));
+    FC_TRY(dev_alloc((void**)&d->table, (uint64_t)n * L * 4 + 4, s));
     d->bytes = ((uint64_t)n + 1) * 4 + entries * 4 + 2ull * n * L * 4;
     if (noff) FC_CUDA_TRY(cudaMemcpyAsync(d_off, g->off.p, noff * 8, cudaMemcpyHostToDevice, s));
     if (entries) FC_CUDA_TRY(cudaMemcpyAsync(d_in, g->adj.p, entries * 4, cudaMemcpyHostToDevice, s));
@@ -160,12 +186,16 @@ void release_device(fc_graph* g) {
     int cur = -1;
     cudaGetDevice(&cur);
     if (d->device >= 0 && d->device != cur) cudaSetDevice(d->device);
+    // the last call's work is done before its memory returns to the pool;
+    // the frees go on the legacy stream, which outlives any caller stream
+    cudaStreamSynchronize(d->home);
+    cudaGetLastError();
     free_densest_state(d);
-    cudaFree(d->node_ptr);
-    cudaFree(d->adj);
-    cudaFree(d->deg0);
-    cudaFree(d->table);
-    if (d->ws) cudaFree(d->ws);
+    dev_free(d->node_ptr, 0);
+    dev_free(d->adj, 0);
+    dev_free(d->deg0, 0);
+    dev_free(d->table, 0);
+    dev_free(d->ws, 0);
     if (cur >= 0 && d->device != cur) cudaSetDevice(cur);
     delete d;
     g->dev = nullptr;

@@ -15,7 +15,8 @@
 //             FCSyncLeft.cpp:99-103).  Each of those crossings happens exactly
 //             once, so every node is queued once.  Removals cascade through
 //             the queue without any barrier; the level ends when no queued item
-//             is left unprocessed (a pending-items counter reaches zero).
+//             is left unprocessed (the processed-items count reaches the
+//             reserved-items count).
 //
 // This computes the same table as the reference's get_index2 bucket peel
 // (CoreIndexParallel/CoreIndex.cpp:62-109) and ParGrid's per-cell PeelSync:
@@ -49,7 +50,7 @@ struct PeelCtl {
     uint32_t level, alive_cur, q_cur, prev_tail;
     uint32_t alive_cnt[2];
     uint32_t q_tail[2], q_head[2];
-    uint32_t pending;     // queued items not yet processed (current level)
+    uint32_t processed[2];  // queue items fully processed, per queue
     uint32_t levels, items, pad;
     uint64_t t_last;      // globaltimer at the last barrier
     uint64_t ph_ns[4];    // time per phase kind: scan, drain
@@ -75,6 +76,9 @@ struct PeelJob {
     PeelCtl* ctl;
     uint32_t max_level;
     uint64_t timeout_ns;
+    // optional per-level trace: [level][scan|drain] = {ns, items, alive}
+    unsigned long long* trace;
+    uint32_t trace_levels;
 };
 
 // ---- memory-model helpers -------------------------------------------------
@@ -112,6 +116,12 @@ __device__ void leader_step(volatile PeelCtl* c, const PeelJob& j) {
         uint64_t now = global_ns();
         uint32_t kind = c->phase == PH_DRAIN ? 1 : 0;
         if (c->t_last) c->ph_ns[kind] += now - c->t_last;
+        if (j.trace && c->t_last && c->level < j.trace_levels && c->phase != PH_INIT) {
+            unsigned long long* r = j.trace + 3ull * (2ull * c->level + kind);
+            r[0] = now - c->t_last;
+            r[1] = c->q_tail[c->q_cur];
+            r[2] = c->alive_cnt[c->alive_cur ^ (kind == 0 ? 1u : 0u)];
+        }
         c->t_last = now;
     }
     auto next_level = [&]() {
@@ -120,7 +130,7 @@ __device__ void leader_step(volatile PeelCtl* c, const PeelJob& j) {
         c->q_cur ^= 1;
         c->q_tail[c->q_cur] = 0;
         c->q_head[c->q_cur] = 0;
-        c->pending = 0;
+        c->processed[c->q_cur] = 0;
         c->level = c->level + 1;
         c->levels = c->levels + 1;
         c->alive_cnt[c->alive_cur ^ 1] = 0;
@@ -199,24 +209,15 @@ __device__ __forceinline__ uint32_t row_len(const PeelJob& j, uint32_t v) {
     return __ldg(j.node_ptr + v + 1) - __ldg(j.node_ptr + v);
 }
 
-// Queue the work items of a removed x (called by the lanes that removed a
-// node, together): one item for a short row, ceil(len / CHUNK) chunk items
-// for a long one.  `pending` is raised before the items become visible, so
-// it cannot reach zero while they wait.
-__device__ __forceinline__ void enqueue(const PeelJob& j, uint32_t q, uint32_t x) {
-    const uint32_t v = x - j.divN.div(x) * j.n;
-    const uint32_t len = row_len(j, v);
-    const uint32_t nit = len <= SMALL_ROW ? 1u : (len + CHUNK - 1) / CHUNK;
-    cg::coalesced_group g = cg::coalesced_threads();
-    const uint32_t incl = cg::inclusive_scan(g, nit);
-    uint32_t base = 0;
-    if (g.thread_rank() == g.size() - 1) {
-        atomicAdd(&j.ctl->pending, incl);
-        base = atomicAdd(&j.ctl->q_tail[q], incl);
-    }
-    base = g.shfl(base, g.size() - 1);
-    __threadfence();
-    const uint32_t first = base + incl - nit;
+// Work items of a removed x: one for a short row, ceil(len / CHUNK) chunk
+// items for a long one.
+__device__ __forceinline__ uint32_t items_of(const PeelJob& j, uint32_t x) {
+    const uint32_t len = row_len(j, x - j.divN.div(x) * j.n);
+    return len <= SMALL_ROW ? 1u : (len + CHUNK - 1) / CHUNK;
+}
+
+__device__ __forceinline__ void write_items(const PeelJob& j, uint32_t q, uint32_t first,
+                                            uint32_t x, uint32_t nit) {
     for (uint32_t c = 0; c < nit; c++) {
         const uint32_t idx = first + c;
         if (idx < j.qcap) {
@@ -227,6 +228,17 @@ __device__ __forceinline__ void enqueue(const PeelJob& j, uint32_t q, uint32_t x
             atomicExch(&j.ctl->err, ERR_QUEUE);
         }
     }
+}
+
+// Warp-wide inclusive scan.
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v) {
+    const uint32_t lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= (uint32_t)o) v += y;
+    }
+    return v;
 }
 
 // Count of the L values row[0..L) that are >= thr, by a group of G lanes (G a
@@ -246,7 +258,8 @@ __device__ __forceinline__ uint32_t group_count_ge(const uint32_t* row, uint32_t
 
 // One removed-neighbour slot per entry, up to four per lane at once (loads
 // first, then the atomics) so each lane keeps several memory operations in
-// flight.
+// flight.  All 32 lanes call it together; the nodes it removes are queued
+// with one reservation for the whole warp.
 __device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&col)[4],
                                        const uint32_t (&slot)[4], const bool (&ok)[4], uint32_t k,
                                        uint32_t q) {
@@ -262,14 +275,31 @@ __device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&col)[4
         old[i] = (ok[i] && cy[i] >= lmd) ? atomicSub(j.deg + (uint64_t)col[i] * j.nL + slot[i], 1u)
                                          : 0u;
     }
+    bool rem[4];
+    uint32_t nit[4], mine = 0;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         const uint32_t lmd = j.col0 + col[i] + 1;
-        if (ok[i] && cy[i] >= lmd && old[i] == k + 1) {
-            if (atomicSub(j.cnt + y[i], 1u) == lmd) {
-                j.t[y[i]] = k;
-                enqueue(j, q, y[i]);
-            }
+        rem[i] = false;
+        if (ok[i] && cy[i] >= lmd && old[i] == k + 1) rem[i] = atomicSub(j.cnt + y[i], 1u) == lmd;
+        nit[i] = 0;
+        if (rem[i]) {
+            j.t[y[i]] = k;
+            nit[i] = items_of(j, y[i]);
+            mine += nit[i];
+        }
+    }
+    if (!__any_sync(0xffffffffu, mine != 0)) return;
+    const uint32_t incl = warp_incl_scan(mine);
+    uint32_t base = 0;
+    if ((threadIdx.x & 31) == 31) base = atomicAdd(&j.ctl->q_tail[q], incl);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    uint32_t first = base + incl - mine;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        if (rem[i]) {
+            write_items(j, q, first, y[i], nit[i]);
+            first += nit[i];
         }
     }
 }
@@ -279,15 +309,18 @@ __device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&col)[4
 // SCAN(K) over `cnt_nodes` alive entries taken from `src` (or 0..nx-1 when
 // src is null, the first level): removed nodes get t = K and are queued,
 // the rest keep their count and move to `out`.
+// Survivors and queue items of a block are reserved with one atomic each per
+// block iteration (the counters are shared by the whole grid).
 template <int G>
 __device__ void scan_nodes(const PeelJob& j, const uint32_t* src, uint32_t cnt_nodes, uint32_t k,
                            uint32_t q, uint32_t* out, uint32_t* out_cnt) {
+    __shared__ uint32_t s_keep[32], s_item[32], s_kbase, s_ibase;
     const uint32_t lane = threadIdx.x & 31;
-    const uint32_t per_warp = 32 / G;
-    const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t base = gw * per_warp; base < cnt_nodes; base += nw * per_warp) {
-        const uint32_t idx = base + lane / G;
+    const uint32_t warp = threadIdx.x >> 5;
+    const uint32_t nwarps = blockDim.x >> 5;
+    const uint32_t per_block = blockDim.x / G;
+    for (uint32_t base = blockIdx.x * per_block; base < cnt_nodes; base += gridDim.x * per_block) {
+        const uint32_t idx = base + threadIdx.x / G;
         bool live = idx < cnt_nodes;
         const uint32_t x = live ? (src ? ld_l2(src + idx) : idx) : 0;
         if (live && src && ld_l2(j.t + x) != UNSET) live = false;  // removed last level
@@ -295,16 +328,38 @@ __device__ void scan_nodes(const PeelJob& j, const uint32_t* src, uint32_t cnt_n
         const uint32_t v = x - c * j.n;
         const uint32_t cnt = group_count_ge<G>(j.deg + (uint64_t)c * j.nL + (uint64_t)v * j.L, j.L,
                                                k + 1, live);
-        if (live && (lane & (G - 1)) == 0) {
+        const bool lead = live && (lane & (G - 1)) == 0;
+        const bool remove = lead && cnt < j.col0 + c + 1;
+        const bool keep = lead && !remove;
+        const uint32_t nit = remove ? items_of(j, x) : 0u;
+        if (lead) {
             j.cnt[x] = cnt;
-            if (cnt < j.col0 + c + 1) {
-                j.t[x] = k;
-                enqueue(j, q, x);
-            } else {
-                if (!src) j.t[x] = UNSET;
-                push(out, out_cnt, x);
-            }
+            if (remove) j.t[x] = k;
+            else if (!src) j.t[x] = UNSET;
         }
+        const uint32_t kin = warp_incl_scan(keep ? 1u : 0u);
+        const uint32_t iin = warp_incl_scan(nit);
+        if (lane == 31) {
+            s_keep[warp] = kin;
+            s_item[warp] = iin;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t kt = 0, it = 0;
+            for (uint32_t w = 0; w < nwarps; w++) {
+                uint32_t a = s_keep[w], b = s_item[w];
+                s_keep[w] = kt;
+                s_item[w] = it;
+                kt += a;
+                it += b;
+            }
+            s_kbase = kt ? atomicAdd(out_cnt, kt) : 0u;
+            s_ibase = it ? atomicAdd(&j.ctl->q_tail[q], it) : 0u;
+        }
+        __syncthreads();
+        if (keep) out[s_kbase + s_keep[warp] + kin - 1] = x;
+        if (remove) write_items(j, q, s_ibase + s_item[warp] + iin - nit, x, nit);
+        __syncthreads();
     }
 }
 
@@ -316,11 +371,6 @@ __device__ void phase_init(const PeelJob& j) {
         const uint32_t d0 = __ldg(j.deg0 + i);
         for (uint32_t c = 0; c < j.ncols; c++) j.deg[(uint64_t)c * j.nL + i] = d0;
     }
-    __threadfence();
-    // the degree copies are read back by other warps of this same phase only
-    // for their own rows, which each group copies itself below
-    const uint32_t lane = threadIdx.x & 31;
-    (void)lane;
 }
 
 template <int G>
@@ -433,18 +483,21 @@ __device__ void phase_drain(const PeelJob& j) {
                     }
                 }
                 if (ready) outstanding = false;
-                // every lane's enqueues raised `pending` before this point
-                // (ordered by the warp barrier), so the decrement cannot let
-                // it reach zero while their items wait
+                // the items this warp queued were reserved (q_tail raised)
+                // before it counts its own items as processed
                 __syncwarp();
                 if (lane == 0) {
                     __threadfence();
-                    atomicSub(&c->pending, (uint32_t)__popc(rmask));
+                    atomicAdd(&c->processed[q], (uint32_t)__popc(rmask));
                 }
                 t0 = global_ns();
             } else {
-                // nothing ready: done when no queued item is left anywhere
-                if (ld_acquire(&c->pending) == 0) {
+                // nothing ready: the level is done once every reserved item
+                // has been processed.  Both counters only grow, so reading
+                // `processed` first and finding it equal to `q_tail` proves
+                // they were equal at that first read.
+                const uint32_t done_items = ld_acquire(&c->processed[q]);
+                if (done_items == ld_acquire(&c->q_tail[q])) {
                     finished = true;
                     break;
                 }
@@ -528,7 +581,7 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
     const uint64_t qcap = nx + ((uint64_t)ncols * d->entries + CHUNK - 1) / CHUNK + 64;
     if (qcap >= (1ull << 32)) return FC_ERR_TOO_LARGE;
     size_t words = 4 * qcap + (size_t)(ncols * nL) + 3 * nx + 256;
-    FC_TRY(ensure_ws(d, words * 4));
+    FC_TRY(ensure_ws(d, words * 4, s));
     uint32_t* w = (uint32_t*)d->ws;
     PeelJob j;
     j.queue[0] = (unsigned long long*)w;
@@ -554,7 +607,15 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
     j.alive[1] = w; w += nx;
     j.ctl = (PeelCtl*)(((uintptr_t)w + 255) & ~(uintptr_t)255);
     j.max_level = d->max_deg + 1;
-    j.timeout_ns = (uint64_t)env_u32("FC_BARRIER_TIMEOUT_MS", 4000) * 1000000ull;
+    j.timeout_ns = (uint64_t)env_u32("FC_BARRIER_TIMEOUT_MS", 10000) * 1000000ull;
+    j.trace = nullptr;
+    j.trace_levels = 0;
+    const bool tracing = env_u32("FC_PEEL_TRACE", 0) != 0;
+    if (tracing) {
+        j.trace_levels = j.max_level + 2;
+        FC_TRY(dev_alloc((void**)&j.trace, 6ull * 8 * j.trace_levels, s));
+        FC_CUDA_TRY(cudaMemsetAsync(j.trace, 0, 6ull * 8 * j.trace_levels, s));
+    }
     PeelCtl init{};
     init.phase = PH_INIT;
     init.alive_cur = 0;
@@ -590,6 +651,18 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
         st->phase_ms[0] = out.ph_ns[0] * 1e-6;
         st->phase_ms[1] = out.ph_ns[1] * 1e-6;
         st->phase_ms[2] = 0;
+    }
+    if (tracing) {
+        // one line per level: level, scan us, drain us, queue items, alive
+        std::vector<unsigned long long> tr(6ull * j.trace_levels);
+        cudaMemcpy(tr.data(), j.trace, tr.size() * 8, cudaMemcpyDeviceToHost);
+        dev_free(j.trace, s);
+        for (uint32_t l = 0; l < j.trace_levels; l++) {
+            const unsigned long long* r = tr.data() + 6ull * l;
+            if (r[0] || r[3])
+                fprintf(stderr, "peel-trace cols %u+%u level %u scan_us %.1f drain_us %.1f items %llu alive %llu\n",
+                        col0, ncols, l, r[0] * 1e-3, r[3] * 1e-3, r[4] ? r[4] : r[1], r[2]);
+        }
     }
     if (out.err) return FC_ERR_ITER_LIMIT;
     return FC_OK;
