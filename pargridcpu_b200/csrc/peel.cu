@@ -45,13 +45,19 @@ enum : uint32_t { ERR_NONE = 0, ERR_BARRIER = 1, ERR_LIMIT = 2, ERR_QUEUE = 3 };
 constexpr uint32_t UNSET = 0xFFFFFFFFu;
 constexpr unsigned long long EMPTY = ~0ull;
 
+// Work queues, per level parity q and kind s (0: nodes with short rows, one
+// u32 item each; 1: CHUNK-entry pieces of long rows, u64 items x | chunk<<32).
+enum : uint32_t { QS = 0, QC = 1 };
+
 struct PeelCtl {
     uint32_t bar_count, bar_gen, err, phase;
-    uint32_t level, alive_cur, q_cur, prev_tail;
+    uint32_t level, alive_cur, q_cur, pad0;
+    uint32_t prev_tail[2];       // per kind: items the previous level's queues held
     uint32_t alive_cnt[2];
-    uint32_t q_tail[2], q_head[2];
-    uint32_t processed[2];  // queue items fully processed, per queue
-    uint32_t levels, items, pad;
+    uint32_t tail[2][2];         // [q][s] items reserved
+    uint32_t head[2][2];         // [q][s] items claimed
+    uint32_t processed[2][2];    // [q][s] items fully processed
+    uint32_t levels, items, pad1, pad2;
     uint64_t t_last;      // globaltimer at the last barrier
     uint64_t ph_ns[4];    // time per phase kind: scan, drain
 };
@@ -59,6 +65,7 @@ struct PeelCtl {
 // rows longer than SMALL_ROW entries are expanded as CHUNK-entry work items
 constexpr uint32_t SMALL_ROW = 32;
 constexpr uint32_t CHUNK = 128;
+constexpr uint32_t EMPTY32 = 0xFFFFFFFFu;
 
 struct PeelJob {
     uint32_t n, L, col0, ncols;
@@ -71,8 +78,9 @@ struct PeelJob {
     uint32_t* t;                   // table + col0 * n: UNSET while alive, then the core
     uint32_t* cnt;                 // ncols * n
     uint32_t* alive[2];            // each ncols * n
-    unsigned long long* queue[2];  // work items (x | chunk << 32), EMPTY when unwritten
-    uint32_t qcap;
+    uint32_t* qs[2];               // short-row node items, EMPTY32 when unwritten
+    unsigned long long* qc[2];     // chunk items, EMPTY when unwritten
+    uint32_t qs_cap, qc_cap;
     PeelCtl* ctl;
     uint32_t max_level;
     uint64_t timeout_ns;
@@ -116,21 +124,26 @@ __device__ void leader_step(volatile PeelCtl* c, const PeelJob& j) {
         uint64_t now = global_ns();
         uint32_t kind = c->phase == PH_DRAIN ? 1 : 0;
         if (c->t_last) c->ph_ns[kind] += now - c->t_last;
+        const uint32_t q = c->q_cur;
         if (j.trace && c->t_last && c->level < j.trace_levels && c->phase != PH_INIT) {
             unsigned long long* r = j.trace + 3ull * (2ull * c->level + kind);
             r[0] = now - c->t_last;
-            r[1] = c->q_tail[c->q_cur];
+            r[1] = c->tail[q][QS] + c->tail[q][QC];
             r[2] = c->alive_cnt[c->alive_cur ^ (kind == 0 ? 1u : 0u)];
         }
         c->t_last = now;
     }
     auto next_level = [&]() {
-        // the queue of this level is done: the other one becomes current
-        c->prev_tail = c->q_tail[c->q_cur];
-        c->q_cur ^= 1;
-        c->q_tail[c->q_cur] = 0;
-        c->q_head[c->q_cur] = 0;
-        c->processed[c->q_cur] = 0;
+        // the queues of this level are done: the other parity becomes current
+        const uint32_t q = c->q_cur;
+        c->prev_tail[QS] = c->tail[q][QS];
+        c->prev_tail[QC] = c->tail[q][QC];
+        c->q_cur = q ^ 1;
+        for (uint32_t s = 0; s < 2; s++) {
+            c->tail[q ^ 1][s] = 0;
+            c->head[q ^ 1][s] = 0;
+            c->processed[q ^ 1][s] = 0;
+        }
         c->level = c->level + 1;
         c->levels = c->levels + 1;
         c->alive_cnt[c->alive_cur ^ 1] = 0;
@@ -146,12 +159,12 @@ __device__ void leader_step(volatile PeelCtl* c, const PeelJob& j) {
             break;
         case PH_SCAN:  // the first scan wrote alive[1]
             c->alive_cur ^= 1;
-            if (c->q_tail[c->q_cur] > 0) c->phase = PH_DRAIN;
+            if (c->tail[c->q_cur][QS] + c->tail[c->q_cur][QC] > 0) c->phase = PH_DRAIN;
             else if (c->alive_cnt[c->alive_cur] == 0) c->phase = PH_DONE;
             else next_level();
             break;
         case PH_DRAIN:
-            c->items = c->items + c->q_tail[c->q_cur];
+            c->items = c->items + c->tail[c->q_cur][QS] + c->tail[c->q_cur][QC];
             if (c->alive_cnt[c->alive_cur] == 0) c->phase = PH_DONE;
             else next_level();
             break;
@@ -209,20 +222,28 @@ __device__ __forceinline__ uint32_t row_len(const PeelJob& j, uint32_t v) {
     return __ldg(j.node_ptr + v + 1) - __ldg(j.node_ptr + v);
 }
 
-// Work items of a removed x: one for a short row, ceil(len / CHUNK) chunk
-// items for a long one.
-__device__ __forceinline__ uint32_t items_of(const PeelJob& j, uint32_t x) {
+// A removed x is queued as one short item when its row has at most SMALL_ROW
+// entries, else as ceil(len / CHUNK) chunk items; returns the chunk count
+// (0 for a short row).
+__device__ __forceinline__ uint32_t chunks_of(const PeelJob& j, uint32_t x) {
     const uint32_t len = row_len(j, x - j.divN.div(x) * j.n);
-    return len <= SMALL_ROW ? 1u : (len + CHUNK - 1) / CHUNK;
+    return len <= SMALL_ROW ? 0u : (len + CHUNK - 1) / CHUNK;
 }
 
-__device__ __forceinline__ void write_items(const PeelJob& j, uint32_t q, uint32_t first,
-                                            uint32_t x, uint32_t nit) {
-    for (uint32_t c = 0; c < nit; c++) {
+__device__ __forceinline__ void write_short(const PeelJob& j, uint32_t q, uint32_t idx, uint32_t x) {
+    if (idx < j.qs_cap)
+        asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(j.qs[q] + idx), "r"(x) : "memory");
+    else
+        atomicExch(&j.ctl->err, ERR_QUEUE);
+}
+
+__device__ __forceinline__ void write_chunks(const PeelJob& j, uint32_t q, uint32_t first,
+                                             uint32_t x, uint32_t nch) {
+    for (uint32_t c = 0; c < nch; c++) {
         const uint32_t idx = first + c;
-        if (idx < j.qcap) {
+        if (idx < j.qc_cap) {
             const unsigned long long it = (unsigned long long)x | ((unsigned long long)c << 32);
-            asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(j.queue[q] + idx), "l"(it)
+            asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(j.qc[q] + idx), "l"(it)
                          : "memory");
         } else {
             atomicExch(&j.ctl->err, ERR_QUEUE);
@@ -276,30 +297,38 @@ __device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&col)[4
                                          : 0u;
     }
     bool rem[4];
-    uint32_t nit[4], mine = 0;
+    uint32_t nch[4], my_s = 0, my_c = 0;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         const uint32_t lmd = j.col0 + col[i] + 1;
         rem[i] = false;
         if (ok[i] && cy[i] >= lmd && old[i] == k + 1) rem[i] = atomicSub(j.cnt + y[i], 1u) == lmd;
-        nit[i] = 0;
+        nch[i] = 0;
         if (rem[i]) {
             j.t[y[i]] = k;
-            nit[i] = items_of(j, y[i]);
-            mine += nit[i];
+            nch[i] = chunks_of(j, y[i]);
+            my_s += nch[i] == 0;
+            my_c += nch[i];
         }
     }
-    if (!__any_sync(0xffffffffu, mine != 0)) return;
-    const uint32_t incl = warp_incl_scan(mine);
-    uint32_t base = 0;
-    if ((threadIdx.x & 31) == 31) base = atomicAdd(&j.ctl->q_tail[q], incl);
-    base = __shfl_sync(0xffffffffu, base, 31);
-    uint32_t first = base + incl - mine;
+    if (!__any_sync(0xffffffffu, (my_s | my_c) != 0)) return;
+    const uint32_t is = warp_incl_scan(my_s);
+    const uint32_t ic = warp_incl_scan(my_c);
+    uint32_t bs = 0, bc = 0;
+    if ((threadIdx.x & 31) == 31) {
+        if (is) bs = atomicAdd(&j.ctl->tail[q][QS], is);
+        if (ic) bc = atomicAdd(&j.ctl->tail[q][QC], ic);
+    }
+    bs = __shfl_sync(0xffffffffu, bs, 31) + is - my_s;
+    bc = __shfl_sync(0xffffffffu, bc, 31) + ic - my_c;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         if (rem[i]) {
-            write_items(j, q, first, y[i], nit[i]);
-            first += nit[i];
+            if (nch[i] == 0) write_short(j, q, bs++, y[i]);
+            else {
+                write_chunks(j, q, bc, y[i], nch[i]);
+                bc += nch[i];
+            }
         }
     }
 }
@@ -312,9 +341,9 @@ __device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&col)[4
 // Survivors and queue items of a block are reserved with one atomic each per
 // block iteration (the counters are shared by the whole grid).
 template <int G>
-__device__ void scan_nodes(const PeelJob& j, const uint32_t* src, uint32_t cnt_nodes, uint32_t k,
+__device__ __forceinline__ void scan_nodes(const PeelJob& j, const uint32_t* src, uint32_t cnt_nodes, uint32_t k,
                            uint32_t q, uint32_t* out, uint32_t* out_cnt) {
-    __shared__ uint32_t s_keep[32], s_item[32], s_kbase, s_ibase;
+    __shared__ uint32_t s_keep[32], s_short[32], s_chunk[32], s_kbase, s_sbase, s_cbase;
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warp = threadIdx.x >> 5;
     const uint32_t nwarps = blockDim.x >> 5;
@@ -331,40 +360,47 @@ __device__ void scan_nodes(const PeelJob& j, const uint32_t* src, uint32_t cnt_n
         const bool lead = live && (lane & (G - 1)) == 0;
         const bool remove = lead && cnt < j.col0 + c + 1;
         const bool keep = lead && !remove;
-        const uint32_t nit = remove ? items_of(j, x) : 0u;
+        const uint32_t nch = remove ? chunks_of(j, x) : 0u;
+        const uint32_t ns = (remove && nch == 0) ? 1u : 0u;
         if (lead) {
             j.cnt[x] = cnt;
             if (remove) j.t[x] = k;
             else if (!src) j.t[x] = UNSET;
         }
         const uint32_t kin = warp_incl_scan(keep ? 1u : 0u);
-        const uint32_t iin = warp_incl_scan(nit);
+        const uint32_t sin = warp_incl_scan(ns);
+        const uint32_t cin = warp_incl_scan(nch);
         if (lane == 31) {
             s_keep[warp] = kin;
-            s_item[warp] = iin;
+            s_short[warp] = sin;
+            s_chunk[warp] = cin;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            uint32_t kt = 0, it = 0;
+            uint32_t kt = 0, st = 0, ct = 0;
             for (uint32_t w = 0; w < nwarps; w++) {
-                uint32_t a = s_keep[w], b = s_item[w];
+                uint32_t a = s_keep[w], b = s_short[w], d = s_chunk[w];
                 s_keep[w] = kt;
-                s_item[w] = it;
+                s_short[w] = st;
+                s_chunk[w] = ct;
                 kt += a;
-                it += b;
+                st += b;
+                ct += d;
             }
             s_kbase = kt ? atomicAdd(out_cnt, kt) : 0u;
-            s_ibase = it ? atomicAdd(&j.ctl->q_tail[q], it) : 0u;
+            s_sbase = st ? atomicAdd(&j.ctl->tail[q][QS], st) : 0u;
+            s_cbase = ct ? atomicAdd(&j.ctl->tail[q][QC], ct) : 0u;
         }
         __syncthreads();
         if (keep) out[s_kbase + s_keep[warp] + kin - 1] = x;
-        if (remove) write_items(j, q, s_ibase + s_item[warp] + iin - nit, x, nit);
+        if (ns) write_short(j, q, s_sbase + s_short[warp] + sin - 1, x);
+        if (nch) write_chunks(j, q, s_cbase + s_chunk[warp] + cin - nch, x, nch);
         __syncthreads();
     }
 }
 
 template <int G>
-__device__ void phase_init(const PeelJob& j) {
+__device__ __forceinline__ void phase_init(const PeelJob& j) {
     // degree tables: every column starts from the full degrees
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < j.nL; i += stride) {
@@ -374,16 +410,17 @@ __device__ void phase_init(const PeelJob& j) {
 }
 
 template <int G>
-__device__ void phase_scan(const PeelJob& j, bool first) {
+__device__ __forceinline__ void phase_scan(const PeelJob& j, bool first) {
     const PeelCtl* c = j.ctl;
     const uint32_t k = ld_l2(&c->level);
     const uint32_t q = ld_l2(&c->q_cur);
-    const uint32_t prev = ld_l2(&c->prev_tail);
-    // the other queue held the previous level's items: blank them for reuse
-    unsigned long long* other = j.queue[q ^ 1];
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < prev && i < j.qcap;
-         i += gridDim.x * blockDim.x)
-        other[i] = EMPTY;
+    // the other parity's queues held the previous level's items: blank them
+    const uint32_t ps = min(ld_l2(&c->prev_tail[QS]), j.qs_cap);
+    const uint32_t pc = min(ld_l2(&c->prev_tail[QC]), j.qc_cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < ps; i += gridDim.x * blockDim.x)
+        j.qs[q ^ 1][i] = EMPTY32;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pc; i += gridDim.x * blockDim.x)
+        j.qc[q ^ 1][i] = EMPTY;
     if (first) {
         scan_nodes<G>(j, nullptr, j.ncols * j.n, k, q, j.alive[1], &j.ctl->alive_cnt[1]);
     } else {
@@ -393,132 +430,174 @@ __device__ void phase_scan(const PeelJob& j, bool first) {
     }
 }
 
-// DRAIN(K): each warp claims 32 queue slots at a time (one per lane) and
-// processes the items that are ready; it stops once no queued item is left
-// unprocessed.
-__device__ void phase_drain(const PeelJob& j) {
+// The level is complete once every reserved item has been processed.  All
+// four counters only grow, so reading the processed counts first and finding
+// their sum equal to the reserved sum proves the two were equal at the time
+// of the first read.
+__device__ __forceinline__ bool level_done(PeelCtl* c, uint32_t q) {
+    const uint32_t p = ld_acquire(&c->processed[q][QS]) + ld_acquire(&c->processed[q][QC]);
+    const uint32_t t = ld_acquire(&c->tail[q][QS]) + ld_acquire(&c->tail[q][QC]);
+    return p == t;
+}
+
+// Warp-uniform decision while waiting (lane 0 decides): 0 keep waiting, 1 the
+// level is done, 2 an error was recorded or this warp made no progress for
+// the timeout.
+__device__ __forceinline__ uint32_t wait_check(const PeelJob& j, uint32_t q, uint64_t t0) {
+    uint32_t r = 0;
+    if ((threadIdx.x & 31) == 0) {
+        if (level_done(j.ctl, q)) {
+            r = 1;
+        } else if (global_ns() - t0 > j.timeout_ns || ld_l2(&j.ctl->err) != ERR_NONE) {
+            atomicCAS(&j.ctl->err, ERR_NONE, ERR_BARRIER);
+            r = 2;
+        }
+    }
+    return __shfl_sync(0xffffffffu, r, 0);
+}
+
+// Count `n` of this warp's items of kind s as processed.  The items the warp
+// queued while processing them were reserved (tail raised) before this, so
+// the sums of level_done cannot meet early.
+__device__ __forceinline__ void mark_processed(PeelCtl* c, uint32_t q, uint32_t s, uint32_t n) {
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) {
+        __threadfence();
+        atomicAdd(&c->processed[q][s], n);
+    }
+}
+
+// Short rows of the lanes with `ready` set (at most SMALL_ROW entries each),
+// flattened over the warp's lanes; the owner of entry q is found by binary
+// search over the warp's exclusive scan of row lengths.
+__device__ __forceinline__ void expand_short(const PeelJob& j, uint32_t k, uint32_t q, uint32_t x,
+                                             bool ready) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t col = j.divN.div(x);
+    const uint32_t v = x - col * j.n;
+    uint32_t b = 0, len = 0;
+    if (ready) {
+        b = __ldg(j.node_ptr + v);
+        len = __ldg(j.node_ptr + v + 1) - b;
+    }
+    const uint32_t incl = warp_incl_scan(len);
+    const uint32_t excl = incl - len;
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    for (uint32_t jb = 0; jb < total; jb += 128) {
+        uint32_t cols[4], slot[4];
+        bool ok[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const uint32_t qq = jb + 32 * i + lane;
+            uint32_t own = 0;
+#pragma unroll
+            for (int step = 16; step >= 1; step >>= 1) {
+                uint32_t cand = own + step;
+                uint32_t ex = __shfl_sync(0xffffffffu, excl, cand & 31);
+                if (cand < 32 && ex <= qq) own = cand;
+            }
+            const uint32_t ob = __shfl_sync(0xffffffffu, b, own);
+            const uint32_t oe = __shfl_sync(0xffffffffu, excl, own);
+            cols[i] = __shfl_sync(0xffffffffu, col, own);
+            ok[i] = qq < total;
+            slot[i] = ok[i] ? __ldg(j.adj + ob + (qq - oe)) : 0u;
+        }
+        visit4(j, cols, slot, ok, k, q);
+    }
+}
+
+// One CHUNK-entry piece of a long row, by the whole warp.
+__device__ __forceinline__ void expand_chunk(const PeelJob& j, uint32_t k, uint32_t q,
+                                             unsigned long long it) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t x = (uint32_t)it, ch = (uint32_t)(it >> 32);
+    const uint32_t col = j.divN.div(x);
+    const uint32_t v = x - col * j.n;
+    const uint32_t cb = __ldg(j.node_ptr + v) + ch * CHUNK;
+    const uint32_t ce = min(__ldg(j.node_ptr + v + 1), cb + CHUNK);
+    for (uint32_t q0 = cb; q0 < ce; q0 += 128) {
+        uint32_t cols[4], slot[4];
+        bool ok[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const uint32_t p = q0 + lane + 32 * i;
+            ok[i] = p < ce;
+            slot[i] = ok[i] ? __ldg(j.adj + p) : 0u;
+            cols[i] = col;
+        }
+        visit4(j, cols, slot, ok, k, q);
+    }
+}
+
+// DRAIN(K): warps take chunk items one at a time and short-row items 32 at a
+// time (one per lane), preferring chunks, and stop once no queued item is
+// left unprocessed.  A claim may run past the reserved items when warps race
+// for the last ones; such a slot is either filled by a later removal or
+// abandoned when the level completes.
+__device__ __forceinline__ void phase_drain(const PeelJob& j) {
     PeelCtl* c = j.ctl;
     const uint32_t k = ld_l2(&c->level);
     const uint32_t q = ld_l2(&c->q_cur);
-    const unsigned long long* Q = j.queue[q];
     const uint32_t lane = threadIdx.x & 31;
     uint64_t t0 = global_ns();  // last progress of this warp
-    bool finished = false;
-    while (!finished) {
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&c->q_head[q], 32u);
+    uint32_t ns = 32;
+    for (;;) {
+        // claim: 1 = one chunk item, 2 = 32 short items, 0 = nothing available
+        uint32_t kind = 0, base = 0;
+        if (lane == 0) {
+            if (ld_l2(&c->tail[q][QC]) > ld_l2(&c->head[q][QC])) {
+                kind = 1;
+                base = atomicAdd(&c->head[q][QC], 1u);
+            } else if (ld_l2(&c->tail[q][QS]) > ld_l2(&c->head[q][QS])) {
+                kind = 2;
+                base = atomicAdd(&c->head[q][QS], 32u);
+            }
+        }
+        kind = __shfl_sync(0xffffffffu, kind, 0);
         base = __shfl_sync(0xffffffffu, base, 0);
-        const uint32_t idx = base + lane;
-        bool outstanding = true;
-        uint32_t ns = 64;
-        while (__any_sync(0xffffffffu, outstanding)) {
-            unsigned long long it = EMPTY;
-            if (outstanding && idx < j.qcap) it = ld_relaxed64(Q + idx);
-            const bool ready = outstanding && it != EMPTY;
-            const uint32_t rmask = __ballot_sync(0xffffffffu, ready);
-            if (rmask) {
-                ns = 64;
-                const uint32_t x = (uint32_t)it, ch = (uint32_t)(it >> 32);
-                const uint32_t col = j.divN.div(x);
-                const uint32_t v = x - col * j.n;
-                uint32_t b = 0, e = 0;
-                if (ready) {
-                    b = __ldg(j.node_ptr + v);
-                    e = __ldg(j.node_ptr + v + 1);
-                }
-                const bool is_chunk = ready && (e - b) > SMALL_ROW;
-                // short rows of the ready lanes, flattened over the warp
-                const uint32_t len = (ready && !is_chunk) ? e - b : 0u;
-                uint32_t incl = len;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= (uint32_t)o) incl += y;
-                }
-                const uint32_t excl = incl - len;
-                const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-                for (uint32_t jb = 0; jb < total; jb += 128) {
-                    uint32_t cols[4], slot[4];
-                    bool ok[4];
-#pragma unroll
-                    for (int i = 0; i < 4; i++) {
-                        const uint32_t qq = jb + 32 * i + lane;
-                        uint32_t own = 0;
-#pragma unroll
-                        for (int step = 16; step >= 1; step >>= 1) {
-                            uint32_t cand = own + step;
-                            uint32_t ex = __shfl_sync(0xffffffffu, excl, cand & 31);
-                            if (cand < 32 && ex <= qq) own = cand;
-                        }
-                        const uint32_t ob = __shfl_sync(0xffffffffu, b, own);
-                        const uint32_t oe = __shfl_sync(0xffffffffu, excl, own);
-                        cols[i] = __shfl_sync(0xffffffffu, col, own);
-                        ok[i] = qq < total;
-                        slot[i] = ok[i] ? __ldg(j.adj + ob + (qq - oe)) : 0u;
-                    }
-                    visit4(j, cols, slot, ok, k, q);
-                }
-                // chunk items, one at a time across the whole warp
-                uint32_t cm = __ballot_sync(0xffffffffu, is_chunk);
-                while (cm) {
-                    const uint32_t src = __ffs(cm) - 1;
-                    cm &= cm - 1;
-                    const uint32_t sb = __shfl_sync(0xffffffffu, b, src);
-                    const uint32_t se = __shfl_sync(0xffffffffu, e, src);
-                    const uint32_t sc = __shfl_sync(0xffffffffu, col, src);
-                    const uint32_t sch = __shfl_sync(0xffffffffu, ch, src);
-                    const uint32_t cb = sb + sch * CHUNK;
-                    const uint32_t ce = min(se, cb + CHUNK);
-                    for (uint32_t q0 = cb; q0 < ce; q0 += 128) {
-                        uint32_t cols[4], slot[4];
-                        bool ok[4];
-#pragma unroll
-                        for (int i = 0; i < 4; i++) {
-                            const uint32_t p = q0 + lane + 32 * i;
-                            ok[i] = p < ce;
-                            slot[i] = ok[i] ? __ldg(j.adj + p) : 0u;
-                            cols[i] = sc;
-                        }
-                        visit4(j, cols, slot, ok, k, q);
-                    }
-                }
-                if (ready) outstanding = false;
-                // the items this warp queued were reserved (q_tail raised)
-                // before it counts its own items as processed
-                __syncwarp();
-                if (lane == 0) {
-                    __threadfence();
-                    atomicAdd(&c->processed[q], (uint32_t)__popc(rmask));
-                }
-                t0 = global_ns();
-            } else {
-                // nothing ready: the level is done once every reserved item
-                // has been processed.  Both counters only grow, so reading
-                // `processed` first and finding it equal to `q_tail` proves
-                // they were equal at that first read.
-                const uint32_t done_items = ld_acquire(&c->processed[q]);
-                if (done_items == ld_acquire(&c->q_tail[q])) {
-                    finished = true;
-                    break;
-                }
-                __nanosleep(ns);
-                if (ns < 1024) ns <<= 1;
-                if (global_ns() - t0 > j.timeout_ns) {
-                    if (lane == 0) atomicExch(&c->err, ERR_BARRIER);
-                    finished = true;
-                    break;
-                }
-                if (ld_acquire(&c->err) != ERR_NONE) {
-                    finished = true;
-                    break;
+        if (kind == 1) {
+            unsigned long long it;
+            for (;;) {
+                it = EMPTY;
+                if (lane == 0 && base < j.qc_cap) it = ld_relaxed64(j.qc[q] + base);
+                it = __shfl_sync(0xffffffffu, it, 0);
+                if (it != EMPTY) break;
+                if (wait_check(j, q, t0)) return;  // level done (an overclaim) or error
+                __nanosleep(64);
+            }
+            expand_chunk(j, k, q, it);
+            mark_processed(c, q, QC, 1);
+            t0 = global_ns();
+            ns = 32;
+        } else if (kind == 2) {
+            const uint32_t idx = base + lane;
+            bool outstanding = true;
+            while (__any_sync(0xffffffffu, outstanding)) {
+                uint32_t x = EMPTY32;
+                if (outstanding && idx < j.qs_cap) x = __ldcg(j.qs[q] + idx);
+                const bool ready = outstanding && x != EMPTY32;
+                const uint32_t rmask = __ballot_sync(0xffffffffu, ready);
+                if (rmask) {
+                    expand_short(j, k, q, ready ? x : 0u, ready);
+                    if (ready) outstanding = false;
+                    mark_processed(c, q, QS, (uint32_t)__popc(rmask));
+                    t0 = global_ns();
+                } else {
+                    if (wait_check(j, q, t0)) return;  // the rest were overclaims, or error
+                    __nanosleep(64);
                 }
             }
+            ns = 32;
+        } else {
+            if (wait_check(j, q, t0)) return;
+            __nanosleep(ns);
+            if (ns < 256) ns <<= 1;
         }
     }
 }
 
 template <int G>
-__global__ void __launch_bounds__(512) k_peel(PeelJob j) {
+__global__ void __launch_bounds__(512, 2) k_peel(PeelJob j) {
     phase_init<G>(j);
     if (!grid_barrier(j)) return;
     phase_scan<G>(j, true);
@@ -575,20 +654,26 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
     const uint32_t n = d->n, L = d->L;
     const uint64_t nx = (uint64_t)ncols * n;
     const uint64_t nL = (uint64_t)n * L;
-    // workspace: queue0 queue1 (uint64) | deg | cnt alive0 alive1 | ctl.
-    // A level queues each removed node once, long rows as entries/CHUNK + 1
-    // items, so a queue holds at most nx + ncols * entries / CHUNK items.
-    const uint64_t qcap = nx + ((uint64_t)ncols * d->entries + CHUNK - 1) / CHUNK + 64;
-    if (qcap >= (1ull << 32)) return FC_ERR_TOO_LARGE;
-    size_t words = 4 * qcap + (size_t)(ncols * nL) + 3 * nx + 256;
+    // workspace: qc0 qc1 (uint64) | qs0 qs1 | deg | cnt alive0 alive1 | ctl.
+    // A level removes each node at most once: short rows take one qs item,
+    // long rows at most entries/CHUNK + 1 qc items.
+    const uint64_t qs_cap = nx + 64;
+    const uint64_t qc_cap = nx + ((uint64_t)ncols * d->entries + CHUNK - 1) / CHUNK + 64;
+    if (qc_cap >= (1ull << 32) || qs_cap >= (1ull << 32)) return FC_ERR_TOO_LARGE;
+    size_t words = 4 * qc_cap + 2 * qs_cap + (size_t)(ncols * nL) + 3 * nx + 256;
     FC_TRY(ensure_ws(d, words * 4, s));
     uint32_t* w = (uint32_t*)d->ws;
     PeelJob j;
-    j.queue[0] = (unsigned long long*)w;
-    w += 2 * qcap;
-    j.queue[1] = (unsigned long long*)w;
-    w += 2 * qcap;
-    j.qcap = (uint32_t)qcap;
+    j.qc[0] = (unsigned long long*)w;
+    w += 2 * qc_cap;
+    j.qc[1] = (unsigned long long*)w;
+    w += 2 * qc_cap;
+    j.qs[0] = w;
+    w += qs_cap;
+    j.qs[1] = w;
+    w += qs_cap;
+    j.qc_cap = (uint32_t)qc_cap;
+    j.qs_cap = (uint32_t)qs_cap;
     j.n = n;
     j.L = L;
     j.col0 = col0;
@@ -620,7 +705,8 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
     init.phase = PH_INIT;
     init.alive_cur = 0;
     init.q_cur = 0;
-    FC_CUDA_TRY(cudaMemsetAsync(j.queue[0], 0xFF, 2 * qcap * 8, s));
+    // every queue slot starts EMPTY (qc and qs are contiguous)
+    FC_CUDA_TRY(cudaMemsetAsync(j.qc[0], 0xFF, (4 * qc_cap + 2 * qs_cap) * 4, s));
     FC_CUDA_TRY(cudaMemcpyAsync(j.ctl, &init, sizeof(init), cudaMemcpyHostToDevice, s));
     cudaEvent_t e0, e1;
     FC_CUDA_TRY(cudaEventCreate(&e0));
