@@ -529,66 +529,71 @@ __device__ __forceinline__ void expand_chunk(const PeelJob& j, uint32_t k, uint3
     }
 }
 
-// DRAIN(K): warps take chunk items one at a time and short-row items 32 at a
-// time (one per lane), preferring chunks, and stop once no queued item is
-// left unprocessed.  A claim may run past the reserved items when warps race
-// for the last ones; such a slot is either filled by a later removal or
-// abandoned when the level completes.
+// DRAIN(K): each warp holds at most one chunk claim (one item) and one
+// short-row claim (32 slots, one per lane) at a time, polls both, and works
+// on whatever is ready; it stops once no queued item is left unprocessed.  A
+// claim may run past the reserved items when warps race for the last ones;
+// such a slot is either filled by a later removal or abandoned when the level
+// completes -- meanwhile the warp keeps serving the other queue.
 __device__ __forceinline__ void phase_drain(const PeelJob& j) {
     PeelCtl* c = j.ctl;
     const uint32_t k = ld_l2(&c->level);
     const uint32_t q = ld_l2(&c->q_cur);
     const uint32_t lane = threadIdx.x & 31;
+    constexpr uint32_t NONE = 0xFFFFFFFFu;
     uint64_t t0 = global_ns();  // last progress of this warp
     uint32_t ns = 32;
+    uint32_t cidx = NONE;       // held chunk slot (warp-uniform)
+    uint32_t sidx = NONE;       // this lane's held short slot
     for (;;) {
-        // claim: 1 = one chunk item, 2 = 32 short items, 0 = nothing available
-        uint32_t kind = 0, base = 0;
+        bool progress = false;
+        // new claims, decided by lane 0
+        uint32_t want = 0, cb = NONE, sb = NONE;
+        const bool hold_s = __any_sync(0xffffffffu, sidx != NONE);
         if (lane == 0) {
-            if (ld_l2(&c->tail[q][QC]) > ld_l2(&c->head[q][QC])) {
-                kind = 1;
-                base = atomicAdd(&c->head[q][QC], 1u);
-            } else if (ld_l2(&c->tail[q][QS]) > ld_l2(&c->head[q][QS])) {
-                kind = 2;
-                base = atomicAdd(&c->head[q][QS], 32u);
+            if (cidx == NONE && ld_l2(&c->tail[q][QC]) > ld_l2(&c->head[q][QC])) {
+                cb = atomicAdd(&c->head[q][QC], 1u);
+                want |= 1;
+            }
+            if (!hold_s && ld_l2(&c->tail[q][QS]) > ld_l2(&c->head[q][QS])) {
+                sb = atomicAdd(&c->head[q][QS], 32u);
+                want |= 2;
             }
         }
-        kind = __shfl_sync(0xffffffffu, kind, 0);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (kind == 1) {
-            unsigned long long it;
-            for (;;) {
-                it = EMPTY;
-                if (lane == 0 && base < j.qc_cap) it = ld_relaxed64(j.qc[q] + base);
-                it = __shfl_sync(0xffffffffu, it, 0);
-                if (it != EMPTY) break;
-                if (wait_check(j, q, t0)) return;  // level done (an overclaim) or error
-                __nanosleep(64);
+        want = __shfl_sync(0xffffffffu, want, 0);
+        if (want & 1) cidx = __shfl_sync(0xffffffffu, cb, 0);
+        if (want & 2) sidx = __shfl_sync(0xffffffffu, sb, 0) + lane;
+        // a ready chunk item
+        if (cidx != NONE) {
+            unsigned long long it = EMPTY;
+            if (lane == 0 && cidx < j.qc_cap) it = ld_relaxed64(j.qc[q] + cidx);
+            it = __shfl_sync(0xffffffffu, it, 0);
+            if (it != EMPTY) {
+                expand_chunk(j, k, q, it);
+                mark_processed(c, q, QC, 1);
+                cidx = NONE;
+                progress = true;
             }
-            expand_chunk(j, k, q, it);
-            mark_processed(c, q, QC, 1);
+        }
+        // the ready short items among this warp's slots
+        {
+            uint32_t x = EMPTY32;
+            if (sidx != NONE && sidx < j.qs_cap) x = __ldcg(j.qs[q] + sidx);
+            const bool ready = x != EMPTY32;
+            const uint32_t rmask = __ballot_sync(0xffffffffu, ready);
+            if (rmask) {
+                expand_short(j, k, q, ready ? x : 0u, ready);
+                if (ready) sidx = NONE;
+                mark_processed(c, q, QS, (uint32_t)__popc(rmask));
+                progress = true;
+            }
+        }
+        if (progress) {
             t0 = global_ns();
             ns = 32;
-        } else if (kind == 2) {
-            const uint32_t idx = base + lane;
-            bool outstanding = true;
-            while (__any_sync(0xffffffffu, outstanding)) {
-                uint32_t x = EMPTY32;
-                if (outstanding && idx < j.qs_cap) x = __ldcg(j.qs[q] + idx);
-                const bool ready = outstanding && x != EMPTY32;
-                const uint32_t rmask = __ballot_sync(0xffffffffu, ready);
-                if (rmask) {
-                    expand_short(j, k, q, ready ? x : 0u, ready);
-                    if (ready) outstanding = false;
-                    mark_processed(c, q, QS, (uint32_t)__popc(rmask));
-                    t0 = global_ns();
-                } else {
-                    if (wait_check(j, q, t0)) return;  // the rest were overclaims, or error
-                    __nanosleep(64);
-                }
-            }
-            ns = 32;
         } else {
+            // nothing ready: done when every reserved item is processed (any
+            // slots still held were overclaims), else wait a little
             if (wait_check(j, q, t0)) return;
             __nanosleep(ns);
             if (ns < 256) ns <<= 1;
