@@ -49,17 +49,23 @@ constexpr unsigned long long EMPTY = ~0ull;
 // u32 item each; 1: CHUNK-entry pieces of long rows, u64 items x | chunk<<32).
 enum : uint32_t { QS = 0, QC = 1 };
 
+// A counter alone on its 128-byte line: the queue counters are hit by atomics
+// and polls from every SM, and must not share a line with each other.
+struct alignas(128) Hot {
+    uint32_t v;
+};
+
 struct PeelCtl {
     uint32_t bar_count, bar_gen, err, phase;
     uint32_t level, alive_cur, q_cur, pad0;
     uint32_t prev_tail[2];       // per kind: items the previous level's queues held
     uint32_t alive_cnt[2];
-    uint32_t tail[2][2];         // [q][s] items reserved
-    uint32_t head[2][2];         // [q][s] items claimed
-    uint32_t processed[2][2];    // [q][s] items fully processed
     uint32_t levels, items, pad1, pad2;
     uint64_t t_last;      // globaltimer at the last barrier
     uint64_t ph_ns[4];    // time per phase kind: scan, drain
+    Hot tail[2][2];       // [q][s] items reserved
+    Hot head[2][2];       // [q][s] items claimed
+    Hot processed[2][2];  // [q][s] items fully processed
 };
 
 // rows longer than SMALL_ROW entries are expanded as CHUNK-entry work items
@@ -83,6 +89,7 @@ struct PeelJob {
     uint32_t qs_cap, qc_cap;
     PeelCtl* ctl;
     uint32_t max_level;
+    uint32_t idle_polls;  // empty polls after which a non-polling warp leaves DRAIN
     uint64_t timeout_ns;
     // optional per-level trace: [level][scan|drain] = {ns, items, alive}
     unsigned long long* trace;
@@ -128,7 +135,7 @@ __device__ void leader_step(volatile PeelCtl* c, const PeelJob& j) {
         if (j.trace && c->t_last && c->level < j.trace_levels && c->phase != PH_INIT) {
             unsigned long long* r = j.trace + 3ull * (2ull * c->level + kind);
             r[0] = now - c->t_last;
-            r[1] = c->tail[q][QS] + c->tail[q][QC];
+            r[1] = c->tail[q][QS].v + c->tail[q][QC].v;
             r[2] = c->alive_cnt[c->alive_cur ^ (kind == 0 ? 1u : 0u)];
         }
         c->t_last = now;
@@ -136,13 +143,13 @@ __device__ void leader_step(volatile PeelCtl* c, const PeelJob& j) {
     auto next_level = [&]() {
         // the queues of this level are done: the other parity becomes current
         const uint32_t q = c->q_cur;
-        c->prev_tail[QS] = c->tail[q][QS];
-        c->prev_tail[QC] = c->tail[q][QC];
+        c->prev_tail[QS] = c->tail[q][QS].v;
+        c->prev_tail[QC] = c->tail[q][QC].v;
         c->q_cur = q ^ 1;
         for (uint32_t s = 0; s < 2; s++) {
-            c->tail[q ^ 1][s] = 0;
-            c->head[q ^ 1][s] = 0;
-            c->processed[q ^ 1][s] = 0;
+            c->tail[q ^ 1][s].v = 0;
+            c->head[q ^ 1][s].v = 0;
+            c->processed[q ^ 1][s].v = 0;
         }
         c->level = c->level + 1;
         c->levels = c->levels + 1;
@@ -159,12 +166,12 @@ __device__ void leader_step(volatile PeelCtl* c, const PeelJob& j) {
             break;
         case PH_SCAN:  // the first scan wrote alive[1]
             c->alive_cur ^= 1;
-            if (c->tail[c->q_cur][QS] + c->tail[c->q_cur][QC] > 0) c->phase = PH_DRAIN;
+            if (c->tail[c->q_cur][QS].v + c->tail[c->q_cur][QC].v > 0) c->phase = PH_DRAIN;
             else if (c->alive_cnt[c->alive_cur] == 0) c->phase = PH_DONE;
             else next_level();
             break;
         case PH_DRAIN:
-            c->items = c->items + c->tail[c->q_cur][QS] + c->tail[c->q_cur][QC];
+            c->items = c->items + c->tail[c->q_cur][QS].v + c->tail[c->q_cur][QC].v;
             if (c->alive_cnt[c->alive_cur] == 0) c->phase = PH_DONE;
             else next_level();
             break;
@@ -316,8 +323,8 @@ __device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&col)[4
     const uint32_t ic = warp_incl_scan(my_c);
     uint32_t bs = 0, bc = 0;
     if ((threadIdx.x & 31) == 31) {
-        if (is) bs = atomicAdd(&j.ctl->tail[q][QS], is);
-        if (ic) bc = atomicAdd(&j.ctl->tail[q][QC], ic);
+        if (is) bs = atomicAdd(&j.ctl->tail[q][QS].v, is);
+        if (ic) bc = atomicAdd(&j.ctl->tail[q][QC].v, ic);
     }
     bs = __shfl_sync(0xffffffffu, bs, 31) + is - my_s;
     bc = __shfl_sync(0xffffffffu, bc, 31) + ic - my_c;
@@ -388,8 +395,8 @@ __device__ __forceinline__ void scan_nodes(const PeelJob& j, const uint32_t* src
                 ct += d;
             }
             s_kbase = kt ? atomicAdd(out_cnt, kt) : 0u;
-            s_sbase = st ? atomicAdd(&j.ctl->tail[q][QS], st) : 0u;
-            s_cbase = ct ? atomicAdd(&j.ctl->tail[q][QC], ct) : 0u;
+            s_sbase = st ? atomicAdd(&j.ctl->tail[q][QS].v, st) : 0u;
+            s_cbase = ct ? atomicAdd(&j.ctl->tail[q][QC].v, ct) : 0u;
         }
         __syncthreads();
         if (keep) out[s_kbase + s_keep[warp] + kin - 1] = x;
@@ -435,8 +442,8 @@ __device__ __forceinline__ void phase_scan(const PeelJob& j, bool first) {
 // their sum equal to the reserved sum proves the two were equal at the time
 // of the first read.
 __device__ __forceinline__ bool level_done(PeelCtl* c, uint32_t q) {
-    const uint32_t p = ld_acquire(&c->processed[q][QS]) + ld_acquire(&c->processed[q][QC]);
-    const uint32_t t = ld_acquire(&c->tail[q][QS]) + ld_acquire(&c->tail[q][QC]);
+    const uint32_t p = ld_acquire(&c->processed[q][QS].v) + ld_acquire(&c->processed[q][QC].v);
+    const uint32_t t = ld_acquire(&c->tail[q][QS].v) + ld_acquire(&c->tail[q][QC].v);
     return p == t;
 }
 
@@ -463,7 +470,7 @@ __device__ __forceinline__ void mark_processed(PeelCtl* c, uint32_t q, uint32_t 
     __syncwarp();
     if ((threadIdx.x & 31) == 0) {
         __threadfence();
-        atomicAdd(&c->processed[q][s], n);
+        atomicAdd(&c->processed[q][s].v, n);
     }
 }
 
@@ -545,18 +552,19 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j) {
     uint32_t ns = 32;
     uint32_t cidx = NONE;       // held chunk slot (warp-uniform)
     uint32_t sidx = NONE;       // this lane's held short slot
+    uint32_t idle = 0;          // consecutive polls without work
     for (;;) {
         bool progress = false;
         // new claims, decided by lane 0
         uint32_t want = 0, cb = NONE, sb = NONE;
         const bool hold_s = __any_sync(0xffffffffu, sidx != NONE);
         if (lane == 0) {
-            if (cidx == NONE && ld_l2(&c->tail[q][QC]) > ld_l2(&c->head[q][QC])) {
-                cb = atomicAdd(&c->head[q][QC], 1u);
+            if (cidx == NONE && ld_l2(&c->tail[q][QC].v) > ld_l2(&c->head[q][QC].v)) {
+                cb = atomicAdd(&c->head[q][QC].v, 1u);
                 want |= 1;
             }
-            if (!hold_s && ld_l2(&c->tail[q][QS]) > ld_l2(&c->head[q][QS])) {
-                sb = atomicAdd(&c->head[q][QS], 32u);
+            if (!hold_s && ld_l2(&c->tail[q][QS].v) > ld_l2(&c->head[q][QS].v)) {
+                sb = atomicAdd(&c->head[q][QS].v, 32u);
                 want |= 2;
             }
         }
@@ -591,18 +599,28 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j) {
         if (progress) {
             t0 = global_ns();
             ns = 32;
+            idle = 0;
         } else {
             // nothing ready: done when every reserved item is processed (any
-            // slots still held were overclaims), else wait a little
+            // slots still held were overclaims), else wait a little.  Only
+            // warp 0 of a block keeps polling for the whole level; the other
+            // warps, once idle for a while and holding no claim, leave to wait
+            // at the block barrier, so that idle warps do not flood the queue
+            // counters with polls.
             if (wait_check(j, q, t0)) return;
+            if (++idle >= j.idle_polls && (threadIdx.x >> 5) != 0 && cidx == NONE &&
+                !__any_sync(0xffffffffu, sidx != NONE))
+                return;
             __nanosleep(ns);
-            if (ns < 256) ns <<= 1;
+            if (ns < 512) ns <<= 1;
         }
     }
 }
 
-template <int G>
-__global__ void __launch_bounds__(512, 2) k_peel(PeelJob j) {
+// T threads per block; at most 64 registers a thread so that 2048 threads fit
+// an SM (512 x 2 or 1024 x 1).
+template <int G, int T>
+__global__ void __launch_bounds__(T, 2048 / T) k_peel(PeelJob j) {
     phase_init<G>(j);
     if (!grid_barrier(j)) return;
     phase_scan<G>(j, true);
@@ -638,20 +656,26 @@ uint32_t peel_columns_per_group(const DeviceGraph* d) {
     return (uint32_t)cols;
 }
 
-template <int G>
-static fc_status launch(PeelJob& j, cudaStream_t s) {
+template <int G, int T>
+static fc_status launch_t(PeelJob& j, cudaStream_t s) {
     int dev = 0, sms = 0, occ = 0;
     FC_CUDA_TRY(cudaGetDevice(&dev));
     FC_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const int threads = 512;
-    FC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_peel<G>, threads, 0));
+    FC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_peel<G, T>, T, 0));
     if (occ < 1) return FC_ERR_DEVICE;
-    uint32_t want_occ = env_u32("FC_PEEL_BLOCKS_PER_SM", 2);
-    if ((int)want_occ < occ) occ = (int)want_occ;
-    dim3 grid(sms * occ), block(threads);
+    uint32_t want_occ = env_u32("FC_PEEL_BLOCKS_PER_SM", 2048 / T);
+    if (want_occ >= 1 && (int)want_occ < occ) occ = (int)want_occ;
+    dim3 grid(sms * occ), block(T);
     void* args[] = {&j};
-    FC_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_peel<G>, grid, block, args, 0, s));
+    FC_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_peel<G, T>, grid, block, args, 0, s));
     return FC_OK;
+}
+
+template <int G>
+static fc_status launch(PeelJob& j, cudaStream_t s) {
+    // FC_PEEL_THREADS: 512 (default, 2 blocks per SM) or 1024 (1 per SM)
+    if (env_u32("FC_PEEL_THREADS", 512) == 1024) return launch_t<G, 1024>(j, s);
+    return launch_t<G, 512>(j, s);
 }
 
 fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream_t s,
@@ -697,6 +721,7 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
     j.alive[1] = w; w += nx;
     j.ctl = (PeelCtl*)(((uintptr_t)w + 255) & ~(uintptr_t)255);
     j.max_level = d->max_deg + 1;
+    j.idle_polls = env_u32("FC_PEEL_IDLE_POLLS", 8);
     j.timeout_ns = (uint64_t)env_u32("FC_BARRIER_TIMEOUT_MS", 10000) * 1000000ull;
     j.trace = nullptr;
     j.trace_levels = 0;
