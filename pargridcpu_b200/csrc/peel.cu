@@ -617,10 +617,10 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j) {
     }
 }
 
-// T threads per block; at most 64 registers a thread so that 2048 threads fit
-// an SM (512 x 2 or 1024 x 1).
+// T threads per block, 1024 threads resident per SM (512 x 2 or 1024 x 1):
+// at most 64 registers a thread.
 template <int G, int T>
-__global__ void __launch_bounds__(T, 2048 / T) k_peel(PeelJob j) {
+__global__ void __launch_bounds__(T, 1024 / T) k_peel(PeelJob j) {
     phase_init<G>(j);
     if (!grid_barrier(j)) return;
     phase_scan<G>(j, true);
@@ -663,7 +663,7 @@ static fc_status launch_t(PeelJob& j, cudaStream_t s) {
     FC_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     FC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_peel<G, T>, T, 0));
     if (occ < 1) return FC_ERR_DEVICE;
-    uint32_t want_occ = env_u32("FC_PEEL_BLOCKS_PER_SM", 2048 / T);
+    uint32_t want_occ = env_u32("FC_PEEL_BLOCKS_PER_SM", 1024 / T);
     if (want_occ >= 1 && (int)want_occ < occ) occ = (int)want_occ;
     dim3 grid(sms * occ), block(T);
     void* args[] = {&j};
