@@ -689,7 +689,9 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
     const uint64_t qs_cap = nx + 64;
     const uint64_t qc_cap = nx + ((uint64_t)ncols * d->entries + CHUNK - 1) / CHUNK + 64;
     if (qc_cap >= (1ull << 32) || qs_cap >= (1ull << 32)) return FC_ERR_TOO_LARGE;
-    size_t words = 4 * qc_cap + 2 * qs_cap + (size_t)(ncols * nL) + 3 * nx + 256;
+    // + the control block, 256-byte aligned after the lists
+    size_t words = 4 * qc_cap + 2 * qs_cap + (size_t)(ncols * nL) + 3 * nx +
+                   (sizeof(PeelCtl) + 256 + 3) / 4;
     FC_TRY(ensure_ws(d, words * 4, s));
     uint32_t* w = (uint32_t*)d->ws;
     PeelJob j;
@@ -720,6 +722,7 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
     j.alive[0] = w; w += nx;
     j.alive[1] = w; w += nx;
     j.ctl = (PeelCtl*)(((uintptr_t)w + 255) & ~(uintptr_t)255);
+    if ((char*)(j.ctl + 1) > (char*)d->ws + d->ws_bytes) return FC_ERR_INVALID;  // layout check
     j.max_level = d->max_deg + 1;
     j.idle_polls = env_u32("FC_PEEL_IDLE_POLLS", 8);
     j.timeout_ns = (uint64_t)env_u32("FC_BARRIER_TIMEOUT_MS", 10000) * 1000000ull;
