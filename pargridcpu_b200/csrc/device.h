@@ -92,6 +92,22 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
                        PeelStats* st);
 uint32_t peel_columns_per_group(const DeviceGraph* d);
 
+// A device-resident graph in the kernels' layout, whoever owns the memory.
+struct PeelGraph {
+    uint32_t n, L;
+    uint64_t entries;
+    const uint32_t* node_ptr;
+    const uint32_t* adj;
+    const uint32_t* deg0;
+    uint32_t max_level;  // bound on the level count (largest degree + 1, or n + 1)
+};
+// scratch bytes one peel launch over `ncols` columns needs
+uint64_t peel_ws_bytes(uint32_t n, uint32_t L, uint64_t entries, uint32_t ncols);
+// columns [col0, col0 + ncols) of `table` (lambda-major), scratch in `ws`;
+// allocates nothing unless `instrument` (events; a trace when FC_PEEL_TRACE)
+fc_status peel_run(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* table, void* ws,
+                   size_t ws_bytes, cudaStream_t s, PeelStats* st, bool instrument);
+
 // last CUDA error text, for diagnostics
 const char* last_cuda_error();
 

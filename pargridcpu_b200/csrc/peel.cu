@@ -40,7 +40,8 @@ namespace cg = cooperative_groups;
 
 namespace fc {
 
-enum : uint32_t { PH_SCAN = 1, PH_DRAIN = 2, PH_DONE = 3, PH_INIT = 4 };
+// PH_INIT is 0 so that a zeroed control block starts a run
+enum : uint32_t { PH_INIT = 0, PH_SCAN = 1, PH_DRAIN = 2, PH_DONE = 3 };
 enum : uint32_t { ERR_NONE = 0, ERR_BARRIER = 1, ERR_LIMIT = 2, ERR_QUEUE = 3 };
 constexpr uint32_t UNSET = 0xFFFFFFFFu;
 constexpr unsigned long long EMPTY = ~0ull;
@@ -678,22 +679,35 @@ static fc_status launch(PeelJob& j, cudaStream_t s) {
     return launch_t<G, 512>(j, s);
 }
 
-fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream_t s,
-                       PeelStats* st) {
-    const uint32_t n = d->n, L = d->L;
+// Workspace of a group of `ncols` columns: qc0 qc1 (uint64) | qs0 qs1 | deg |
+// cnt alive0 alive1 | control block.  A level removes each node at most once:
+// short rows take one qs item, long rows at most entries/CHUNK + 1 qc items.
+static void peel_caps(uint32_t n, uint32_t L, uint64_t entries, uint32_t ncols, uint64_t* qs_cap,
+                      uint64_t* qc_cap) {
+    const uint64_t nx = (uint64_t)ncols * n;
+    *qs_cap = nx + 64;
+    *qc_cap = nx + ((uint64_t)ncols * entries + CHUNK - 1) / CHUNK + 64;
+    (void)L;
+}
+
+uint64_t peel_ws_bytes(uint32_t n, uint32_t L, uint64_t entries, uint32_t ncols) {
+    uint64_t qs_cap, qc_cap;
+    peel_caps(n, L, entries, ncols, &qs_cap, &qc_cap);
+    const uint64_t nx = (uint64_t)ncols * n;
+    // + the control block, 256-byte aligned after the lists
+    return 4 * (4 * qc_cap + 2 * qs_cap + (uint64_t)ncols * n * L + 3 * nx) + sizeof(PeelCtl) + 256;
+}
+
+fc_status peel_run(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* table, void* ws,
+                   size_t ws_bytes, cudaStream_t s, PeelStats* st, bool instrument) {
+    const uint32_t n = g.n, L = g.L;
     const uint64_t nx = (uint64_t)ncols * n;
     const uint64_t nL = (uint64_t)n * L;
-    // workspace: qc0 qc1 (uint64) | qs0 qs1 | deg | cnt alive0 alive1 | ctl.
-    // A level removes each node at most once: short rows take one qs item,
-    // long rows at most entries/CHUNK + 1 qc items.
-    const uint64_t qs_cap = nx + 64;
-    const uint64_t qc_cap = nx + ((uint64_t)ncols * d->entries + CHUNK - 1) / CHUNK + 64;
+    uint64_t qs_cap, qc_cap;
+    peel_caps(n, L, g.entries, ncols, &qs_cap, &qc_cap);
     if (qc_cap >= (1ull << 32) || qs_cap >= (1ull << 32)) return FC_ERR_TOO_LARGE;
-    // + the control block, 256-byte aligned after the lists
-    size_t words = 4 * qc_cap + 2 * qs_cap + (size_t)(ncols * nL) + 3 * nx +
-                   (sizeof(PeelCtl) + 256 + 3) / 4;
-    FC_TRY(ensure_ws(d, words * 4, s));
-    uint32_t* w = (uint32_t*)d->ws;
+    if (peel_ws_bytes(n, L, g.entries, ncols) > ws_bytes) return FC_ERR_INVALID;
+    uint32_t* w = (uint32_t*)ws;
     PeelJob j;
     j.qc[0] = (unsigned long long*)w;
     w += 2 * qc_cap;
@@ -712,39 +726,38 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
     j.nL = nL;
     j.divL.init(L);
     j.divN.init(n);
-    j.node_ptr = d->node_ptr;
-    j.adj = d->adj;
-    j.deg0 = d->deg0;
+    j.node_ptr = g.node_ptr;
+    j.adj = g.adj;
+    j.deg0 = g.deg0;
     j.deg = w;
     w += ncols * nL;
-    j.t = d->table + (uint64_t)col0 * n;
+    j.t = table + (uint64_t)col0 * n;
     j.cnt = w; w += nx;
     j.alive[0] = w; w += nx;
     j.alive[1] = w; w += nx;
     j.ctl = (PeelCtl*)(((uintptr_t)w + 255) & ~(uintptr_t)255);
-    if ((char*)(j.ctl + 1) > (char*)d->ws + d->ws_bytes) return FC_ERR_INVALID;  // layout check
-    j.max_level = d->max_deg + 1;
+    if ((char*)(j.ctl + 1) > (char*)ws + ws_bytes) return FC_ERR_INVALID;  // layout check
+    j.max_level = g.max_level;
     j.idle_polls = env_u32("FC_PEEL_IDLE_POLLS", 8);
     j.timeout_ns = (uint64_t)env_u32("FC_BARRIER_TIMEOUT_MS", 10000) * 1000000ull;
     j.trace = nullptr;
     j.trace_levels = 0;
-    const bool tracing = env_u32("FC_PEEL_TRACE", 0) != 0;
+    const bool tracing = instrument && env_u32("FC_PEEL_TRACE", 0) != 0;
     if (tracing) {
         j.trace_levels = j.max_level + 2;
         FC_TRY(dev_alloc((void**)&j.trace, 6ull * 8 * j.trace_levels, s));
         FC_CUDA_TRY(cudaMemsetAsync(j.trace, 0, 6ull * 8 * j.trace_levels, s));
     }
-    PeelCtl init{};
-    init.phase = PH_INIT;
-    init.alive_cur = 0;
-    init.q_cur = 0;
-    // every queue slot starts EMPTY (qc and qs are contiguous)
+    // every queue slot starts EMPTY (qc and qs are contiguous); the control
+    // block starts all zero, which is phase INIT
     FC_CUDA_TRY(cudaMemsetAsync(j.qc[0], 0xFF, (4 * qc_cap + 2 * qs_cap) * 4, s));
-    FC_CUDA_TRY(cudaMemcpyAsync(j.ctl, &init, sizeof(init), cudaMemcpyHostToDevice, s));
-    cudaEvent_t e0, e1;
-    FC_CUDA_TRY(cudaEventCreate(&e0));
-    FC_CUDA_TRY(cudaEventCreate(&e1));
-    FC_CUDA_TRY(cudaEventRecord(e0, s));
+    FC_CUDA_TRY(cudaMemsetAsync(j.ctl, 0, sizeof(PeelCtl), s));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (instrument) {
+        FC_CUDA_TRY(cudaEventCreate(&e0));
+        FC_CUDA_TRY(cudaEventCreate(&e1));
+        FC_CUDA_TRY(cudaEventRecord(e0, s));
+    }
     fc_status rc;
     if (L <= 1) rc = launch<1>(j, s);
     else if (L <= 2) rc = launch<2>(j, s);
@@ -754,14 +767,16 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
     else rc = launch<32>(j, s);
     FC_TRY(rc);
     count_launch();
-    FC_CUDA_TRY(cudaEventRecord(e1, s));
-    PeelCtl out{};
+    if (instrument) FC_CUDA_TRY(cudaEventRecord(e1, s));
+    PeelCtl out;
     FC_CUDA_TRY(cudaMemcpyAsync(&out, j.ctl, sizeof(out), cudaMemcpyDeviceToHost, s));
     FC_CUDA_TRY(cudaStreamSynchronize(s));
     float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    if (instrument) {
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
     if (st) {
         st->ms = ms;
         st->levels = out.levels;
@@ -785,6 +800,14 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
     }
     if (out.err) return FC_ERR_ITER_LIMIT;
     return FC_OK;
+}
+
+fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream_t s,
+                       PeelStats* st) {
+    const uint64_t bytes = peel_ws_bytes(d->n, d->L, d->entries, ncols);
+    FC_TRY(ensure_ws(d, bytes, s));
+    PeelGraph g{d->n, d->L, d->entries, d->node_ptr, d->adj, d->deg0, d->max_deg + 1};
+    return peel_run(g, col0, ncols, d->table, d->ws, d->ws_bytes, s, st, true);
 }
 
 }  // namespace fc
