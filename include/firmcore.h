@@ -195,6 +195,27 @@ fc_status fc_server_wait(fc_server* s, uint64_t ticket, int64_t timeout_ms, fc_s
                          double* latency_ms);
 fc_status fc_server_destroy(fc_server* s);
 
+/* ---- core index without device allocation --------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory -- an application whose memory manager has reserved the whole
+ * device, or a latency-bound loop that cannot take the stall a device
+ * allocation may cause -- this computes the same table as fc_coreindex from a
+ * graph already in device memory the caller owns, with its scratch carved
+ * from one fixed 64 MiB device array that every GPU loading the library keeps
+ * until the process exits.  It allocates nothing.
+ *   Inputs (device): node_ptr[n+1] and adj[entries] -- node-major rows, each
+ *   entry the slot u*L + l (neighbour u in layer l), v's layers in order --
+ *   and deg0[n*L] = |N_l(v)| at v*L + l.  Output (device): table[L*n],
+ *   lambda-major.  The call returns when the table is complete.
+ * A graph whose one column needs more than 64 MiB of scratch (about
+ * 4*n*L + 36*n + entries/16 bytes) is rejected with FC_ERR_TOO_LARGE before
+ * any device work.  The first call on a device looks the array up (make it
+ * before any stream capture).  All calls share the array, so calls that
+ * overlap on the GPU race; each call clears the parts that must start empty. */
+fc_status fc_coreindex_fixed_scratch(uint32_t n, uint32_t n_layers, uint64_t entries,
+                                     const uint32_t* node_ptr, const uint32_t* adj,
+                                     const uint32_t* deg0, uint32_t* table, void* stream);
+
 /* ---- diagnostics ---------------------------------------------------------
  * Timings of the last fc_coreindex / fc_densest on a graph, taken with CUDA
  * events recorded around the kernels on the stream they ran on, and the

@@ -27,7 +27,7 @@ EXPORTS = [
     "fc_graph_release_device", "fc_graph_reset_results", "fc_graph_device_bytes", "fc_coreindex",
     "fc_densest", "fc_densest_members", "fc_cells", "fc_batch_run", "fc_server_create",
     "fc_server_submit", "fc_server_wait", "fc_server_destroy", "fc_graph_stats",
-    "fc_launch_count",
+    "fc_launch_count", "fc_coreindex_fixed_scratch",
 ]
 
 
@@ -112,6 +112,7 @@ def lib():
         "fc_server_destroy": ([p], i32),
         "fc_graph_stats": ([p, p], i32),
         "fc_launch_count": ([], u64),
+        "fc_coreindex_fixed_scratch": ([u32, u32, u64, p, p, p, p, p], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
