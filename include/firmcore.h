@@ -156,19 +156,36 @@ fc_status fc_cells(fc_graph* g, double beta, fc_cell* cells, uint32_t cap, uint3
 
 /* ---- batch ---------------------------------------------------------------
  * Many graphs at once: all (graph, lambda) columns in one persistent kernel
- * launch that pulls work items from a device queue, captured in a CUDA graph,
- * plus the densest search for `beta` on every graph.  tables[i] (host, may be
- * NULL) receives graph i's L*n table, res[i] (may be NULL) its densest result.
- * The equivalent of running the reference once per graph. */
+ * launch whose warps pull work items from device queues (captured in a CUDA
+ * graph when use_cuda_graph is set), then the densest search for `beta` on
+ * every graph.  tables[i] (host, may be NULL) receives graph i's L*n table,
+ * res[i] (may be NULL) its densest result.  The equivalent of running the
+ * reference once per graph; every result is identical to fc_coreindex +
+ * fc_densest on the graph alone.  With `plain` set it runs the baseline
+ * instead: one graph and one lambda column per launch, one after another. */
 typedef struct fc_batch_options {
-    uint32_t block_threads;    /* 0 = autotuned */
-    uint32_t hub_threshold;    /* adjacency length above which a node is split; 0 = autotuned */
-    int use_cuda_graph;        /* capture the launch sequence in a CUDA graph (default 1) */
+    uint32_t block_threads;    /* 512 or 1024 threads per block; 0 = autotuned */
+    uint32_t hub_threshold;    /* longest row queued as one work item (longer rows are
+                                  split in 128-entry pieces); 0 = autotuned */
+    int use_cuda_graph;        /* capture the batched launch in a CUDA graph */
+    int plain;                 /* 1 = the one-column-per-launch baseline */
 } fc_batch_options;
+
+/* What a batch run did (any pointer field may be ignored). */
+typedef struct fc_batch_report {
+    double peel_ms;            /* device time of the peel launch(es), CUDA events */
+    double densest_ms;         /* device time of the densest searches */
+    uint32_t peel_launches;
+    uint32_t block_threads;    /* the configuration used */
+    uint32_t hub_threshold;
+    uint32_t levels;
+    int used_cuda_graph;
+    int autotuned;             /* 1 when this call measured the candidates */
+} fc_batch_report;
 
 fc_status fc_batch_run(fc_graph* const* graphs, uint32_t count, double beta,
                        uint32_t* const* tables, fc_densest_result* res,
-                       const fc_batch_options* opt, void* stream);
+                       const fc_batch_options* opt, fc_batch_report* report, void* stream);
 
 /* ---- serving -------------------------------------------------------------
  * A continuous-batching request loop: requests (a graph + beta) are admitted

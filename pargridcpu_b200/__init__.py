@@ -233,20 +233,22 @@ def launch_count():
 
 
 def batch_run(graphs, beta=1.0, want_tables=True, block_threads=0, hub_threshold=0,
-              use_cuda_graph=True, stream=None):
+              use_cuda_graph=True, plain=False, stream=None):
     """Every (graph, lambda) column of many graphs in one batched launch plus
-    the densest search; returns (tables, results)."""
+    the densest search (``plain=True``: the one-column-per-launch baseline);
+    returns (tables, results, report)."""
     cnt = len(graphs)
     hs = (C.c_void_p * max(cnt, 1))(*[g.handle.value for g in graphs])
     tables = [np.zeros((g.L, g.n), np.uint32) for g in graphs] if want_tables else None
     tp = (C.c_void_p * max(cnt, 1))(*[t.ctypes.data for t in tables]) if want_tables else None
     res = (_n.DensestResult * max(cnt, 1))()
-    opt = _n.BatchOptions(block_threads, hub_threshold, int(use_cuda_graph))
+    opt = _n.BatchOptions(block_threads, hub_threshold, int(use_cuda_graph), int(plain))
+    rep = _n.BatchReport()
     _n.check(_n.lib().fc_batch_run(C.cast(hs, C.c_void_p), cnt, float(beta),
                                    C.cast(tp, C.c_void_p) if tp is not None else None,
-                                   C.cast(res, C.c_void_p), C.byref(opt),
+                                   C.cast(res, C.c_void_p), C.byref(opt), C.byref(rep),
                                    _n.stream_handle(stream)), "batch_run")
-    return tables, [r.as_dict() for r in res[:cnt]]
+    return tables, [r.as_dict() for r in res[:cnt]], rep.as_dict()
 
 
 class Server:

@@ -221,9 +221,11 @@ uint64_t fc_launch_count(void) { return g_launches.load(std::memory_order_relaxe
 
 fc_status fc_batch_run(fc_graph* const* graphs, uint32_t count, double beta,
                        uint32_t* const* tables, fc_densest_result* res,
-                       const fc_batch_options* opt, void* stream) {
+                       const fc_batch_options* opt, fc_batch_report* report, void* stream) {
     if (count && !graphs) return FC_ERR_INVALID;
-    return batch_run(graphs, count, beta, tables, res, opt, (cudaStream_t)stream);
+    for (uint32_t i = 0; i < count; i++)
+        if (!graphs[i]) return FC_ERR_INVALID;
+    return batch_run(graphs, count, beta, tables, res, opt, report, (cudaStream_t)stream);
 }
 
 }  // extern "C"

@@ -1,33 +1,253 @@
-// Batched decomposition of many graphs.
+// Batched decomposition of many graphs (fc_batch_run).
+//
+// Batched form: every graph is one segment of a single persistent peel launch
+// (all its lambda columns; graphs whose scratch would not fit one launch are
+// spread over a few launches), optionally captured in a CUDA graph; then the
+// densest search per graph.  The block size and the hub threshold (longest
+// row queued as one work item) are chosen by an autotuner that times the
+// candidates on a sample of the batch and remembers the winner per batch
+// shape.  Results do not depend on either, so tuning never changes an output.
+//
+// Plain form (the baseline): one graph after another, one lambda column per
+// launch -- "a single launch per lambda".
+#include <algorithm>
+#include <chrono>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
 #include "device.h"
 
 namespace fc {
 
-// One graph after another through the single-graph path (plain launches):
-// the baseline the persistent batched kernel is measured against.
-static fc_status batch_plain(fc_graph* const* gs, uint32_t count, double beta,
-                             uint32_t* const* tables, fc_densest_result* res, cudaStream_t s) {
+static uint32_t env_u32b(const char* name, uint32_t dflt) {
+    const char* s = getenv(name);
+    return s && *s ? (uint32_t)strtoul(s, nullptr, 10) : dflt;
+}
+
+static fc_status densest_all(fc_graph* const* gs, uint32_t count, double beta,
+                             fc_densest_result* res, cudaStream_t s, double* ms) {
+    *ms = 0;
     for (uint32_t i = 0; i < count; i++) {
         fc_graph* g = gs[i];
-        if (!g) return FC_ERR_INVALID;
-        FC_TRY(coreindex(g, tables ? tables[i] : nullptr, false, s));
-        if (res) {
-            if (g->n && g->L) {
-                FC_TRY(densest(g, &beta, 1, res + i, s));
-            } else {
-                res[i] = fc_densest_result{};
-                res[i].beta = beta;
-            }
+        if (!res) continue;
+        if (g->n && g->L) {
+            FC_TRY(densest(g, &beta, 1, res + i, s));
+            *ms += g->dev->stats.densest_ms;
+        } else {
+            res[i] = fc_densest_result{};
+            res[i].beta = beta;
         }
     }
     return FC_OK;
 }
 
+static fc_status copy_tables(fc_graph* const* gs, uint32_t count, uint32_t* const* tables,
+                             cudaStream_t s) {
+    if (!tables) return FC_OK;
+    for (uint32_t i = 0; i < count; i++) {
+        fc_graph* g = gs[i];
+        const uint64_t bytes = (uint64_t)g->n * g->L * 4;
+        if (tables[i] && bytes)
+            FC_CUDA_TRY(cudaMemcpyAsync(tables[i], g->dev->table, bytes, cudaMemcpyDeviceToHost, s));
+    }
+    FC_CUDA_TRY(cudaStreamSynchronize(s));
+    return FC_OK;
+}
+
+// ---- plain: one lambda column per launch -------------------------------------
+
+static fc_status batch_plain(fc_graph* const* gs, uint32_t count, double beta,
+                             uint32_t* const* tables, fc_densest_result* res,
+                             fc_batch_report* rep, cudaStream_t s) {
+    double peel_ms = 0;
+    uint32_t launches = 0, levels = 0;
+    for (uint32_t i = 0; i < count; i++) {
+        fc_graph* g = gs[i];
+        FC_TRY(upload(g, s));
+        DeviceGraph* d = g->dev;
+        d->home = s;
+        invalidate_densest(d);
+        for (uint32_t c = 0; c < d->L && d->n; c++) {
+            PeelStats st;
+            FC_TRY(peel_columns(d, c, 1, s, &st));
+            peel_ms += st.ms;
+            launches++;
+            levels += st.levels;
+        }
+        d->table_valid = true;
+    }
+    double dms = 0;
+    FC_TRY(densest_all(gs, count, beta, res, s, &dms));
+    FC_TRY(copy_tables(gs, count, tables, s));
+    if (rep) {
+        rep->peel_ms = peel_ms;
+        rep->densest_ms = dms;
+        rep->peel_launches = launches;
+        rep->levels = levels;
+        rep->used_cuda_graph = 0;
+    }
+    return FC_OK;
+}
+
+// ---- batched: segments in persistent launches --------------------------------
+
+struct TuneKey {
+    uint32_t count, maxL;
+    uint64_t entries_mb;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(count, maxL, entries_mb) < std::tie(o.count, o.maxL, o.entries_mb);
+    }
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, std::pair<uint32_t, uint32_t>> g_tuned;  // -> (threads, small_row)
+
+// Launch groups: consecutive graphs whose peel scratch stays within the
+// budget (FC_BATCH_WS_MB, default 32 GiB) share one launch.
+static void plan_groups(const std::vector<PeelSegSpec>& specs, uint64_t budget,
+                        std::vector<std::pair<size_t, size_t>>* groups) {
+    size_t i = 0;
+    while (i < specs.size()) {
+        size_t e = i + 1;
+        while (e < specs.size()) {
+            std::vector<PeelSegSpec> trial(specs.begin() + i, specs.begin() + e + 1);
+            if (peel_batch_ws_bytes(trial) > budget) break;
+            e++;
+        }
+        groups->push_back({i, e});
+        i = e;
+    }
+}
+
+static fc_status run_groups(const std::vector<PeelSegSpec>& specs,
+                            const std::vector<std::pair<size_t, size_t>>& groups, void* ws,
+                            uint64_t ws_bytes, cudaStream_t s, uint32_t threads, uint32_t small_row,
+                            bool want_graph, double* ms, uint32_t* levels, bool* graphed) {
+    *ms = 0;
+    *levels = 0;
+    *graphed = want_graph;
+    for (const auto& gr : groups) {
+        std::vector<PeelSegSpec> part(specs.begin() + gr.first, specs.begin() + gr.second);
+        PeelStats st;
+        bool g = want_graph;
+        FC_TRY(peel_batch(part, ws, ws_bytes, s, &st, threads, small_row, &g));
+        *graphed = *graphed && g;
+        *ms += st.ms;
+        *levels += st.levels;
+    }
+    return FC_OK;
+}
+
+static fc_status batch_persistent(fc_graph* const* gs, uint32_t count, double beta,
+                                  uint32_t* const* tables, fc_densest_result* res,
+                                  const fc_batch_options* opt, fc_batch_report* rep,
+                                  cudaStream_t s) {
+    std::vector<PeelSegSpec> specs;
+    uint32_t maxL = 1;
+    uint64_t entries = 0;
+    for (uint32_t i = 0; i < count; i++) {
+        fc_graph* g = gs[i];
+        FC_TRY(upload(g, s));
+        DeviceGraph* d = g->dev;
+        d->home = s;
+        invalidate_densest(d);
+        if (d->n && d->L) {
+            PeelSegSpec sp;
+            sp.g = PeelGraph{d->n, d->L, d->entries, d->node_ptr, d->adj, d->deg0, d->max_deg + 1};
+            sp.col0 = 0;
+            sp.ncols = d->L;
+            sp.table = d->table;
+            specs.push_back(sp);
+            maxL = std::max(maxL, d->L);
+            entries += (uint64_t)d->entries * d->L;
+        }
+    }
+    const uint64_t budget = (uint64_t)env_u32b("FC_BATCH_WS_MB", 32768) << 20;
+    std::vector<std::pair<size_t, size_t>> groups;
+    plan_groups(specs, budget, &groups);
+    uint64_t ws_bytes = 0;
+    for (const auto& gr : groups) {
+        std::vector<PeelSegSpec> part(specs.begin() + gr.first, specs.begin() + gr.second);
+        ws_bytes = std::max(ws_bytes, peel_batch_ws_bytes(part));
+    }
+    void* ws = nullptr;
+    if (!specs.empty()) FC_TRY(dev_alloc(&ws, ws_bytes, s));
+    const bool want_graph = opt ? opt->use_cuda_graph != 0 : true;
+    uint32_t threads = opt ? opt->block_threads : 0;
+    uint32_t small_row = opt ? opt->hub_threshold : 0;
+    bool tuned_now = false;
+    fc_status rc = FC_OK;
+    if (!specs.empty() && (!threads || !small_row)) {
+        TuneKey key{count, maxL, entries >> 20};
+        std::pair<uint32_t, uint32_t> best{0, 0};
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            auto it = g_tuned.find(key);
+            if (it != g_tuned.end()) best = it->second;
+        }
+        if (!best.first) {
+            // candidates timed on a sample: every k-th graph, up to 32 of them
+            std::vector<PeelSegSpec> sample;
+            const size_t step = std::max<size_t>(1, specs.size() / 32);
+            for (size_t i = 0; i < specs.size(); i += step) sample.push_back(specs[i]);
+            std::vector<std::pair<size_t, size_t>> sg;
+            plan_groups(sample, ws_bytes, &sg);
+            double best_ms = 1e300;
+            for (uint32_t th : {512u, 1024u})
+                for (uint32_t sr : {16u, 32u, 64u}) {
+                    double ms;
+                    uint32_t lv;
+                    bool gr;
+                    rc = run_groups(sample, sg, ws, ws_bytes, s, th, sr, false, &ms, &lv, &gr);
+                    if (rc != FC_OK) break;
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        best = {th, sr};
+                    }
+                }
+            if (rc == FC_OK) {
+                std::lock_guard<std::mutex> lk(g_tune_mu);
+                g_tuned[key] = best;
+                tuned_now = true;
+            }
+        }
+        if (!threads) threads = best.first;
+        if (!small_row) small_row = best.second;
+    }
+    double peel_ms = 0;
+    uint32_t levels = 0;
+    bool graphed = false;
+    if (rc == FC_OK && !specs.empty())
+        rc = run_groups(specs, groups, ws, ws_bytes, s, threads, small_row, want_graph, &peel_ms,
+                        &levels, &graphed);
+    if (ws) dev_free(ws, s);
+    FC_TRY(rc);
+    for (uint32_t i = 0; i < count; i++) gs[i]->dev->table_valid = true;
+    double dms = 0;
+    FC_TRY(densest_all(gs, count, beta, res, s, &dms));
+    FC_TRY(copy_tables(gs, count, tables, s));
+    if (rep) {
+        rep->peel_ms = peel_ms;
+        rep->densest_ms = dms;
+        rep->peel_launches = (uint32_t)groups.size();
+        rep->block_threads = threads;
+        rep->hub_threshold = small_row;
+        rep->levels = levels;
+        rep->used_cuda_graph = graphed ? 1 : 0;
+        rep->autotuned = tuned_now ? 1 : 0;
+    }
+    return FC_OK;
+}
+
 fc_status batch_run(fc_graph* const* gs, uint32_t count, double beta, uint32_t* const* tables,
-                    fc_densest_result* res, const fc_batch_options* opt, cudaStream_t s) {
-    (void)opt;
+                    fc_densest_result* res, const fc_batch_options* opt, fc_batch_report* rep,
+                    cudaStream_t s) {
     if (!cuda_available()) return FC_ERR_NO_DEVICE;
-    return batch_plain(gs, count, beta, tables, res, s);
+    if (rep) *rep = fc_batch_report{};
+    if (opt && opt->plain) return batch_plain(gs, count, beta, tables, res, rep, s);
+    return batch_persistent(gs, count, beta, tables, res, opt, rep, s);
 }
 
 }  // namespace fc

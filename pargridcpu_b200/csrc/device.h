@@ -108,6 +108,21 @@ uint64_t peel_ws_bytes(uint32_t n, uint32_t L, uint64_t entries, uint32_t ncols)
 fc_status peel_run(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* table, void* ws,
                    size_t ws_bytes, cudaStream_t s, PeelStats* st, bool instrument);
 
+// One segment of a batched launch: columns [col0, col0 + ncols) of graph g,
+// written to table (lambda-major, L*n).
+struct PeelSegSpec {
+    PeelGraph g;
+    uint32_t col0, ncols;
+    uint32_t* table;
+};
+uint64_t peel_batch_ws_bytes(const std::vector<PeelSegSpec>& specs);
+// All segments in one persistent launch (threads per block and the longest row
+// queued as one item: 0 = defaults).  With *use_graph set the launch is
+// captured in a CUDA graph; on return *use_graph says whether it was.
+fc_status peel_batch(const std::vector<PeelSegSpec>& specs, void* ws, size_t ws_bytes,
+                     cudaStream_t s, PeelStats* st, uint32_t threads, uint32_t small_row,
+                     bool* use_graph);
+
 // last CUDA error text, for diagnostics
 const char* last_cuda_error();
 

@@ -1,35 +1,39 @@
-// The fcgrid peel: core_lambda(v) for a group of lambda columns of one graph,
-// in one persistent cooperative kernel with the level loop inside.
+// The fcgrid peel: core_lambda(v) for groups of lambda columns of one or many
+// graphs, in one persistent cooperative kernel with the level loop inside.
 //
-// x = (column c, node v) ranges over the group's columns, lambda = col0+c+1.
-// All columns advance together, level by level, K = 0, 1, 2, ...:
+// A launch covers segments; a segment is one graph's group of columns (lambda
+// = col0+c+1 for c < ncols).  Segments are laid end to end in one index space
+// x, so one launch peels many graphs at once and they share the level loop.
+// Edges never cross graphs: a queued node resolves its segment once and all
+// its visits stay inside it.  All columns advance together, level by level,
+// K = 0, 1, 2, ...:
 //
 //   SCAN(K)   every alive x counts its layers with degree >= K+1 inside the
 //             alive set, cnt[x].  cnt < lambda means Top-lambda(x) <= K: x is
 //             removed at level K (core = K).  The others keep cnt.
-//   DRAIN(K)  removed nodes are expanded from a device work queue: each
+//   DRAIN(K)  removed nodes are expanded from device work queues: each
 //             adjacency slot (u,l) of a removed x decrements deg[u][l] of an
 //             alive u; a decrement from exactly K+1 to K lowers cnt[u], and the
 //             decrement that takes cnt[u] from lambda to lambda-1 removes u at
 //             level K too -- ParGrid's own trigger (CoreParallel/
 //             FCSyncLeft.cpp:99-103).  Each of those crossings happens exactly
 //             once, so every node is queued once.  Removals cascade through
-//             the queue without any barrier; the level ends when no queued item
-//             is left unprocessed (the processed-items count reaches the
+//             the queues without any barrier; the level ends when no queued
+//             item is left unprocessed (the processed-items count reaches the
 //             reserved-items count).
 //
 // This computes the same table as the reference's get_index2 bucket peel
 // (CoreIndexParallel/CoreIndex.cpp:62-109) and ParGrid's per-cell PeelSync:
 // core_lambda is the unique fixpoint, whatever the removal order.
 //
-// Long rows (more than SMALL_ROW entries) are queued as CHUNK-entry items so
-// that hubs spread over many warps.  SCAN and DRAIN are separated by a grid
+// Long rows (more than `small_row` entries, 32 by default; the batch
+// autotuner picks it) are queued as CHUNK-entry items so that hubs spread over
+// many warps.  SCAN and DRAIN are separated by a grid
 // barrier whose last arriving block runs the serial "leader" step (level
 // change, counter resets).  Every wait -- barrier or queue -- is bounded by a
 // timeout after which the kernel records an error and winds down; the level
 // count is bounded by the largest degree.
 #include <cooperative_groups.h>
-#include <cooperative_groups/scan.h>
 
 #include <cstdio>
 #include <cstdlib>
@@ -45,10 +49,16 @@ enum : uint32_t { PH_INIT = 0, PH_SCAN = 1, PH_DRAIN = 2, PH_DONE = 3 };
 enum : uint32_t { ERR_NONE = 0, ERR_BARRIER = 1, ERR_LIMIT = 2, ERR_QUEUE = 3 };
 constexpr uint32_t UNSET = 0xFFFFFFFFu;
 constexpr unsigned long long EMPTY = ~0ull;
+constexpr uint32_t EMPTY32 = 0xFFFFFFFFu;
 
 // Work queues, per level parity q and kind s (0: nodes with short rows, one
 // u32 item each; 1: CHUNK-entry pieces of long rows, u64 items x | chunk<<32).
 enum : uint32_t { QS = 0, QC = 1 };
+
+// rows longer than the job's small_row entries are expanded as CHUNK-entry
+// work items
+constexpr uint32_t SMALL_ROW_DEFAULT = 32;
+constexpr uint32_t CHUNK = 128;
 
 // A counter alone on its 128-byte line: the queue counters are hit by atomics
 // and polls from every SM, and must not share a line with each other.
@@ -69,28 +79,34 @@ struct PeelCtl {
     Hot processed[2][2];  // [q][s] items fully processed
 };
 
-// rows longer than SMALL_ROW entries are expanded as CHUNK-entry work items
-constexpr uint32_t SMALL_ROW = 32;
-constexpr uint32_t CHUNK = 128;
-constexpr uint32_t EMPTY32 = 0xFFFFFFFFu;
-
-struct PeelJob {
-    uint32_t n, L, col0, ncols;
-    uint64_t nL;  // n * L
+// One segment: a graph's group of columns, as the kernel reads it.
+struct SegP {
+    uint32_t xbase;            // first x of the segment
+    uint32_t n, L, col0;
     FastDiv divL, divN;
+    uint64_t nL;               // n * L
     const uint32_t* node_ptr;
     const uint32_t* adj;
     const uint32_t* deg0;
-    uint32_t* deg;                 // ncols * n * L, degrees inside the alive set
-    uint32_t* t;                   // table + col0 * n: UNSET while alive, then the core
-    uint32_t* cnt;                 // ncols * n
-    uint32_t* alive[2];            // each ncols * n
+    uint32_t* deg;             // ncols * n * L, degrees inside the alive set
+    uint32_t* t;               // table + col0 * n: UNSET while alive, then the core
+    uint32_t ncols, pad;
+};
+
+struct PeelJob {
+    SegP seg0;                     // the only segment when the launch has one
+    const SegP* segs;              // nseg segments (device), when more than one
+    const uint32_t* seg_xbase;     // nseg + 1 (device): segment starts, then nx
+    uint32_t nseg, nx;
+    uint32_t* cnt;                 // nx
+    uint32_t* alive[2];            // each nx
     uint32_t* qs[2];               // short-row node items, EMPTY32 when unwritten
     unsigned long long* qc[2];     // chunk items, EMPTY when unwritten
     uint32_t qs_cap, qc_cap;
     PeelCtl* ctl;
     uint32_t max_level;
     uint32_t idle_polls;  // empty polls after which a non-polling warp leaves DRAIN
+    uint32_t small_row;   // longest row queued as one item; longer rows go in chunks
     uint64_t timeout_ns;
     // optional per-level trace: [level][scan|drain] = {ns, items, alive}
     unsigned long long* trace;
@@ -124,6 +140,47 @@ __device__ __forceinline__ uint64_t global_ns() {
 }
 // data written by other SMs during the kernel is read through L2 only
 __device__ __forceinline__ uint32_t ld_l2(const uint32_t* p) { return __ldcg(p); }
+
+// ---- segments ---------------------------------------------------------------
+
+template <bool MULTI>
+__device__ __forceinline__ uint32_t seg_of(const PeelJob& j, uint32_t x) {
+    if (!MULTI) return 0;
+    uint32_t lo = 0, hi = j.nseg;  // seg_xbase[lo] <= x < seg_xbase[hi]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(j.seg_xbase + mid) <= x) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <bool MULTI>
+__device__ __forceinline__ SegP seg_load(const PeelJob& j, uint32_t s) {
+    if (!MULTI) return j.seg0;
+    SegP g;
+    const SegP* p = j.segs + s;
+    g.xbase = __ldg(&p->xbase);
+    g.n = __ldg(&p->n);
+    g.L = __ldg(&p->L);
+    g.col0 = __ldg(&p->col0);
+    g.divL.d = __ldg(&p->divL.d);
+    g.divL.m = __ldg(&p->divL.m);
+    g.divL.s1 = __ldg(&p->divL.s1);
+    g.divL.s2 = __ldg(&p->divL.s2);
+    g.divN.d = __ldg(&p->divN.d);
+    g.divN.m = __ldg(&p->divN.m);
+    g.divN.s1 = __ldg(&p->divN.s1);
+    g.divN.s2 = __ldg(&p->divN.s2);
+    g.nL = __ldg((const unsigned long long*)&p->nL);
+    g.node_ptr = (const uint32_t*)__ldg((const unsigned long long*)&p->node_ptr);
+    g.adj = (const uint32_t*)__ldg((const unsigned long long*)&p->adj);
+    g.deg0 = (const uint32_t*)__ldg((const unsigned long long*)&p->deg0);
+    g.deg = (uint32_t*)__ldg((const unsigned long long*)&p->deg);
+    g.t = (uint32_t*)__ldg((const unsigned long long*)&p->t);
+    g.ncols = __ldg(&p->ncols);
+    return g;
+}
 
 // ---- leader step: phase transitions (one thread, all blocks parked) -------
 
@@ -215,27 +272,14 @@ __device__ bool grid_barrier(const PeelJob& j) {
     return ld_acquire(&c->err) == ERR_NONE;
 }
 
-// ---- warp helpers -----------------------------------------------------------
+// ---- queues -----------------------------------------------------------------
 
-// Append `val` to list/counter from the lanes that call it together.
-__device__ __forceinline__ void push(uint32_t* list, uint32_t* cnt, uint32_t val) {
-    cg::coalesced_group g = cg::coalesced_threads();
-    uint32_t base = 0;
-    if (g.thread_rank() == 0) base = atomicAdd(cnt, g.size());
-    base = g.shfl(base, 0);
-    list[base + g.thread_rank()] = val;
-}
-
-__device__ __forceinline__ uint32_t row_len(const PeelJob& j, uint32_t v) {
-    return __ldg(j.node_ptr + v + 1) - __ldg(j.node_ptr + v);
-}
-
-// A removed x is queued as one short item when its row has at most SMALL_ROW
-// entries, else as ceil(len / CHUNK) chunk items; returns the chunk count
-// (0 for a short row).
-__device__ __forceinline__ uint32_t chunks_of(const PeelJob& j, uint32_t x) {
-    const uint32_t len = row_len(j, x - j.divN.div(x) * j.n);
-    return len <= SMALL_ROW ? 0u : (len + CHUNK - 1) / CHUNK;
+// A removed node is queued as one short item when its row has at most
+// small_row entries, else as ceil(len / CHUNK) chunk items; returns the chunk
+// count (0 for a short row).
+__device__ __forceinline__ uint32_t chunks_of(const SegP& g, uint32_t v, uint32_t small_row) {
+    const uint32_t len = __ldg(g.node_ptr + v + 1) - __ldg(g.node_ptr + v);
+    return len <= small_row ? 0u : (len + CHUNK - 1) / CHUNK;
 }
 
 __device__ __forceinline__ void write_short(const PeelJob& j, uint32_t q, uint32_t idx, uint32_t x) {
@@ -271,8 +315,8 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v) {
 }
 
 // Count of the L values row[0..L) that are >= thr, by a group of G lanes (G a
-// power of two; all 32 lanes of the warp call this together).  Every lane of
-// a group returns the group's count.
+// power of two; all 32 lanes of the warp call this together, each group with
+// its own row and L).  Every lane of a group returns the group's count.
 template <int G>
 __device__ __forceinline__ uint32_t group_count_ge(const uint32_t* row, uint32_t L, uint32_t thr,
                                                    bool live) {
@@ -285,36 +329,44 @@ __device__ __forceinline__ uint32_t group_count_ge(const uint32_t* row, uint32_t
     return cnt;
 }
 
-// One removed-neighbour slot per entry, up to four per lane at once (loads
-// first, then the atomics) so each lane keeps several memory operations in
-// flight.  All 32 lanes call it together; the nodes it removes are queued
-// with one reservation for the whole warp.
-__device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&col)[4],
-                                       const uint32_t (&slot)[4], const bool (&ok)[4], uint32_t k,
-                                       uint32_t q) {
-    uint32_t y[4], cy[4], old[4];
+// Up to four removed-neighbour slots per lane at once (loads first, then the
+// atomics) so each lane keeps several memory operations in flight.  Entry i is
+// slot slot[i] of column col[i] of segment seg[i].  All 32 lanes call it
+// together; the nodes it removes are queued with one reservation per queue
+// for the whole warp.
+template <bool MULTI>
+__device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&seg)[4],
+                                       const uint32_t (&col)[4], const uint32_t (&slot)[4],
+                                       const bool (&ok)[4], uint32_t k, uint32_t q) {
+    uint32_t yl[4], yg[4], cy[4], old[4], lmd[4];
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        y[i] = col[i] * j.n + j.divL.div(slot[i]);
-        cy[i] = ok[i] ? ld_l2(j.cnt + y[i]) : 0u;
+        const SegP g = seg_load<MULTI>(j, seg[i]);
+        yl[i] = col[i] * g.n + g.divL.div(slot[i]);  // within the segment
+        yg[i] = g.xbase + yl[i];                      // in the launch
+        lmd[i] = g.col0 + col[i] + 1;
+        cy[i] = ok[i] ? ld_l2(j.cnt + yg[i]) : 0u;
     }
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        const uint32_t lmd = j.col0 + col[i] + 1;
-        old[i] = (ok[i] && cy[i] >= lmd) ? atomicSub(j.deg + (uint64_t)col[i] * j.nL + slot[i], 1u)
-                                         : 0u;
+        old[i] = 0u;
+        if (ok[i] && cy[i] >= lmd[i]) {
+            const SegP g = seg_load<MULTI>(j, seg[i]);
+            old[i] = atomicSub(g.deg + (uint64_t)col[i] * g.nL + slot[i], 1u);
+        }
     }
     bool rem[4];
     uint32_t nch[4], my_s = 0, my_c = 0;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        const uint32_t lmd = j.col0 + col[i] + 1;
         rem[i] = false;
-        if (ok[i] && cy[i] >= lmd && old[i] == k + 1) rem[i] = atomicSub(j.cnt + y[i], 1u) == lmd;
+        if (ok[i] && cy[i] >= lmd[i] && old[i] == k + 1)
+            rem[i] = atomicSub(j.cnt + yg[i], 1u) == lmd[i];
         nch[i] = 0;
         if (rem[i]) {
-            j.t[y[i]] = k;
-            nch[i] = chunks_of(j, y[i]);
+            const SegP g = seg_load<MULTI>(j, seg[i]);
+            g.t[yl[i]] = k;
+            nch[i] = chunks_of(g, yl[i] - col[i] * g.n, j.small_row);
             my_s += nch[i] == 0;
             my_c += nch[i];
         }
@@ -332,9 +384,9 @@ __device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&col)[4
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         if (rem[i]) {
-            if (nch[i] == 0) write_short(j, q, bs++, y[i]);
+            if (nch[i] == 0) write_short(j, q, bs++, yg[i]);
             else {
-                write_chunks(j, q, bc, y[i], nch[i]);
+                write_chunks(j, q, bc, yg[i], nch[i]);
                 bc += nch[i];
             }
         }
@@ -345,12 +397,13 @@ __device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&col)[4
 
 // SCAN(K) over `cnt_nodes` alive entries taken from `src` (or 0..nx-1 when
 // src is null, the first level): removed nodes get t = K and are queued,
-// the rest keep their count and move to `out`.
-// Survivors and queue items of a block are reserved with one atomic each per
-// block iteration (the counters are shared by the whole grid).
-template <int G>
-__device__ __forceinline__ void scan_nodes(const PeelJob& j, const uint32_t* src, uint32_t cnt_nodes, uint32_t k,
-                           uint32_t q, uint32_t* out, uint32_t* out_cnt) {
+// the rest keep their count and move to `out`.  Survivors and queue items of
+// a block are reserved with one atomic each per block iteration (the
+// counters are shared by the whole grid).
+template <int G, bool MULTI>
+__device__ __forceinline__ void scan_nodes(const PeelJob& j, const uint32_t* src, uint32_t cnt_nodes,
+                                           uint32_t k, uint32_t q, uint32_t* out,
+                                           uint32_t* out_cnt) {
     __shared__ uint32_t s_keep[32], s_short[32], s_chunk[32], s_kbase, s_sbase, s_cbase;
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warp = threadIdx.x >> 5;
@@ -360,20 +413,22 @@ __device__ __forceinline__ void scan_nodes(const PeelJob& j, const uint32_t* src
         const uint32_t idx = base + threadIdx.x / G;
         bool live = idx < cnt_nodes;
         const uint32_t x = live ? (src ? ld_l2(src + idx) : idx) : 0;
-        if (live && src && ld_l2(j.t + x) != UNSET) live = false;  // removed last level
-        const uint32_t c = j.divN.div(x);
-        const uint32_t v = x - c * j.n;
-        const uint32_t cnt = group_count_ge<G>(j.deg + (uint64_t)c * j.nL + (uint64_t)v * j.L, j.L,
+        const SegP g = seg_load<MULTI>(j, seg_of<MULTI>(j, x));
+        const uint32_t xl = x - g.xbase;
+        if (live && src && ld_l2(g.t + xl) != UNSET) live = false;  // removed last level
+        const uint32_t c = g.divN.div(xl);
+        const uint32_t v = xl - c * g.n;
+        const uint32_t cnt = group_count_ge<G>(g.deg + (uint64_t)c * g.nL + (uint64_t)v * g.L, g.L,
                                                k + 1, live);
         const bool lead = live && (lane & (G - 1)) == 0;
-        const bool remove = lead && cnt < j.col0 + c + 1;
+        const bool remove = lead && cnt < g.col0 + c + 1;
         const bool keep = lead && !remove;
-        const uint32_t nch = remove ? chunks_of(j, x) : 0u;
+        const uint32_t nch = remove ? chunks_of(g, v, j.small_row) : 0u;
         const uint32_t ns = (remove && nch == 0) ? 1u : 0u;
         if (lead) {
             j.cnt[x] = cnt;
-            if (remove) j.t[x] = k;
-            else if (!src) j.t[x] = UNSET;
+            if (remove) g.t[xl] = k;
+            else if (!src) g.t[xl] = UNSET;
         }
         const uint32_t kin = warp_incl_scan(keep ? 1u : 0u);
         const uint32_t sin = warp_incl_scan(ns);
@@ -407,17 +462,21 @@ __device__ __forceinline__ void scan_nodes(const PeelJob& j, const uint32_t* src
     }
 }
 
-template <int G>
+// Every column of every segment starts from the full degrees.
+template <bool MULTI>
 __device__ __forceinline__ void phase_init(const PeelJob& j) {
-    // degree tables: every column starts from the full degrees
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < j.nL; i += stride) {
-        const uint32_t d0 = __ldg(j.deg0 + i);
-        for (uint32_t c = 0; c < j.ncols; c++) j.deg[(uint64_t)c * j.nL + i] = d0;
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    for (uint32_t s = 0; s < j.nseg; s++) {
+        const SegP g = seg_load<MULTI>(j, s);
+        for (uint64_t i = tid; i < g.nL; i += stride) {
+            const uint32_t d0 = __ldg(g.deg0 + i);
+            for (uint32_t c = 0; c < g.ncols; c++) g.deg[(uint64_t)c * g.nL + i] = d0;
+        }
     }
 }
 
-template <int G>
+template <int G, bool MULTI>
 __device__ __forceinline__ void phase_scan(const PeelJob& j, bool first) {
     const PeelCtl* c = j.ctl;
     const uint32_t k = ld_l2(&c->level);
@@ -430,11 +489,11 @@ __device__ __forceinline__ void phase_scan(const PeelJob& j, bool first) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pc; i += gridDim.x * blockDim.x)
         j.qc[q ^ 1][i] = EMPTY;
     if (first) {
-        scan_nodes<G>(j, nullptr, j.ncols * j.n, k, q, j.alive[1], &j.ctl->alive_cnt[1]);
+        scan_nodes<G, MULTI>(j, nullptr, j.nx, k, q, j.alive[1], &j.ctl->alive_cnt[1]);
     } else {
         const uint32_t a = ld_l2(&c->alive_cur);
-        scan_nodes<G>(j, j.alive[a], ld_l2(&c->alive_cnt[a]), k, q, j.alive[a ^ 1],
-                      &j.ctl->alive_cnt[a ^ 1]);
+        scan_nodes<G, MULTI>(j, j.alive[a], ld_l2(&c->alive_cnt[a]), k, q, j.alive[a ^ 1],
+                             &j.ctl->alive_cnt[a ^ 1]);
     }
 }
 
@@ -475,24 +534,29 @@ __device__ __forceinline__ void mark_processed(PeelCtl* c, uint32_t q, uint32_t 
     }
 }
 
-// Short rows of the lanes with `ready` set (at most SMALL_ROW entries each),
+// Short rows of the lanes with `ready` set (at most small_row entries each),
 // flattened over the warp's lanes; the owner of entry q is found by binary
 // search over the warp's exclusive scan of row lengths.
+template <bool MULTI>
 __device__ __forceinline__ void expand_short(const PeelJob& j, uint32_t k, uint32_t q, uint32_t x,
                                              bool ready) {
     const uint32_t lane = threadIdx.x & 31;
-    const uint32_t col = j.divN.div(x);
-    const uint32_t v = x - col * j.n;
+    const uint32_t s = seg_of<MULTI>(j, x);
+    const SegP g = seg_load<MULTI>(j, s);
+    const uint32_t xl = x - g.xbase;
+    const uint32_t col = g.divN.div(xl);
+    const uint32_t v = xl - col * g.n;
     uint32_t b = 0, len = 0;
+    const uint32_t* adj = g.adj;
     if (ready) {
-        b = __ldg(j.node_ptr + v);
-        len = __ldg(j.node_ptr + v + 1) - b;
+        b = __ldg(g.node_ptr + v);
+        len = __ldg(g.node_ptr + v + 1) - b;
     }
     const uint32_t incl = warp_incl_scan(len);
     const uint32_t excl = incl - len;
     const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
     for (uint32_t jb = 0; jb < total; jb += 128) {
-        uint32_t cols[4], slot[4];
+        uint32_t segs[4], cols[4], slot[4];
         bool ok[4];
 #pragma unroll
         for (int i = 0; i < 4; i++) {
@@ -507,33 +571,42 @@ __device__ __forceinline__ void expand_short(const PeelJob& j, uint32_t k, uint3
             const uint32_t ob = __shfl_sync(0xffffffffu, b, own);
             const uint32_t oe = __shfl_sync(0xffffffffu, excl, own);
             cols[i] = __shfl_sync(0xffffffffu, col, own);
+            segs[i] = MULTI ? __shfl_sync(0xffffffffu, s, own) : 0u;
+            const uint32_t* oadj = MULTI ? (const uint32_t*)__shfl_sync(
+                                               0xffffffffu, (unsigned long long)adj, own)
+                                         : adj;
             ok[i] = qq < total;
-            slot[i] = ok[i] ? __ldg(j.adj + ob + (qq - oe)) : 0u;
+            slot[i] = ok[i] ? __ldg(oadj + ob + (qq - oe)) : 0u;
         }
-        visit4(j, cols, slot, ok, k, q);
+        visit4<MULTI>(j, segs, cols, slot, ok, k, q);
     }
 }
 
 // One CHUNK-entry piece of a long row, by the whole warp.
+template <bool MULTI>
 __device__ __forceinline__ void expand_chunk(const PeelJob& j, uint32_t k, uint32_t q,
                                              unsigned long long it) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t x = (uint32_t)it, ch = (uint32_t)(it >> 32);
-    const uint32_t col = j.divN.div(x);
-    const uint32_t v = x - col * j.n;
-    const uint32_t cb = __ldg(j.node_ptr + v) + ch * CHUNK;
-    const uint32_t ce = min(__ldg(j.node_ptr + v + 1), cb + CHUNK);
+    const uint32_t s = seg_of<MULTI>(j, x);
+    const SegP g = seg_load<MULTI>(j, s);
+    const uint32_t xl = x - g.xbase;
+    const uint32_t col = g.divN.div(xl);
+    const uint32_t v = xl - col * g.n;
+    const uint32_t cb = __ldg(g.node_ptr + v) + ch * CHUNK;
+    const uint32_t ce = min(__ldg(g.node_ptr + v + 1), cb + CHUNK);
     for (uint32_t q0 = cb; q0 < ce; q0 += 128) {
-        uint32_t cols[4], slot[4];
+        uint32_t segs[4], cols[4], slot[4];
         bool ok[4];
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             const uint32_t p = q0 + lane + 32 * i;
             ok[i] = p < ce;
-            slot[i] = ok[i] ? __ldg(j.adj + p) : 0u;
+            slot[i] = ok[i] ? __ldg(g.adj + p) : 0u;
             cols[i] = col;
+            segs[i] = s;
         }
-        visit4(j, cols, slot, ok, k, q);
+        visit4<MULTI>(j, segs, cols, slot, ok, k, q);
     }
 }
 
@@ -543,6 +616,7 @@ __device__ __forceinline__ void expand_chunk(const PeelJob& j, uint32_t k, uint3
 // claim may run past the reserved items when warps race for the last ones;
 // such a slot is either filled by a later removal or abandoned when the level
 // completes -- meanwhile the warp keeps serving the other queue.
+template <bool MULTI>
 __device__ __forceinline__ void phase_drain(const PeelJob& j) {
     PeelCtl* c = j.ctl;
     const uint32_t k = ld_l2(&c->level);
@@ -578,7 +652,7 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j) {
             if (lane == 0 && cidx < j.qc_cap) it = ld_relaxed64(j.qc[q] + cidx);
             it = __shfl_sync(0xffffffffu, it, 0);
             if (it != EMPTY) {
-                expand_chunk(j, k, q, it);
+                expand_chunk<MULTI>(j, k, q, it);
                 mark_processed(c, q, QC, 1);
                 cidx = NONE;
                 progress = true;
@@ -591,7 +665,7 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j) {
             const bool ready = x != EMPTY32;
             const uint32_t rmask = __ballot_sync(0xffffffffu, ready);
             if (rmask) {
-                expand_short(j, k, q, ready ? x : 0u, ready);
+                expand_short<MULTI>(j, k, q, ready ? x : 0u, ready);
                 if (ready) sidx = NONE;
                 mark_processed(c, q, QS, (uint32_t)__popc(rmask));
                 progress = true;
@@ -620,16 +694,16 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j) {
 
 // T threads per block, 1024 threads resident per SM (512 x 2 or 1024 x 1):
 // at most 64 registers a thread.
-template <int G, int T>
+template <int G, int T, bool MULTI>
 __global__ void __launch_bounds__(T, 1024 / T) k_peel(PeelJob j) {
-    phase_init<G>(j);
+    phase_init<MULTI>(j);
     if (!grid_barrier(j)) return;
-    phase_scan<G>(j, true);
+    phase_scan<G, MULTI>(j, true);
     if (!grid_barrier(j)) return;
     for (;;) {
         const uint32_t ph = ld_l2(&j.ctl->phase);
-        if (ph == PH_DRAIN) phase_drain(j);
-        else if (ph == PH_SCAN) phase_scan<G>(j, false);
+        if (ph == PH_DRAIN) phase_drain<MULTI>(j);
+        else if (ph == PH_SCAN) phase_scan<G, MULTI>(j, false);
         else return;
         if (!grid_barrier(j)) return;
     }
@@ -657,88 +731,112 @@ uint32_t peel_columns_per_group(const DeviceGraph* d) {
     return (uint32_t)cols;
 }
 
-template <int G, int T>
+template <int G, int T, bool MULTI>
 static fc_status launch_t(PeelJob& j, cudaStream_t s) {
     int dev = 0, sms = 0, occ = 0;
     FC_CUDA_TRY(cudaGetDevice(&dev));
     FC_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    FC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_peel<G, T>, T, 0));
+    FC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_peel<G, T, MULTI>, T, 0));
     if (occ < 1) return FC_ERR_DEVICE;
     uint32_t want_occ = env_u32("FC_PEEL_BLOCKS_PER_SM", 1024 / T);
     if (want_occ >= 1 && (int)want_occ < occ) occ = (int)want_occ;
     dim3 grid(sms * occ), block(T);
     void* args[] = {&j};
-    FC_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_peel<G, T>, grid, block, args, 0, s));
+    FC_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_peel<G, T, MULTI>, grid, block, args, 0, s));
     return FC_OK;
 }
 
-template <int G>
-static fc_status launch(PeelJob& j, cudaStream_t s) {
-    // FC_PEEL_THREADS: 512 (default, 2 blocks per SM) or 1024 (1 per SM)
-    if (env_u32("FC_PEEL_THREADS", 512) == 1024) return launch_t<G, 1024>(j, s);
-    return launch_t<G, 512>(j, s);
+template <int G, bool MULTI>
+static fc_status launch_g(PeelJob& j, uint32_t threads, cudaStream_t s) {
+    if (threads == 1024) return launch_t<G, 1024, MULTI>(j, s);
+    return launch_t<G, 512, MULTI>(j, s);
 }
 
-// Workspace of a group of `ncols` columns: qc0 qc1 (uint64) | qs0 qs1 | deg |
-// cnt alive0 alive1 | control block.  A level removes each node at most once:
-// short rows take one qs item, long rows at most entries/CHUNK + 1 qc items.
-static void peel_caps(uint32_t n, uint32_t L, uint64_t entries, uint32_t ncols, uint64_t* qs_cap,
-                      uint64_t* qc_cap) {
-    const uint64_t nx = (uint64_t)ncols * n;
+// Group of G lanes per node in SCAN: the smallest power of two >= L, at most 32.
+template <bool MULTI>
+static fc_status launch(PeelJob& j, uint32_t maxL, uint32_t threads, cudaStream_t s) {
+    if (maxL <= 1) return launch_g<1, MULTI>(j, threads, s);
+    if (maxL <= 2) return launch_g<2, MULTI>(j, threads, s);
+    if (maxL <= 4) return launch_g<4, MULTI>(j, threads, s);
+    if (maxL <= 8) return launch_g<8, MULTI>(j, threads, s);
+    if (maxL <= 16) return launch_g<16, MULTI>(j, threads, s);
+    return launch_g<32, MULTI>(j, threads, s);
+}
+
+static uint32_t default_threads() { return env_u32("FC_PEEL_THREADS", 512) == 1024 ? 1024 : 512; }
+
+// Queue capacities: a level removes each node at most once; short rows take
+// one qs item, long rows at most entries/CHUNK + 1 qc items.
+static void queue_caps(uint64_t nx, uint64_t col_entries, uint64_t* qs_cap, uint64_t* qc_cap) {
     *qs_cap = nx + 64;
-    *qc_cap = nx + ((uint64_t)ncols * entries + CHUNK - 1) / CHUNK + 64;
-    (void)L;
+    *qc_cap = nx + (col_entries + CHUNK - 1) / CHUNK + 64;
+}
+
+static uint64_t shared_ws_bytes(uint64_t nx, uint64_t col_entries) {
+    uint64_t qs_cap, qc_cap;
+    queue_caps(nx, col_entries, &qs_cap, &qc_cap);
+    // qc0 qc1 (u64) | qs0 qs1 | cnt alive0 alive1 | control block (256-aligned)
+    return 4 * (4 * qc_cap + 2 * qs_cap + 3 * nx) + sizeof(PeelCtl) + 256;
 }
 
 uint64_t peel_ws_bytes(uint32_t n, uint32_t L, uint64_t entries, uint32_t ncols) {
-    uint64_t qs_cap, qc_cap;
-    peel_caps(n, L, entries, ncols, &qs_cap, &qc_cap);
     const uint64_t nx = (uint64_t)ncols * n;
-    // + the control block, 256-byte aligned after the lists
-    return 4 * (4 * qc_cap + 2 * qs_cap + (uint64_t)ncols * n * L + 3 * nx) + sizeof(PeelCtl) + 256;
+    return shared_ws_bytes(nx, (uint64_t)ncols * entries) + 4ull * ncols * n * L;
 }
 
-fc_status peel_run(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* table, void* ws,
-                   size_t ws_bytes, cudaStream_t s, PeelStats* st, bool instrument) {
-    const uint32_t n = g.n, L = g.L;
-    const uint64_t nx = (uint64_t)ncols * n;
-    const uint64_t nL = (uint64_t)n * L;
+// Lays the shared part of the workspace out at `w` (queues, counts, lists,
+// control block) and sets the job's pointers; returns the first free byte.
+static char* carve_shared(PeelJob& j, char* w, char* end, uint64_t nx, uint64_t col_entries,
+                          cudaStream_t s, fc_status* rc) {
     uint64_t qs_cap, qc_cap;
-    peel_caps(n, L, g.entries, ncols, &qs_cap, &qc_cap);
-    if (qc_cap >= (1ull << 32) || qs_cap >= (1ull << 32)) return FC_ERR_TOO_LARGE;
-    if (peel_ws_bytes(n, L, g.entries, ncols) > ws_bytes) return FC_ERR_INVALID;
-    uint32_t* w = (uint32_t*)ws;
-    PeelJob j;
-    j.qc[0] = (unsigned long long*)w;
-    w += 2 * qc_cap;
-    j.qc[1] = (unsigned long long*)w;
-    w += 2 * qc_cap;
-    j.qs[0] = w;
-    w += qs_cap;
-    j.qs[1] = w;
-    w += qs_cap;
+    queue_caps(nx, col_entries, &qs_cap, &qc_cap);
+    *rc = FC_OK;
+    if (qc_cap >= (1ull << 32) || qs_cap >= (1ull << 32) || nx >= (1ull << 32)) {
+        *rc = FC_ERR_TOO_LARGE;
+        return w;
+    }
+    uint32_t* p = (uint32_t*)w;
+    j.qc[0] = (unsigned long long*)p;
+    p += 2 * qc_cap;
+    j.qc[1] = (unsigned long long*)p;
+    p += 2 * qc_cap;
+    j.qs[0] = p;
+    p += qs_cap;
+    j.qs[1] = p;
+    p += qs_cap;
     j.qc_cap = (uint32_t)qc_cap;
     j.qs_cap = (uint32_t)qs_cap;
-    j.n = n;
-    j.L = L;
-    j.col0 = col0;
-    j.ncols = ncols;
-    j.nL = nL;
-    j.divL.init(L);
-    j.divN.init(n);
-    j.node_ptr = g.node_ptr;
-    j.adj = g.adj;
-    j.deg0 = g.deg0;
-    j.deg = w;
-    w += ncols * nL;
-    j.t = table + (uint64_t)col0 * n;
-    j.cnt = w; w += nx;
-    j.alive[0] = w; w += nx;
-    j.alive[1] = w; w += nx;
-    j.ctl = (PeelCtl*)(((uintptr_t)w + 255) & ~(uintptr_t)255);
-    if ((char*)(j.ctl + 1) > (char*)ws + ws_bytes) return FC_ERR_INVALID;  // layout check
-    j.max_level = g.max_level;
+    j.nx = (uint32_t)nx;
+    j.cnt = p;
+    p += nx;
+    j.alive[0] = p;
+    p += nx;
+    j.alive[1] = p;
+    p += nx;
+    j.ctl = (PeelCtl*)(((uintptr_t)p + 255) & ~(uintptr_t)255);
+    char* next = (char*)(j.ctl + 1);
+    if (next > end) {  // layout check
+        *rc = FC_ERR_INVALID;
+        return w;
+    }
+    return next;  // the queues and the control block are cleared by reset_job
+}
+
+// Launches the prepared job and reads its control block back.
+// Every queue slot starts EMPTY (qc and qs are contiguous); the control block
+// starts all zero, which is phase INIT.
+static fc_status reset_job(const PeelJob& j, cudaStream_t s) {
+    FC_CUDA_TRY(cudaMemsetAsync(j.qc[0], 0xFF, (4ull * j.qc_cap + 2ull * j.qs_cap) * 4, s));
+    FC_CUDA_TRY(cudaMemsetAsync(j.ctl, 0, sizeof(PeelCtl), s));
+    return FC_OK;
+}
+
+template <bool MULTI>
+static fc_status run_job(PeelJob& j, uint32_t maxL, uint32_t threads, cudaStream_t s,
+                         PeelStats* st, bool instrument, uint32_t col0, uint32_t ncols,
+                         bool* use_graph = nullptr) {
     j.idle_polls = env_u32("FC_PEEL_IDLE_POLLS", 8);
+    if (!j.small_row) j.small_row = env_u32("FC_PEEL_SMALL_ROW", SMALL_ROW_DEFAULT);
     j.timeout_ns = (uint64_t)env_u32("FC_BARRIER_TIMEOUT_MS", 10000) * 1000000ull;
     j.trace = nullptr;
     j.trace_levels = 0;
@@ -748,26 +846,48 @@ fc_status peel_run(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* 
         FC_TRY(dev_alloc((void**)&j.trace, 6ull * 8 * j.trace_levels, s));
         FC_CUDA_TRY(cudaMemsetAsync(j.trace, 0, 6ull * 8 * j.trace_levels, s));
     }
-    // every queue slot starts EMPTY (qc and qs are contiguous); the control
-    // block starts all zero, which is phase INIT
-    FC_CUDA_TRY(cudaMemsetAsync(j.qc[0], 0xFF, (4 * qc_cap + 2 * qs_cap) * 4, s));
-    FC_CUDA_TRY(cudaMemsetAsync(j.ctl, 0, sizeof(PeelCtl), s));
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (instrument) {
         FC_CUDA_TRY(cudaEventCreate(&e0));
         FC_CUDA_TRY(cudaEventCreate(&e1));
-        FC_CUDA_TRY(cudaEventRecord(e0, s));
     }
-    fc_status rc;
-    if (L <= 1) rc = launch<1>(j, s);
-    else if (L <= 2) rc = launch<2>(j, s);
-    else if (L <= 4) rc = launch<4>(j, s);
-    else if (L <= 8) rc = launch<8>(j, s);
-    else if (L <= 16) rc = launch<16>(j, s);
-    else rc = launch<32>(j, s);
-    FC_TRY(rc);
+    // the run: clear the queues and the control block, then the launch --
+    // captured as one CUDA graph when asked (and when the driver captures a
+    // cooperative launch), else issued directly
+    bool graphed = false;
+    if (use_graph && *use_graph) {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        bool ok = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+        if (ok) {
+            fc_status r1 = reset_job(j, s);
+            fc_status r2 = r1 == FC_OK ? launch<MULTI>(j, maxL, threads, s) : r1;
+            ok = cudaStreamEndCapture(s, &graph) == cudaSuccess && r2 == FC_OK;
+        }
+        if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+        if (ok) {
+            if (instrument) FC_CUDA_TRY(cudaEventRecord(e0, s));
+            ok = cudaGraphLaunch(exec, s) == cudaSuccess;
+            graphed = ok;
+        }
+        cudaGetLastError();  // a refused capture falls back to direct launches
+        if (graph && !graphed) cudaGraphDestroy(graph);
+        if (exec && !graphed) cudaGraphExecDestroy(exec);
+        if (graphed) {
+            if (instrument) FC_CUDA_TRY(cudaEventRecord(e1, s));
+            FC_CUDA_TRY(cudaStreamSynchronize(s));
+            cudaGraphExecDestroy(exec);
+            cudaGraphDestroy(graph);
+        }
+    }
+    if (!graphed) {
+        if (instrument) FC_CUDA_TRY(cudaEventRecord(e0, s));
+        FC_TRY(reset_job(j, s));
+        FC_TRY(launch<MULTI>(j, maxL, threads, s));
+        if (instrument) FC_CUDA_TRY(cudaEventRecord(e1, s));
+    }
+    if (use_graph) *use_graph = graphed;
     count_launch();
-    if (instrument) FC_CUDA_TRY(cudaEventRecord(e1, s));
     PeelCtl out;
     FC_CUDA_TRY(cudaMemcpyAsync(&out, j.ctl, sizeof(out), cudaMemcpyDeviceToHost, s));
     FC_CUDA_TRY(cudaStreamSynchronize(s));
@@ -800,6 +920,112 @@ fc_status peel_run(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* 
     }
     if (out.err) return FC_ERR_ITER_LIMIT;
     return FC_OK;
+}
+
+static SegP make_seg(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* table,
+                     uint32_t* deg, uint32_t xbase) {
+    SegP p{};
+    p.xbase = xbase;
+    p.n = g.n;
+    p.L = g.L;
+    p.col0 = col0;
+    p.divL.init(g.L);
+    p.divN.init(g.n);
+    p.nL = (uint64_t)g.n * g.L;
+    p.node_ptr = g.node_ptr;
+    p.adj = g.adj;
+    p.deg0 = g.deg0;
+    p.deg = deg;
+    p.t = table + (uint64_t)col0 * g.n;
+    p.ncols = ncols;
+    return p;
+}
+
+fc_status peel_run(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* table, void* ws,
+                   size_t ws_bytes, cudaStream_t s, PeelStats* st, bool instrument) {
+    const uint64_t nx = (uint64_t)ncols * g.n;
+    if (peel_ws_bytes(g.n, g.L, g.entries, ncols) > ws_bytes) return FC_ERR_INVALID;
+    PeelJob j{};
+    char* w = (char*)ws;
+    char* end = w + ws_bytes;
+    uint32_t* deg = (uint32_t*)w;  // ncols * n * L at the start (4-byte aligned)
+    w += 4ull * ncols * g.n * g.L;
+    fc_status rc;
+    carve_shared(j, w, end, nx, (uint64_t)ncols * g.entries, s, &rc);
+    FC_TRY(rc);
+    j.seg0 = make_seg(g, col0, ncols, table, deg, 0);
+    j.segs = nullptr;
+    j.seg_xbase = nullptr;
+    j.nseg = 1;
+    j.max_level = g.max_level;
+    return run_job<false>(j, g.L, default_threads(), s, st, instrument, col0, ncols);
+}
+
+uint64_t peel_batch_ws_bytes(const std::vector<PeelSegSpec>& specs) {
+    uint64_t nx = 0, ent = 0, deg = 0;
+    for (const auto& sp : specs) {
+        nx += (uint64_t)sp.ncols * sp.g.n;
+        ent += (uint64_t)sp.ncols * sp.g.entries;
+        deg += 4ull * sp.ncols * sp.g.n * sp.g.L;
+    }
+    const uint64_t nseg = specs.size();
+    const uint64_t seg_bytes = (nseg * sizeof(SegP) + 4 * (nseg + 1) + 511) & ~511ull;
+    return shared_ws_bytes(nx, ent) + deg + seg_bytes + 256;
+}
+
+fc_status peel_batch(const std::vector<PeelSegSpec>& specs, void* ws, size_t ws_bytes,
+                     cudaStream_t s, PeelStats* st, uint32_t threads, uint32_t small_row,
+                     bool* use_graph) {
+    if (specs.empty()) return FC_OK;
+    if (peel_batch_ws_bytes(specs) > ws_bytes) return FC_ERR_INVALID;
+    char* w = (char*)ws;
+    char* end = w + ws_bytes;
+    // segment table and bases first (kept 256-byte aligned), then the degree
+    // tables, then the shared lists
+    const uint32_t nseg = (uint32_t)specs.size();
+    std::vector<SegP> host(nseg);
+    std::vector<uint32_t> xb(nseg + 1);
+    uint64_t nx = 0, ent = 0;
+    uint32_t maxL = 1, max_level = 1;
+    SegP* dsegs = (SegP*)w;
+    uint32_t* dxb = (uint32_t*)(w + nseg * sizeof(SegP));
+    w += (nseg * sizeof(SegP) + 4 * (nseg + 1) + 511) & ~511ull;
+    for (uint32_t i = 0; i < nseg; i++) {
+        const PeelSegSpec& sp = specs[i];
+        if (nx >= (1ull << 32)) return FC_ERR_TOO_LARGE;
+        uint32_t* deg = (uint32_t*)w;
+        w += 4ull * sp.ncols * sp.g.n * sp.g.L;
+        host[i] = make_seg(sp.g, sp.col0, sp.ncols, sp.table, deg, (uint32_t)nx);
+        xb[i] = (uint32_t)nx;
+        nx += (uint64_t)sp.ncols * sp.g.n;
+        ent += (uint64_t)sp.ncols * sp.g.entries;
+        maxL = sp.g.L > maxL ? sp.g.L : maxL;
+        max_level = sp.g.max_level > max_level ? sp.g.max_level : max_level;
+    }
+    if (nx >= (1ull << 32)) return FC_ERR_TOO_LARGE;
+    xb[nseg] = (uint32_t)nx;
+    w = (char*)(((uintptr_t)w + 255) & ~(uintptr_t)255);
+    PeelJob j{};
+    fc_status rc;
+    carve_shared(j, w, end, nx, ent, s, &rc);
+    FC_TRY(rc);
+    FC_CUDA_TRY(cudaMemcpyAsync(dsegs, host.data(), nseg * sizeof(SegP), cudaMemcpyHostToDevice, s));
+    FC_CUDA_TRY(cudaMemcpyAsync(dxb, xb.data(), 4 * (nseg + 1), cudaMemcpyHostToDevice, s));
+    j.seg0 = host[0];
+    j.segs = dsegs;
+    j.seg_xbase = dxb;
+    j.nseg = nseg;
+    j.max_level = max_level;
+    j.small_row = small_row;
+    if (!threads) threads = default_threads();
+    // the segment table must be on the device before a captured launch runs
+    if (use_graph && *use_graph) FC_CUDA_TRY(cudaStreamSynchronize(s));
+    if (nseg == 1) {
+        j.segs = nullptr;
+        return run_job<false>(j, maxL, threads, s, st, true, specs[0].col0, specs[0].ncols,
+                              use_graph);
+    }
+    return run_job<true>(j, maxL, threads, s, st, true, 0, 0, use_graph);
 }
 
 fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream_t s,

@@ -53,7 +53,17 @@ class Cell(C.Structure):
 
 class BatchOptions(C.Structure):
     _fields_ = [("block_threads", C.c_uint32), ("hub_threshold", C.c_uint32),
-                ("use_cuda_graph", C.c_int)]
+                ("use_cuda_graph", C.c_int), ("plain", C.c_int)]
+
+
+class BatchReport(C.Structure):
+    _fields_ = [("peel_ms", C.c_double), ("densest_ms", C.c_double),
+                ("peel_launches", C.c_uint32), ("block_threads", C.c_uint32),
+                ("hub_threshold", C.c_uint32), ("levels", C.c_uint32),
+                ("used_cuda_graph", C.c_int), ("autotuned", C.c_int)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 class Stats(C.Structure):
@@ -105,7 +115,7 @@ def lib():
         "fc_densest": ([p, p, u32, p, p], i32),
         "fc_densest_members": ([p, p, p, p, p], i32),
         "fc_cells": ([p, C.c_double, p, u32, C.POINTER(u32), p], i32),
-        "fc_batch_run": ([p, u32, C.c_double, p, p, p, p], i32),
+        "fc_batch_run": ([p, u32, C.c_double, p, p, p, p, p], i32),
         "fc_server_create": ([p, pp], i32),
         "fc_server_submit": ([p, p, C.c_double, p, p, C.POINTER(u64)], i32),
         "fc_server_wait": ([p, u64, C.c_int64, C.POINTER(i32), C.POINTER(C.c_double)], i32),

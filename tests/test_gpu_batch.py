@@ -1,0 +1,86 @@
+"""Batched decomposition (fc_batch_run): one persistent launch over many
+graphs must give every graph exactly the table and densest result it gets
+alone -- checked against the reference's golden outputs and the oracle, in
+the batched form (with and without CUDA-graph capture, autotuned and with
+fixed configurations) and in the plain one-column-per-launch form."""
+import numpy as np
+import pytest
+
+import golden_cases as G
+import oracle as O
+from pargridcpu_b200 import MultilayerGraph, batch_run, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _batch_inputs():
+    gens = [G.inputs(name) for name in ("mix0", "mix1", "mix2", "mix3", "tiny_dirty", "layers33")]
+    gens += [synth.chung_lu_graph(800, 1, 2400, 2.2, 0.0, 301).layers,
+             synth.chung_lu_graph(3000, 2, 6000, 2.4, 0.5, 302).layers,
+             synth.erdos_renyi_graph(50, 40, 0.02, 0.1, 303).layers,
+             synth.chung_lu_graph(12000, 7, 30000, 2.05, 0.3, 304).layers,
+             [np.array([[1, 2]], np.uint32)]]
+    gens += [g.layers for g in synth.batch_mix(count=10, seed=305, n_lo=500, n_hi=8000)]
+    return gens
+
+
+@pytest.fixture(scope="module")
+def batch():
+    layers = _batch_inputs()
+    expected = []
+    for ls in layers:
+        og = O.OracleGraph(ls)
+        t = og.coreindex()
+        expected.append((t, og.densest(t, 1.0, with_cells=False)))
+    return layers, expected
+
+
+def _check(tables, results, expected):
+    for i, ((t, o), got_t, r) in enumerate(zip(expected, tables, results)):
+        assert np.array_equal(got_t, t), f"graph {i}: table"
+        assert (r["k"], r["lmd"], r["length"], r["lstar"]) == (o["k"], o["lmd"], o["length"],
+                                                                o["lstar"]), f"graph {i}"
+        assert r["density"] == o["density"], f"graph {i}: density"
+        assert np.float32(r["max_density_f"]) == np.float32(o["max_density_f"])
+
+
+@pytest.mark.parametrize("mode", [
+    dict(),                                                  # autotuned, CUDA graph
+    dict(use_cuda_graph=False),
+    dict(block_threads=1024, hub_threshold=16),
+    dict(block_threads=512, hub_threshold=64, use_cuda_graph=False),
+    dict(plain=True),
+], ids=["auto", "no-graph", "t1024-h16", "t512-h64", "plain"])
+def test_batch_matches_oracle(batch, mode):
+    layers, expected = batch
+    graphs = [MultilayerGraph.from_pairs(ls) for ls in layers]
+    tables, results, report = batch_run(graphs, beta=1.0, **mode)
+    _check(tables, results, expected)
+    if not mode.get("plain"):
+        assert report["peel_launches"] >= 1
+        assert report["block_threads"] in (512, 1024)
+    print(mode, report)
+
+
+def test_batch_golden_fixtures():
+    names = ["mix0", "mix1", "mix2", "mix3", "c1", "c2"]
+    graphs = [MultilayerGraph.from_pairs(G.inputs(n)) for n in names]
+    tables, results, _ = batch_run(graphs, beta=2.0)
+    for name, t, r in zip(names, tables, results):
+        exp = G.expected(name)
+        assert np.array_equal(t, exp["table"]), name
+        k, lmd, length = (int(x) for x in exp["b2.0_result"])
+        assert (r["k"], r["lmd"], r["length"]) == (k, lmd, length), name
+        assert np.float32(r["max_density_f"]) == exp["b2.0_maxf"]
+
+
+def test_batch_same_as_alone():
+    gens = synth.batch_mix(count=6, seed=306, n_lo=2000, n_hi=30000)
+    graphs = [MultilayerGraph.from_pairs(g.layers) for g in gens]
+    tables, results, _ = batch_run(graphs, beta=1.0)
+    for g, t, r in zip(gens, tables, results):
+        alone = MultilayerGraph.from_pairs(g.layers)
+        assert np.array_equal(alone.coreindex(), t)
+        a = alone.densest([1.0])[0]
+        assert (a["k"], a["lmd"], a["length"], a["density"]) == (r["k"], r["lmd"], r["length"],
+                                                                 r["density"])
