@@ -12,6 +12,7 @@
 // launch -- "a single launch per lambda".
 #include <algorithm>
 #include <chrono>
+#include <cstdio>
 #include <cstdlib>
 #include <map>
 #include <mutex>
@@ -27,6 +28,21 @@ static uint32_t env_u32b(const char* name, uint32_t dflt) {
     return s && *s ? (uint32_t)strtoul(s, nullptr, 10) : dflt;
 }
 
+// FC_DEBUG=1: one stderr line per step of a batched run
+static bool debug_on() {
+    static int v = -1;
+    if (v < 0) v = env_u32b("FC_DEBUG", 0) ? 1 : 0;
+    return v == 1;
+}
+#define BATCH_TRACE(...)                          \
+    do {                                          \
+        if (debug_on()) {                         \
+            fprintf(stderr, "batch: " __VA_ARGS__); \
+            fputc('\n', stderr);                  \
+            fflush(stderr);                       \
+        }                                         \
+    } while (0)
+
 static fc_status densest_all(fc_graph* const* gs, uint32_t count, double beta,
                              fc_densest_result* res, cudaStream_t s, double* ms) {
     *ms = 0;
@@ -34,6 +50,7 @@ static fc_status densest_all(fc_graph* const* gs, uint32_t count, double beta,
         fc_graph* g = gs[i];
         if (!res) continue;
         if (g->n && g->L) {
+            BATCH_TRACE("densest graph %u (n %u, L %u)", i, g->n, g->L);
             FC_TRY(densest(g, &beta, 1, res + i, s));
             *ms += g->dev->stats.densest_ms;
         } else {
@@ -132,7 +149,10 @@ static fc_status run_groups(const std::vector<PeelSegSpec>& specs,
         std::vector<PeelSegSpec> part(specs.begin() + gr.first, specs.begin() + gr.second);
         PeelStats st;
         bool g = want_graph;
+        BATCH_TRACE("peel graphs [%zu, %zu) threads %u small_row %u graph %d", gr.first,
+                    gr.second, threads, small_row, (int)g);
         FC_TRY(peel_batch(part, ws, ws_bytes, s, &st, threads, small_row, &g));
+        BATCH_TRACE("  done: %.3f ms, %u levels, cuda graph %d", st.ms, st.levels, (int)g);
         *graphed = *graphed && g;
         *ms += st.ms;
         *levels += st.levels;
@@ -172,6 +192,8 @@ static fc_status batch_persistent(fc_graph* const* gs, uint32_t count, double be
         std::vector<PeelSegSpec> part(specs.begin() + gr.first, specs.begin() + gr.second);
         ws_bytes = std::max(ws_bytes, peel_batch_ws_bytes(part));
     }
+    BATCH_TRACE("%u graphs uploaded, %zu segments, %zu launch groups, workspace %llu bytes", count,
+                specs.size(), groups.size(), (unsigned long long)ws_bytes);
     void* ws = nullptr;
     if (!specs.empty()) FC_TRY(dev_alloc(&ws, ws_bytes, s));
     const bool want_graph = opt ? opt->use_cuda_graph != 0 : true;

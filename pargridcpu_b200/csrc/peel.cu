@@ -46,7 +46,12 @@ namespace fc {
 
 // PH_INIT is 0 so that a zeroed control block starts a run
 enum : uint32_t { PH_INIT = 0, PH_SCAN = 1, PH_DRAIN = 2, PH_DONE = 3 };
-enum : uint32_t { ERR_NONE = 0, ERR_BARRIER = 1, ERR_LIMIT = 2, ERR_QUEUE = 3 };
+// ERR_DEADLINE: the whole run took longer than its deadline (a bound on
+// every loop, including ones that keep making progress); ERR_ITEM: a dequeued
+// item named no node of the launch (recorded and skipped, never expanded).
+enum : uint32_t {
+    ERR_NONE = 0, ERR_BARRIER = 1, ERR_LIMIT = 2, ERR_QUEUE = 3, ERR_DEADLINE = 4, ERR_ITEM = 5
+};
 constexpr uint32_t UNSET = 0xFFFFFFFFu;
 constexpr unsigned long long EMPTY = ~0ull;
 constexpr uint32_t EMPTY32 = 0xFFFFFFFFu;
@@ -73,7 +78,9 @@ struct PeelCtl {
     uint32_t alive_cnt[2];
     uint32_t levels, items, pad1, pad2;
     uint64_t t_last;      // globaltimer at the last barrier
+    uint64_t t_start;     // globaltimer at the first barrier
     uint64_t ph_ns[4];    // time per phase kind: scan, drain
+    uint32_t bad_item, bad_where, err_level, pad3;  // what ERR_ITEM saw; level of the error
     Hot tail[2][2];       // [q][s] items reserved
     Hot head[2][2];       // [q][s] items claimed
     Hot processed[2][2];  // [q][s] items fully processed
@@ -107,7 +114,8 @@ struct PeelJob {
     uint32_t max_level;
     uint32_t idle_polls;  // empty polls after which a non-polling warp leaves DRAIN
     uint32_t small_row;   // longest row queued as one item; longer rows go in chunks
-    uint64_t timeout_ns;
+    uint64_t timeout_ns;  // longest wait without progress
+    uint64_t deadline_ns; // longest whole run
     // optional per-level trace: [level][scan|drain] = {ns, items, alive}
     unsigned long long* trace;
     uint32_t trace_levels;
@@ -140,6 +148,9 @@ __device__ __forceinline__ uint64_t global_ns() {
 }
 // data written by other SMs during the kernel is read through L2 only
 __device__ __forceinline__ uint32_t ld_l2(const uint32_t* p) { return __ldcg(p); }
+__device__ __forceinline__ uint64_t ld_l2_64(const uint64_t* p) {
+    return __ldcg((const unsigned long long*)p);
+}
 
 // ---- segments ---------------------------------------------------------------
 
@@ -220,6 +231,7 @@ __device__ void leader_step(volatile PeelCtl* c, const PeelJob& j) {
     };
     switch (c->phase) {
         case PH_INIT:  // degree tables copied: the first scan follows
+            c->t_start = c->t_last;
             c->phase = PH_SCAN;
             break;
         case PH_SCAN:  // the first scan wrote alive[1]
@@ -236,7 +248,10 @@ __device__ void leader_step(volatile PeelCtl* c, const PeelJob& j) {
         default:
             c->phase = PH_DONE;
     }
-    if (c->err) c->phase = PH_DONE;
+    if (c->err) {
+        c->err_level = c->level;
+        c->phase = PH_DONE;
+    }
 }
 
 // Grid barrier with a bounded wait.  Returns false once any block has
@@ -510,17 +525,34 @@ __device__ __forceinline__ bool level_done(PeelCtl* c, uint32_t q) {
 // Warp-uniform decision while waiting (lane 0 decides): 0 keep waiting, 1 the
 // level is done, 2 an error was recorded or this warp made no progress for
 // the timeout.
+__device__ __forceinline__ bool past_deadline(const PeelJob& j, uint64_t now) {
+    return now - ld_l2_64(&j.ctl->t_start) > j.deadline_ns;
+}
+
 __device__ __forceinline__ uint32_t wait_check(const PeelJob& j, uint32_t q, uint64_t t0) {
     uint32_t r = 0;
     if ((threadIdx.x & 31) == 0) {
+        const uint64_t now = global_ns();
         if (level_done(j.ctl, q)) {
             r = 1;
-        } else if (global_ns() - t0 > j.timeout_ns || ld_l2(&j.ctl->err) != ERR_NONE) {
+        } else if (now - t0 > j.timeout_ns || ld_l2(&j.ctl->err) != ERR_NONE) {
             atomicCAS(&j.ctl->err, ERR_NONE, ERR_BARRIER);
+            r = 2;
+        } else if (past_deadline(j, now)) {
+            atomicCAS(&j.ctl->err, ERR_NONE, ERR_DEADLINE);
             r = 2;
         }
     }
     return __shfl_sync(0xffffffffu, r, 0);
+}
+
+// A dequeued item that names no node of the launch: the first one is
+// recorded and the run ends with ERR_ITEM; the item itself is skipped.
+__device__ __noinline__ void record_bad(const PeelJob& j, uint32_t item, uint32_t where) {
+    if (atomicCAS(&j.ctl->err, ERR_NONE, ERR_ITEM) == ERR_NONE) {
+        j.ctl->bad_item = item;
+        j.ctl->bad_where = where;
+    }
 }
 
 // Count `n` of this warp's items of kind s as processed.  The items the warp
@@ -551,6 +583,10 @@ __device__ __forceinline__ void expand_short(const PeelJob& j, uint32_t k, uint3
     if (ready) {
         b = __ldg(g.node_ptr + v);
         len = __ldg(g.node_ptr + v + 1) - b;
+        if (len > j.small_row) {  // long rows are never queued as short items
+            record_bad(j, x, 1);
+            len = 0;
+        }
     }
     const uint32_t incl = warp_incl_scan(len);
     const uint32_t excl = incl - len;
@@ -593,8 +629,13 @@ __device__ __forceinline__ void expand_chunk(const PeelJob& j, uint32_t k, uint3
     const uint32_t xl = x - g.xbase;
     const uint32_t col = g.divN.div(xl);
     const uint32_t v = xl - col * g.n;
-    const uint32_t cb = __ldg(g.node_ptr + v) + ch * CHUNK;
-    const uint32_t ce = min(__ldg(g.node_ptr + v + 1), cb + CHUNK);
+    const uint32_t rb = __ldg(g.node_ptr + v), re = __ldg(g.node_ptr + v + 1);
+    if (ch >= (re - rb + CHUNK - 1) / CHUNK) {  // no such chunk of the row
+        if (lane == 0) record_bad(j, x, 2);
+        return;
+    }
+    const uint32_t cb = rb + ch * CHUNK;
+    const uint32_t ce = min(re, cb + CHUNK);
     for (uint32_t q0 = cb; q0 < ce; q0 += 128) {
         uint32_t segs[4], cols[4], slot[4];
         bool ok[4];
@@ -628,6 +669,7 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j) {
     uint32_t cidx = NONE;       // held chunk slot (warp-uniform)
     uint32_t sidx = NONE;       // this lane's held short slot
     uint32_t idle = 0;          // consecutive polls without work
+    uint32_t busy = 0;          // polls with work (lane 0's count)
     for (;;) {
         bool progress = false;
         // new claims, decided by lane 0
@@ -652,7 +694,8 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j) {
             if (lane == 0 && cidx < j.qc_cap) it = ld_relaxed64(j.qc[q] + cidx);
             it = __shfl_sync(0xffffffffu, it, 0);
             if (it != EMPTY) {
-                expand_chunk<MULTI>(j, k, q, it);
+                if ((uint32_t)it < j.nx) expand_chunk<MULTI>(j, k, q, it);
+                else if (lane == 0) record_bad(j, (uint32_t)it, 3);
                 mark_processed(c, q, QC, 1);
                 cidx = NONE;
                 progress = true;
@@ -663,9 +706,11 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j) {
             uint32_t x = EMPTY32;
             if (sidx != NONE && sidx < j.qs_cap) x = __ldcg(j.qs[q] + sidx);
             const bool ready = x != EMPTY32;
+            const bool bad = ready && x >= j.nx;
+            if (bad) record_bad(j, x, 4);
             const uint32_t rmask = __ballot_sync(0xffffffffu, ready);
             if (rmask) {
-                expand_short<MULTI>(j, k, q, ready ? x : 0u, ready);
+                expand_short<MULTI>(j, k, q, ready && !bad ? x : 0u, ready && !bad);
                 if (ready) sidx = NONE;
                 mark_processed(c, q, QS, (uint32_t)__popc(rmask));
                 progress = true;
@@ -675,6 +720,14 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j) {
             t0 = global_ns();
             ns = 32;
             idle = 0;
+            // a warp that keeps finding work still ends by the run's deadline
+            uint32_t stop = 0;
+            if (lane == 0 && ((++busy & 63) == 0) &&
+                (past_deadline(j, t0) || ld_l2(&c->err) != ERR_NONE)) {
+                atomicCAS(&c->err, ERR_NONE, ERR_DEADLINE);
+                stop = 1;
+            }
+            if (__shfl_sync(0xffffffffu, stop, 0)) return;
         } else {
             // nothing ready: done when every reserved item is processed (any
             // slots still held were overclaims), else wait a little.  Only
@@ -781,7 +834,7 @@ static uint64_t shared_ws_bytes(uint64_t nx, uint64_t col_entries) {
 
 uint64_t peel_ws_bytes(uint32_t n, uint32_t L, uint64_t entries, uint32_t ncols) {
     const uint64_t nx = (uint64_t)ncols * n;
-    return shared_ws_bytes(nx, (uint64_t)ncols * entries) + 4ull * ncols * n * L;
+    return shared_ws_bytes(nx, (uint64_t)ncols * entries) + 4ull * ncols * n * L + 256;
 }
 
 // Lays the shared part of the workspace out at `w` (queues, counts, lists,
@@ -838,6 +891,7 @@ static fc_status run_job(PeelJob& j, uint32_t maxL, uint32_t threads, cudaStream
     j.idle_polls = env_u32("FC_PEEL_IDLE_POLLS", 8);
     if (!j.small_row) j.small_row = env_u32("FC_PEEL_SMALL_ROW", SMALL_ROW_DEFAULT);
     j.timeout_ns = (uint64_t)env_u32("FC_BARRIER_TIMEOUT_MS", 10000) * 1000000ull;
+    j.deadline_ns = (uint64_t)env_u32("FC_PEEL_DEADLINE_MS", 60000) * 1000000ull;
     j.trace = nullptr;
     j.trace_levels = 0;
     const bool tracing = instrument && env_u32("FC_PEEL_TRACE", 0) != 0;
@@ -918,7 +972,12 @@ static fc_status run_job(PeelJob& j, uint32_t maxL, uint32_t threads, cudaStream
                         col0, ncols, l, r[0] * 1e-3, r[3] * 1e-3, r[4] ? r[4] : r[1], r[2]);
         }
     }
-    if (out.err) return FC_ERR_ITER_LIMIT;
+    if (out.err) {
+        if (env_u32("FC_DEBUG", 0))
+            fprintf(stderr, "peel: error %u at level %u of %u (bad item %u, check %u), %u segments\n",
+                    out.err, out.err_level, j.max_level, out.bad_item, out.bad_where, j.nseg);
+        return FC_ERR_ITER_LIMIT;
+    }
     return FC_OK;
 }
 
@@ -948,8 +1007,10 @@ fc_status peel_run(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* 
     PeelJob j{};
     char* w = (char*)ws;
     char* end = w + ws_bytes;
-    uint32_t* deg = (uint32_t*)w;  // ncols * n * L at the start (4-byte aligned)
+    uint32_t* deg = (uint32_t*)w;  // ncols * n * L at the start
     w += 4ull * ncols * g.n * g.L;
+    // the chunk queues hold 8-byte items: start them on a 256-byte boundary
+    w = (char*)(((uintptr_t)w + 255) & ~(uintptr_t)255);
     fc_status rc;
     carve_shared(j, w, end, nx, (uint64_t)ncols * g.entries, s, &rc);
     FC_TRY(rc);
