@@ -45,7 +45,8 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3"])
+    ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--beta", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -342,6 +343,78 @@ def run_ours(args, world, rank, local):
     print(json.dumps(line))
 
 
+def run_batch(args, world, rank, local):
+    """The 256-graph mix: every (graph, lambda) column in one persistent launch
+    (batched form) against one graph and one column per launch (plain form),
+    same graphs, tables compared.  Each rank takes every world-th graph."""
+    import torch
+    from concurrent.futures import ThreadPoolExecutor
+    from pargridcpu_b200 import MultilayerGraph, batch_run, synth
+
+    torch.cuda.set_device(local)
+    t0 = time.time()
+    gens =synth.batch_mix(count=args.batch_count, seed=404, workers=os.cpu_count() or 1)[rank::world]
+    with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+        graphs = list(ex.map(lambda g: MultilayerGraph.from_pairs(g.layers), gens))
+    del gens
+    gen_s = time.time() - t0
+    for g in graphs:
+        g.upload()
+    visits = sum(int(g.layer_m().sum()) * g.L for g in graphs)
+    stream = torch.cuda.Stream()
+
+    def timed(**kw):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        tables, res, rep = batch_run(graphs, beta=args.beta, want_tables=False, stream=stream, **kw)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), res, rep
+
+    timed()  # autotunes and warms up
+    for _ in range(max(0, args.warmup - 1)):
+        timed()
+    clocks = Clocks(local)
+    clocks.start()
+    batched = [timed() for _ in range(args.steps)]
+    clk = clocks.stop()
+    plain_ms, plain_res, plain_rep = timed(plain=True)
+    b_ms = statistics.mean(b[0] for b in batched)
+    same = all(a == b for a, b in zip(batched[-1][1], plain_res))
+    tb, _, _ = batch_run(graphs, beta=args.beta)
+    tp, _, _ = batch_run(graphs, beta=args.beta, plain=True)
+    same = same and all(np.array_equal(a, b) for a, b in zip(tb, tp))
+    ms = b_ms
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([b_ms, plain_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, plain_ms = float(t[0]), float(t[1])
+        v = torch.tensor([float(visits)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(v)
+        visits = int(v.item())
+    if rank != 0:
+        return
+    rep = batched[-1][2]
+    line = {"metric": METRIC, "value": visits / (ms / 1e3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded; shapes of the named configuration)",
+            "config": {"workload": f"c4: {args.batch_count} Chung-Lu graphs, n log-uniform "
+                                   "[1k,200k], L uniform [2,24], mean layer degree log-uniform "
+                                   "[2,32], gamma U[2,3], copy U[0,0.6], seed 404; full fcgrid "
+                                   "+ densest(beta) per graph",
+                       "graphs": len(graphs), "edge_visits_per_step": visits, "beta": args.beta,
+                       "parallelism": "graphs split over ranks" if world > 1 else "single GPU"},
+            "batched": {"ms": ms, "report": rep},
+            "plain": {"ms": plain_ms, "report": plain_rep,
+                      "form": "one graph and one lambda column per launch, one after another"},
+            "speedup_batched_vs_plain": plain_ms / ms, "identical_results": bool(same),
+            "clocks": clk, "setup_s": gen_s}
+    print(json.dumps(line))
+
+
 def main():
     args = parse_args()
     world, rank, local = dist_setup()
@@ -349,6 +422,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.workload == "c4":
+            run_batch(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -179,18 +179,15 @@ def config_graph(name, scale=1.0, seed=None):
     return erdos_renyi_graph(c["n"], c["L"], c["p_lo"], c["p_hi"], c["seed"], name=name)
 
 
-def batch_mix(count=256, seed=404, n_lo=1_000, n_hi=200_000, large_frac=0.0, large=None):
-    """The uneven batch: per graph n log-uniform in [n_lo, n_hi], L uniform in
-    [2, 24], mean per-layer degree log-uniform in [2, 32], gamma ~ U[2, 3], copy
-    ~ U[0, 0.6].  With ``large_frac`` > 0 that share of graphs is drawn from
-    ``large`` (a CONFIGS-style dict) instead."""
+def batch_params(count=256, seed=404, n_lo=1_000, n_hi=200_000, large_frac=0.0, large=None):
+    """The per-graph parameters of batch_mix (cheap; no graph is built)."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
         if large_frac > 0 and rng.random() < large_frac:
             c = large or CONFIGS["c5_large"]
-            out.append(chung_lu_graph(c["n"], c["L"], c["m"], c["gamma"], c["copy"],
-                                      int(rng.integers(1 << 30)), name=f"large{i}"))
+            out.append(dict(n=c["n"], n_layers=c["L"], m_per_layer=c["m"], gamma=c["gamma"],
+                            copy=c["copy"], seed=int(rng.integers(1 << 30)), name=f"large{i}"))
             continue
         n = int(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi))))
         L = int(rng.integers(2, 25))
@@ -198,9 +195,29 @@ def batch_mix(count=256, seed=404, n_lo=1_000, n_hi=200_000, large_frac=0.0, lar
         gamma = float(rng.uniform(2.0, 3.0))
         copy = float(rng.uniform(0.0, 0.6))
         m = max(1, int(n * deg / 2))
-        out.append(chung_lu_graph(n, L, m, gamma, copy, int(rng.integers(1 << 30)),
-                                  name=f"g{i}"))
+        out.append(dict(n=n, n_layers=L, m_per_layer=m, gamma=gamma, copy=copy,
+                        seed=int(rng.integers(1 << 30)), name=f"g{i}"))
     return out
+
+
+def _make(p):
+    return chung_lu_graph(**p)
+
+
+def batch_mix(count=256, seed=404, n_lo=1_000, n_hi=200_000, large_frac=0.0, large=None,
+              workers=0):
+    """The uneven batch: per graph n log-uniform in [n_lo, n_hi], L uniform in
+    [2, 24], mean per-layer degree log-uniform in [2, 32], gamma ~ U[2, 3], copy
+    ~ U[0, 0.6].  With ``large_frac`` > 0 that share of graphs is drawn from
+    ``large`` (a CONFIGS-style dict) instead.  Each graph has its own seed, so
+    ``workers`` > 1 (a spawned process pool) builds the same graphs."""
+    params = batch_params(count, seed, n_lo, n_hi, large_frac, large)
+    if workers and workers > 1 and count > 1:
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        with ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+            return list(ex.map(_make, params, chunksize=1))
+    return [_make(p) for p in params]
 
 
 # ---- files -----------------------------------------------------------------
