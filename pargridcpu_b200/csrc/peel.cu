@@ -63,7 +63,7 @@ enum : uint32_t { QS = 0, QC = 1 };
 // rows longer than the job's small_row entries are expanded as CHUNK-entry
 // work items
 constexpr uint32_t SMALL_ROW_DEFAULT = 32;
-constexpr uint32_t CHUNK = 128;
+constexpr uint32_t CHUNK = 256;
 
 // A counter alone on its 128-byte line: the queue counters are hit by atomics
 // and polls from every SM, and must not share a line with each other.
@@ -105,14 +105,15 @@ struct PeelJob {
     const SegP* segs;              // nseg segments (device), when more than one
     const uint32_t* seg_xbase;     // nseg + 1 (device): segment starts, then nx
     uint32_t nseg, nx;
-    uint32_t* cnt;                 // nx
+    uint32_t* cnt;                 // nx: layers with degree >= level+1, kept for alive x
     uint32_t* alive[2];            // each nx
+    uint32_t* bits;                // (nx + 31) / 32: bit x set while x is not removed
     uint32_t* qs[2];               // short-row node items, EMPTY32 when unwritten
     unsigned long long* qc[2];     // chunk items, EMPTY when unwritten
     uint32_t qs_cap, qc_cap;
     PeelCtl* ctl;
     uint32_t max_level;
-    uint32_t idle_polls;  // empty polls after which a non-polling warp leaves DRAIN
+    uint32_t idle_polls;  // empty polls after which a warp other than warp 0 parks
     uint32_t small_row;   // longest row queued as one item; longer rows go in chunks
     uint64_t timeout_ns;  // longest wait without progress
     uint64_t deadline_ns; // longest whole run
@@ -150,6 +151,16 @@ __device__ __forceinline__ uint64_t global_ns() {
 __device__ __forceinline__ uint32_t ld_l2(const uint32_t* p) { return __ldcg(p); }
 __device__ __forceinline__ uint64_t ld_l2_64(const uint64_t* p) {
     return __ldcg((const unsigned long long*)p);
+}
+
+// The alive bitmap: one bit per x, cleared once when x is removed.  It is
+// small enough to stay in L2, so the "is the neighbour still alive" test of
+// every visit is an L2 hit rather than a DRAM read of cnt.
+__device__ __forceinline__ uint32_t is_alive(const PeelJob& j, uint32_t x) {
+    return (ld_l2(j.bits + (x >> 5)) >> (x & 31)) & 1u;
+}
+__device__ __forceinline__ void clear_alive(const PeelJob& j, uint32_t x) {
+    atomicAnd(j.bits + (x >> 5), ~(1u << (x & 31)));
 }
 
 // ---- segments ---------------------------------------------------------------
@@ -329,14 +340,21 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v) {
     return v;
 }
 
-// Count of the L values row[0..L) that are >= thr, by a group of G lanes (G a
-// power of two; all 32 lanes of the warp call this together, each group with
-// its own row and L).  Every lane of a group returns the group's count.
+// Count of the L values row[0..L) that are >= thr, by a group of G lanes (G 1
+// or 32; all 32 lanes of the warp call this together, each group with its own
+// row and L).  Every lane of a group returns the group's count.
 template <int G>
 __device__ __forceinline__ uint32_t group_count_ge(const uint32_t* row, uint32_t L, uint32_t thr,
                                                    bool live) {
-    const uint32_t gl = (threadIdx.x & 31) & (G - 1);
     uint32_t cnt = 0;
+    if (G == 1) {  // one lane per node: its L loads are independent
+        if (live) {
+#pragma unroll 8
+            for (uint32_t li = 0; li < L; li++) cnt += ld_l2(row + li) >= thr;
+        }
+        return cnt;
+    }
+    const uint32_t gl = (threadIdx.x & 31) & (G - 1);
     if (live)
         for (uint32_t li = gl; li < L; li += G) cnt += ld_l2(row + li) >= thr;
 #pragma unroll
@@ -344,48 +362,14 @@ __device__ __forceinline__ uint32_t group_count_ge(const uint32_t* row, uint32_t
     return cnt;
 }
 
-// Up to four removed-neighbour slots per lane at once (loads first, then the
-// atomics) so each lane keeps several memory operations in flight.  Entry i is
-// slot slot[i] of column col[i] of segment seg[i].  All 32 lanes call it
-// together; the nodes it removes are queued with one reservation per queue
-// for the whole warp.
-template <bool MULTI>
-__device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&seg)[4],
-                                       const uint32_t (&col)[4], const uint32_t (&slot)[4],
-                                       const bool (&ok)[4], uint32_t k, uint32_t q) {
-    uint32_t yl[4], yg[4], cy[4], old[4], lmd[4];
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const SegP g = seg_load<MULTI>(j, seg[i]);
-        yl[i] = col[i] * g.n + g.divL.div(slot[i]);  // within the segment
-        yg[i] = g.xbase + yl[i];                      // in the launch
-        lmd[i] = g.col0 + col[i] + 1;
-        cy[i] = ok[i] ? ld_l2(j.cnt + yg[i]) : 0u;
-    }
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        old[i] = 0u;
-        if (ok[i] && cy[i] >= lmd[i]) {
-            const SegP g = seg_load<MULTI>(j, seg[i]);
-            old[i] = atomicSub(g.deg + (uint64_t)col[i] * g.nL + slot[i], 1u);
-        }
-    }
-    bool rem[4];
-    uint32_t nch[4], my_s = 0, my_c = 0;
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        rem[i] = false;
-        if (ok[i] && cy[i] >= lmd[i] && old[i] == k + 1)
-            rem[i] = atomicSub(j.cnt + yg[i], 1u) == lmd[i];
-        nch[i] = 0;
-        if (rem[i]) {
-            const SegP g = seg_load<MULTI>(j, seg[i]);
-            g.t[yl[i]] = k;
-            nch[i] = chunks_of(g, yl[i] - col[i] * g.n, j.small_row);
-            my_s += nch[i] == 0;
-            my_c += nch[i];
-        }
-    }
+// Queues the nodes this warp's lanes removed (rem[i]: launch index yg[i],
+// nch[i] chunk items or one short item when 0), with one reservation per
+// queue for the whole warp.  my_s / my_c are the lane's short / chunk item
+// counts.  All 32 lanes call it together.
+template <int N>
+__device__ __forceinline__ void enqueue_removed(const PeelJob& j, uint32_t q, const bool (&rem)[N],
+                                                const uint32_t (&yg)[N], const uint32_t (&nch)[N],
+                                                uint32_t my_s, uint32_t my_c) {
     if (!__any_sync(0xffffffffu, (my_s | my_c) != 0)) return;
     const uint32_t is = warp_incl_scan(my_s);
     const uint32_t ic = warp_incl_scan(my_c);
@@ -397,7 +381,7 @@ __device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&seg)[4
     bs = __shfl_sync(0xffffffffu, bs, 31) + is - my_s;
     bc = __shfl_sync(0xffffffffu, bc, 31) + ic - my_c;
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
+    for (int i = 0; i < N; i++) {
         if (rem[i]) {
             if (nch[i] == 0) write_short(j, q, bs++, yg[i]);
             else {
@@ -406,6 +390,92 @@ __device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&seg)[4
             }
         }
     }
+}
+
+// Up to four removed-neighbour slots per lane at once (loads first, then the
+// atomics) so each lane keeps several memory operations in flight.  Entry i is
+// slot slot[i] of column col[i] of segment seg[i] (entries of different nodes:
+// the short-row path).  All 32 lanes call it together.
+//
+// An entry is skipped when its neighbour is already removed (alive bit
+// clear).  A neighbour removed concurrently may still take a decrement; that
+// is harmless: its degrees are never read again, and its count is already
+// below lambda, so the count crossing that queues a node cannot recur.
+template <bool MULTI>
+__device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&seg)[4],
+                                       const uint32_t (&col)[4], const uint32_t (&slot)[4],
+                                       const bool (&ok)[4], uint32_t k, uint32_t q) {
+    uint32_t yl[4], yg[4], cy[4], old[4], lmd[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const SegP g = seg_load<MULTI>(j, seg[i]);
+        yl[i] = col[i] * g.n + g.divL.div(slot[i]);  // within the segment
+        yg[i] = g.xbase + yl[i];                      // in the launch
+        lmd[i] = g.col0 + col[i] + 1;
+        cy[i] = ok[i] ? is_alive(j, yg[i]) : 0u;
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        old[i] = 0u;
+        if (cy[i]) {
+            const SegP g = seg_load<MULTI>(j, seg[i]);
+            old[i] = atomicSub(g.deg + (uint64_t)col[i] * g.nL + slot[i], 1u);
+        }
+    }
+    bool rem[4];
+    uint32_t nch[4], my_s = 0, my_c = 0;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        rem[i] = false;
+        if (cy[i] && old[i] == k + 1) rem[i] = atomicSub(j.cnt + yg[i], 1u) == lmd[i];
+        nch[i] = 0;
+        if (rem[i]) {
+            const SegP g = seg_load<MULTI>(j, seg[i]);
+            clear_alive(j, yg[i]);
+            g.t[yl[i]] = k;
+            nch[i] = chunks_of(g, yl[i] - col[i] * g.n, j.small_row);
+            my_s += nch[i] == 0;
+            my_c += nch[i];
+        }
+    }
+    enqueue_removed<4>(j, q, rem, yg, nch, my_s, my_c);
+}
+
+// The same for N entries per lane that all belong to one node (a chunk of a
+// long row): the segment and column are shared, so they are loaded once and
+// each lane can keep more entries in flight.
+template <int N>
+__device__ __forceinline__ void visit_node(const PeelJob& j, const SegP& g, uint32_t col,
+                                           const uint32_t (&slot)[N], const bool (&ok)[N],
+                                           uint32_t k, uint32_t q) {
+    const uint32_t lmd = g.col0 + col + 1;
+    const uint32_t cb = col * g.n;
+    uint32_t* const deg = g.deg + (uint64_t)col * g.nL;
+    uint32_t yg[N], cy[N], old[N];
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        yg[i] = g.xbase + cb + g.divL.div(slot[i]);
+        cy[i] = ok[i] ? is_alive(j, yg[i]) : 0u;
+    }
+#pragma unroll
+    for (int i = 0; i < N; i++) old[i] = cy[i] ? atomicSub(deg + slot[i], 1u) : 0u;
+    bool rem[N];
+    uint32_t nch[N], my_s = 0, my_c = 0;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        rem[i] = false;
+        if (cy[i] && old[i] == k + 1) rem[i] = atomicSub(j.cnt + yg[i], 1u) == lmd;
+        nch[i] = 0;
+        if (rem[i]) {
+            const uint32_t yl = yg[i] - g.xbase;
+            clear_alive(j, yg[i]);
+            g.t[yl] = k;
+            nch[i] = chunks_of(g, yl - cb, j.small_row);
+            my_s += nch[i] == 0;
+            my_c += nch[i];
+        }
+    }
+    enqueue_removed<N>(j, q, rem, yg, nch, my_s, my_c);
 }
 
 // ---- phases ---------------------------------------------------------------
@@ -428,9 +498,9 @@ __device__ __forceinline__ void scan_nodes(const PeelJob& j, const uint32_t* src
         const uint32_t idx = base + threadIdx.x / G;
         bool live = idx < cnt_nodes;
         const uint32_t x = live ? (src ? ld_l2(src + idx) : idx) : 0;
+        if (live && src && !is_alive(j, x)) live = false;  // removed in the last drain
         const SegP g = seg_load<MULTI>(j, seg_of<MULTI>(j, x));
         const uint32_t xl = x - g.xbase;
-        if (live && src && ld_l2(g.t + xl) != UNSET) live = false;  // removed last level
         const uint32_t c = g.divN.div(xl);
         const uint32_t v = xl - c * g.n;
         const uint32_t cnt = group_count_ge<G>(g.deg + (uint64_t)c * g.nL + (uint64_t)v * g.L, g.L,
@@ -440,10 +510,12 @@ __device__ __forceinline__ void scan_nodes(const PeelJob& j, const uint32_t* src
         const bool keep = lead && !remove;
         const uint32_t nch = remove ? chunks_of(g, v, j.small_row) : 0u;
         const uint32_t ns = (remove && nch == 0) ? 1u : 0u;
-        if (lead) {
+        if (remove) {
+            clear_alive(j, x);
+            g.t[xl] = k;
+        } else if (keep) {
             j.cnt[x] = cnt;
-            if (remove) g.t[xl] = k;
-            else if (!src) g.t[xl] = UNSET;
+            if (!src) g.t[xl] = UNSET;
         }
         const uint32_t kin = warp_incl_scan(keep ? 1u : 0u);
         const uint32_t sin = warp_incl_scan(ns);
@@ -555,15 +627,23 @@ __device__ __noinline__ void record_bad(const PeelJob& j, uint32_t item, uint32_
     }
 }
 
-// Count `n` of this warp's items of kind s as processed.  The items the warp
-// queued while processing them were reserved (tail raised) before this, so
-// the sums of level_done cannot meet early.
-__device__ __forceinline__ void mark_processed(PeelCtl* c, uint32_t q, uint32_t s, uint32_t n) {
+// Adds this warp's processed-item counts (ps short, pc chunk items; warp
+// uniform) to the grid-wide ones and clears them.  The items the warp queued
+// while processing them were reserved (tail raised, by returning atomics)
+// before the fence, so the sums of level_done cannot meet early.  Counts are
+// flushed in batches -- the fence is the expensive part -- and always before
+// the warp polls for the end of the level, so they only ever lag.
+__device__ __forceinline__ void flush_processed(PeelCtl* c, uint32_t q, uint32_t& ps,
+                                                uint32_t& pc) {
+    if ((ps | pc) == 0) return;
     __syncwarp();
     if ((threadIdx.x & 31) == 0) {
         __threadfence();
-        atomicAdd(&c->processed[q][s].v, n);
+        if (ps) atomicAdd(&c->processed[q][QS].v, ps);
+        if (pc) atomicAdd(&c->processed[q][QC].v, pc);
     }
+    ps = 0;
+    pc = 0;
 }
 
 // Short rows of the lanes with `ready` set (at most small_row entries each),
@@ -618,14 +698,15 @@ __device__ __forceinline__ void expand_short(const PeelJob& j, uint32_t k, uint3
     }
 }
 
-// One CHUNK-entry piece of a long row, by the whole warp.
+// One CHUNK-entry piece of a long row, by the whole warp (CHUNK / 32 entries
+// per lane).
 template <bool MULTI>
 __device__ __forceinline__ void expand_chunk(const PeelJob& j, uint32_t k, uint32_t q,
                                              unsigned long long it) {
+    constexpr int PER_LANE = CHUNK / 32;
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t x = (uint32_t)it, ch = (uint32_t)(it >> 32);
-    const uint32_t s = seg_of<MULTI>(j, x);
-    const SegP g = seg_load<MULTI>(j, s);
+    const SegP g = seg_load<MULTI>(j, seg_of<MULTI>(j, x));
     const uint32_t xl = x - g.xbase;
     const uint32_t col = g.divN.div(xl);
     const uint32_t v = xl - col * g.n;
@@ -636,19 +717,49 @@ __device__ __forceinline__ void expand_chunk(const PeelJob& j, uint32_t k, uint3
     }
     const uint32_t cb = rb + ch * CHUNK;
     const uint32_t ce = min(re, cb + CHUNK);
-    for (uint32_t q0 = cb; q0 < ce; q0 += 128) {
-        uint32_t segs[4], cols[4], slot[4];
-        bool ok[4];
+    uint32_t slot[PER_LANE];
+    bool ok[PER_LANE];
 #pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const uint32_t p = q0 + lane + 32 * i;
-            ok[i] = p < ce;
-            slot[i] = ok[i] ? __ldg(g.adj + p) : 0u;
-            cols[i] = col;
-            segs[i] = s;
-        }
-        visit4<MULTI>(j, segs, cols, slot, ok, k, q);
+    for (int i = 0; i < PER_LANE; i++) {
+        const uint32_t p = cb + lane + 32 * i;
+        ok[i] = p < ce;
+        slot[i] = ok[i] ? __ldg(g.adj + p) : 0u;
     }
+    visit_node<PER_LANE>(j, g, col, slot, ok, k, q);
+}
+
+// Per-block drain state in shared memory: `done` is set when the level is
+// over (or the run failed), `wake` is bumped by warp 0 whenever it sees more
+// unclaimed queue items than it takes itself.
+struct DrainBlock {
+    uint32_t done, wake;
+};
+
+// An idle warp holding no claim parks on its block's shared state instead of
+// polling the grid-wide queue counters: it resumes claiming when warp 0 sees
+// unclaimed work, and leaves DRAIN when the level is over.  Returns true to
+// leave.  Bounded by the run's deadline.
+__device__ __forceinline__ bool park(const PeelJob& j, volatile DrainBlock* sb) {
+    uint32_t r = 0;
+    if ((threadIdx.x & 31) == 0) {
+        const uint32_t w0 = sb->wake;
+        for (uint32_t spins = 1;; spins++) {
+            if (sb->done) {
+                r = 1;
+                break;
+            }
+            if (sb->wake != w0) break;
+            __nanosleep(256);
+            if ((spins & 255) == 0 &&
+                (past_deadline(j, global_ns()) || ld_l2(&j.ctl->err) != ERR_NONE)) {
+                atomicCAS(&j.ctl->err, ERR_NONE, ERR_DEADLINE);
+                sb->done = 1;
+                r = 1;
+                break;
+            }
+        }
+    }
+    return __shfl_sync(0xffffffffu, r, 0) != 0;
 }
 
 // DRAIN(K): each warp holds at most one chunk claim (one item) and one
@@ -658,11 +769,12 @@ __device__ __forceinline__ void expand_chunk(const PeelJob& j, uint32_t k, uint3
 // such a slot is either filled by a later removal or abandoned when the level
 // completes -- meanwhile the warp keeps serving the other queue.
 template <bool MULTI>
-__device__ __forceinline__ void phase_drain(const PeelJob& j) {
+__device__ __forceinline__ void phase_drain(const PeelJob& j, volatile DrainBlock* sb) {
     PeelCtl* c = j.ctl;
     const uint32_t k = ld_l2(&c->level);
     const uint32_t q = ld_l2(&c->q_cur);
     const uint32_t lane = threadIdx.x & 31;
+    const bool warp0 = (threadIdx.x >> 5) == 0;
     constexpr uint32_t NONE = 0xFFFFFFFFu;
     uint64_t t0 = global_ns();  // last progress of this warp
     uint32_t ns = 32;
@@ -670,24 +782,29 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j) {
     uint32_t sidx = NONE;       // this lane's held short slot
     uint32_t idle = 0;          // consecutive polls without work
     uint32_t busy = 0;          // polls with work (lane 0's count)
+    uint32_t pend_s = 0, pend_c = 0;  // processed items not yet flushed
     for (;;) {
         bool progress = false;
         // new claims, decided by lane 0
-        uint32_t want = 0, cb = NONE, sb = NONE;
+        uint32_t want = 0, cb = NONE, sbase = NONE;
         const bool hold_s = __any_sync(0xffffffffu, sidx != NONE);
         if (lane == 0) {
-            if (cidx == NONE && ld_l2(&c->tail[q][QC].v) > ld_l2(&c->head[q][QC].v)) {
+            const uint32_t tc = ld_l2(&c->tail[q][QC].v), hc = ld_l2(&c->head[q][QC].v);
+            const uint32_t ts = ld_l2(&c->tail[q][QS].v), hs = ld_l2(&c->head[q][QS].v);
+            if (cidx == NONE && tc > hc) {
                 cb = atomicAdd(&c->head[q][QC].v, 1u);
                 want |= 1;
             }
-            if (!hold_s && ld_l2(&c->tail[q][QS].v) > ld_l2(&c->head[q][QS].v)) {
-                sb = atomicAdd(&c->head[q][QS].v, 32u);
+            if (!hold_s && ts > hs) {
+                sbase = atomicAdd(&c->head[q][QS].v, 32u);
                 want |= 2;
             }
+            // more unclaimed items than this warp takes: wake the parked warps
+            if (warp0 && (tc > hc + 1 || ts > hs + 32)) sb->wake = sb->wake + 1;
         }
         want = __shfl_sync(0xffffffffu, want, 0);
         if (want & 1) cidx = __shfl_sync(0xffffffffu, cb, 0);
-        if (want & 2) sidx = __shfl_sync(0xffffffffu, sb, 0) + lane;
+        if (want & 2) sidx = __shfl_sync(0xffffffffu, sbase, 0) + lane;
         // a ready chunk item
         if (cidx != NONE) {
             unsigned long long it = EMPTY;
@@ -696,7 +813,7 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j) {
             if (it != EMPTY) {
                 if ((uint32_t)it < j.nx) expand_chunk<MULTI>(j, k, q, it);
                 else if (lane == 0) record_bad(j, (uint32_t)it, 3);
-                mark_processed(c, q, QC, 1);
+                pend_c += 1;
                 cidx = NONE;
                 progress = true;
             }
@@ -712,11 +829,12 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j) {
             if (rmask) {
                 expand_short<MULTI>(j, k, q, ready && !bad ? x : 0u, ready && !bad);
                 if (ready) sidx = NONE;
-                mark_processed(c, q, QS, (uint32_t)__popc(rmask));
+                pend_s += (uint32_t)__popc(rmask);
                 progress = true;
             }
         }
         if (progress) {
+            if (pend_s + pend_c >= 16) flush_processed(c, q, pend_s, pend_c);
             t0 = global_ns();
             ns = 32;
             idle = 0;
@@ -725,20 +843,30 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j) {
             if (lane == 0 && ((++busy & 63) == 0) &&
                 (past_deadline(j, t0) || ld_l2(&c->err) != ERR_NONE)) {
                 atomicCAS(&c->err, ERR_NONE, ERR_DEADLINE);
+                sb->done = 1;
                 stop = 1;
             }
             if (__shfl_sync(0xffffffffu, stop, 0)) return;
         } else {
             // nothing ready: done when every reserved item is processed (any
-            // slots still held were overclaims), else wait a little.  Only
-            // warp 0 of a block keeps polling for the whole level; the other
-            // warps, once idle for a while and holding no claim, leave to wait
-            // at the block barrier, so that idle warps do not flood the queue
+            // slots still held were overclaims), else wait a little.  Warp 0
+            // keeps polling the grid-wide counters for the whole level; the
+            // other warps, once idle for a while and holding no claim, park
+            // on the block's shared state so that idle warps do not flood the
             // counters with polls.
-            if (wait_check(j, q, t0)) return;
-            if (++idle >= j.idle_polls && (threadIdx.x >> 5) != 0 && cidx == NONE &&
-                !__any_sync(0xffffffffu, sidx != NONE))
+            flush_processed(c, q, pend_s, pend_c);
+            if (wait_check(j, q, t0)) {
+                if (lane == 0) sb->done = 1;
                 return;
+            }
+            if (!warp0 && ++idle >= j.idle_polls && cidx == NONE &&
+                !__any_sync(0xffffffffu, sidx != NONE)) {
+                if (park(j, sb)) return;
+                idle = 0;
+                ns = 32;
+                t0 = global_ns();
+                continue;
+            }
             __nanosleep(ns);
             if (ns < 512) ns <<= 1;
         }
@@ -749,15 +877,22 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j) {
 // at most 64 registers a thread.
 template <int G, int T, bool MULTI>
 __global__ void __launch_bounds__(T, 1024 / T) k_peel(PeelJob j) {
+    __shared__ DrainBlock s_drain;
     phase_init<MULTI>(j);
     if (!grid_barrier(j)) return;
     phase_scan<G, MULTI>(j, true);
     if (!grid_barrier(j)) return;
     for (;;) {
         const uint32_t ph = ld_l2(&j.ctl->phase);
-        if (ph == PH_DRAIN) phase_drain<MULTI>(j);
-        else if (ph == PH_SCAN) phase_scan<G, MULTI>(j, false);
-        else return;
+        if (ph == PH_DRAIN) {
+            if (threadIdx.x == 0) s_drain = DrainBlock{0u, 0u};
+            __syncthreads();
+            phase_drain<MULTI>(j, &s_drain);
+        } else if (ph == PH_SCAN) {
+            phase_scan<G, MULTI>(j, false);
+        } else {
+            return;
+        }
         if (!grid_barrier(j)) return;
     }
 }
@@ -805,14 +940,11 @@ static fc_status launch_g(PeelJob& j, uint32_t threads, cudaStream_t s) {
     return launch_t<G, 512, MULTI>(j, s);
 }
 
-// Group of G lanes per node in SCAN: the smallest power of two >= L, at most 32.
+// Lanes per node in SCAN: one when every segment has at most 32 layers (its L
+// loads are independent), else a group of 32.
 template <bool MULTI>
 static fc_status launch(PeelJob& j, uint32_t maxL, uint32_t threads, cudaStream_t s) {
-    if (maxL <= 1) return launch_g<1, MULTI>(j, threads, s);
-    if (maxL <= 2) return launch_g<2, MULTI>(j, threads, s);
-    if (maxL <= 4) return launch_g<4, MULTI>(j, threads, s);
-    if (maxL <= 8) return launch_g<8, MULTI>(j, threads, s);
-    if (maxL <= 16) return launch_g<16, MULTI>(j, threads, s);
+    if (maxL <= 32) return launch_g<1, MULTI>(j, threads, s);
     return launch_g<32, MULTI>(j, threads, s);
 }
 
@@ -828,8 +960,8 @@ static void queue_caps(uint64_t nx, uint64_t col_entries, uint64_t* qs_cap, uint
 static uint64_t shared_ws_bytes(uint64_t nx, uint64_t col_entries) {
     uint64_t qs_cap, qc_cap;
     queue_caps(nx, col_entries, &qs_cap, &qc_cap);
-    // qc0 qc1 (u64) | qs0 qs1 | cnt alive0 alive1 | control block (256-aligned)
-    return 4 * (4 * qc_cap + 2 * qs_cap + 3 * nx) + sizeof(PeelCtl) + 256;
+    // qc0 qc1 (u64) | qs0 qs1 | bits | cnt alive0 alive1 | control block (256-aligned)
+    return 4 * (4 * qc_cap + 2 * qs_cap + (nx + 31) / 32 + 3 * nx) + sizeof(PeelCtl) + 256;
 }
 
 uint64_t peel_ws_bytes(uint32_t n, uint32_t L, uint64_t entries, uint32_t ncols) {
@@ -857,6 +989,8 @@ static char* carve_shared(PeelJob& j, char* w, char* end, uint64_t nx, uint64_t 
     p += qs_cap;
     j.qs[1] = p;
     p += qs_cap;
+    j.bits = p;
+    p += (nx + 31) / 32;
     j.qc_cap = (uint32_t)qc_cap;
     j.qs_cap = (uint32_t)qs_cap;
     j.nx = (uint32_t)nx;
@@ -876,10 +1010,11 @@ static char* carve_shared(PeelJob& j, char* w, char* end, uint64_t nx, uint64_t 
 }
 
 // Launches the prepared job and reads its control block back.
-// Every queue slot starts EMPTY (qc and qs are contiguous); the control block
-// starts all zero, which is phase INIT.
+// Every queue slot starts EMPTY and every x alive (qc, qs and the bitmap are
+// contiguous); the control block starts all zero, which is phase INIT.
 static fc_status reset_job(const PeelJob& j, cudaStream_t s) {
-    FC_CUDA_TRY(cudaMemsetAsync(j.qc[0], 0xFF, (4ull * j.qc_cap + 2ull * j.qs_cap) * 4, s));
+    const uint64_t words = 4ull * j.qc_cap + 2ull * j.qs_cap + (j.nx + 31ull) / 32;
+    FC_CUDA_TRY(cudaMemsetAsync(j.qc[0], 0xFF, words * 4, s));
     FC_CUDA_TRY(cudaMemsetAsync(j.ctl, 0, sizeof(PeelCtl), s));
     return FC_OK;
 }
