@@ -166,7 +166,7 @@ fc_status fc_cells(fc_graph* g, double beta, fc_cell* cells, uint32_t cap, uint3
 typedef struct fc_batch_options {
     uint32_t block_threads;    /* 512 or 1024 threads per block; 0 = autotuned */
     uint32_t hub_threshold;    /* longest row queued as one work item (longer rows are
-                                  split in 128-entry pieces); 0 = autotuned */
+                                  split in 256-entry pieces); 0 = autotuned */
     int use_cuda_graph;        /* capture the batched launch in a CUDA graph */
     int plain;                 /* 1 = the one-column-per-launch baseline */
 } fc_batch_options;
@@ -188,28 +188,63 @@ fc_status fc_batch_run(fc_graph* const* graphs, uint32_t count, double beta,
                        const fc_batch_options* opt, fc_batch_report* report, void* stream);
 
 /* ---- serving -------------------------------------------------------------
- * A continuous-batching request loop: requests (a graph + beta) are admitted
- * while their device footprint fits the budget and a slot is free, their work
- * overlaps on the device with requests already running, and each completes
- * independently.  Results are identical to fc_coreindex + fc_densest on the
- * graph alone. */
+ * A continuous-batching request loop.  Requests (a graph + beta) queue in
+ * arrival order; each of `lanes` lanes (a host thread and a stream) that is
+ * free takes every pending request that fits and runs them as one batch --
+ * one persistent peel launch over their graphs, whose grid covers SMs/lanes
+ * SMs, then their densest searches -- so requests that arrive while batches
+ * are on the device join the next batch as a lane and memory free up, and
+ * the batches of different lanes overlap on the device.  A request is
+ * admitted while the device bytes of resident graphs plus running batches
+ * stay within the budget; graphs stay resident between requests and the
+ * least recently used ones that no batch is using are released when memory
+ * is short.  Each result is identical to fc_coreindex + fc_densest on the
+ * graph alone.  The plain form (one lane, one request at a time, one lambda
+ * column per launch) is the baseline it is measured against.
+ * A graph handed to a server must not be used by other calls, nor freed,
+ * while any request of it is pending; afterwards the server may release its
+ * device copy at any time (fc_graph_free is always safe once its requests
+ * have completed). */
 typedef struct fc_server fc_server;
 
 typedef struct fc_server_options {
     uint64_t hbm_budget_bytes;  /* admission budget (0 = 150 GB) */
-    uint32_t max_inflight;      /* concurrent requests on the device (0 = 16) */
+    uint32_t max_inflight;      /* requests on the device at once (0 = 256) */
+    uint32_t lanes;             /* batches on the device at once (0 = 2) */
+    uint32_t max_batch_graphs;  /* distinct graphs in one batch (0 = 64) */
+    uint32_t block_threads;     /* peel launch shape (0 = 1024 threads, */
+    uint32_t hub_threshold;     /*   rows of more than 64 entries split) */
+    int plain;                  /* 1 = the one-at-a-time baseline */
 } fc_server_options;
 
+/* Counters since fc_server_create. */
+typedef struct fc_server_stats {
+    uint64_t requests_done;
+    uint64_t batches;
+    uint64_t graphs_peeled;     /* distinct graphs over all batches */
+    uint64_t uploads;           /* device copies made */
+    uint64_t evictions;         /* resident copies released for room */
+    uint64_t resident_bytes;    /* device copies this server keeps now */
+    uint64_t peak_bytes;        /* most bytes admitted at once */
+    double busy_ms;             /* time with a batch running */
+    double overlap_ms;          /* time with two or more batches running */
+    uint32_t max_batch;         /* most requests in one batch */
+    uint32_t lanes;
+} fc_server_stats;
+
 fc_status fc_server_create(const fc_server_options* opt, fc_server** out);
-/* Enqueue a request.  The graph must stay alive until the request completes;
- * table (host, L*n, may be NULL) and res (may be NULL) are filled on
- * completion.  *ticket identifies it. */
+/* Enqueue a request.  table (host, L*n, may be NULL) and res (may be NULL)
+ * are filled on completion.  *ticket identifies it. */
 fc_status fc_server_submit(fc_server* s, fc_graph* g, double beta, uint32_t* table,
                            fc_densest_result* res, uint64_t* ticket);
 /* Wait up to timeout_ms (negative = forever) for a ticket; FC_ERR_ITER_LIMIT
- * on timeout.  *status receives the request's own status. */
+ * on timeout.  *status receives the request's own status (FC_ERR_BUDGET for a
+ * request that alone exceeds the budget); *latency_ms its time from submit to
+ * completion. */
 fc_status fc_server_wait(fc_server* s, uint64_t ticket, int64_t timeout_ms, fc_status* status,
                          double* latency_ms);
+fc_status fc_server_query(fc_server* s, fc_server_stats* out);
+/* Completes every pending request, then stops the lanes. */
 fc_status fc_server_destroy(fc_server* s);
 
 /* ---- core index without device allocation --------------------------------

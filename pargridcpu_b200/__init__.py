@@ -252,16 +252,22 @@ def batch_run(graphs, beta=1.0, want_tables=True, block_threads=0, hub_threshold
 
 
 class Server:
-    """Continuous-batching request loop (fc_server_*)."""
+    """Continuous-batching request loop (fc_server_*): requests queue in
+    arrival order, free lanes take every pending request that fits the
+    device-memory budget as one batch, and the lanes' batches overlap on the
+    device.  ``plain=True`` is the one-at-a-time baseline."""
 
-    def __init__(self, hbm_budget_bytes=0, max_inflight=0):
-        opt = _n.ServerOptions(hbm_budget_bytes, max_inflight)
+    def __init__(self, hbm_budget_bytes=0, max_inflight=0, lanes=0, max_batch_graphs=0,
+                 block_threads=0, hub_threshold=0, plain=False):
+        opt = _n.ServerOptions(hbm_budget_bytes, max_inflight, lanes, max_batch_graphs,
+                               block_threads, hub_threshold, int(plain))
         h = C.c_void_p()
         _n.check(_n.lib().fc_server_create(C.byref(opt), C.byref(h)), "server_create")
         self._h = h
         self._keep = {}
 
     def submit(self, mg: MultilayerGraph, beta=1.0, want_table=True):
+        """Queues a decomposition + densest request; returns its ticket."""
         table = np.zeros((mg.L, mg.n), np.uint32) if want_table else None
         res = _n.DensestResult()
         t = C.c_uint64()
@@ -271,6 +277,8 @@ class Server:
         return t.value
 
     def wait(self, ticket, timeout_ms=-1):
+        """(table, densest result, latency ms) of a ticket; raises FcError with
+        the request's own status when it failed."""
         st = C.c_int()
         lat = C.c_double()
         _n.check(_n.lib().fc_server_wait(self._h, ticket, timeout_ms, C.byref(st), C.byref(lat)),
@@ -278,6 +286,11 @@ class Server:
         mg, table, res = self._keep.pop(ticket)
         _n.check(st.value, "request")
         return table, res.as_dict(), lat.value
+
+    def stats(self):
+        out = _n.ServerStats()
+        _n.check(_n.lib().fc_server_query(self._h, C.byref(out)), "server_query")
+        return out.as_dict()
 
     def close(self):
         if self._h:

@@ -40,13 +40,15 @@ fc_status coreindex(fc_graph* g, uint32_t* out, bool out_on_device, cudaStream_t
     if (out) {
         uint64_t bytes = (uint64_t)d->n * d->L * 4;
         if (bytes) {
-            FC_CUDA_TRY(cudaMemcpyAsync(out, d->table, bytes,
-                                        out_on_device ? cudaMemcpyDeviceToDevice
-                                                      : cudaMemcpyDeviceToHost,
-                                        s));
-            if (!out_on_device) FC_CUDA_TRY(cudaStreamSynchronize(s));
+            if (out_on_device)
+                FC_CUDA_TRY(cudaMemcpyAsync(out, d->table, bytes, cudaMemcpyDeviceToDevice, s));
+            else
+                FC_TRY(to_host(out, d->table, bytes, s));
         }
     }
+    // every peel launch ended with a synchronize; only a device-to-device
+    // copy of the table may still be in flight
+    if (!out || !out_on_device) d->home = nullptr;
     return FC_OK;
 }
 

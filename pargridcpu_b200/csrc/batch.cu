@@ -68,7 +68,7 @@ static fc_status copy_tables(fc_graph* const* gs, uint32_t count, uint32_t* cons
         fc_graph* g = gs[i];
         const uint64_t bytes = (uint64_t)g->n * g->L * 4;
         if (tables[i] && bytes)
-            FC_CUDA_TRY(cudaMemcpyAsync(tables[i], g->dev->table, bytes, cudaMemcpyDeviceToHost, s));
+            FC_TRY(to_host(tables[i], g->dev->table, bytes, s));
     }
     FC_CUDA_TRY(cudaStreamSynchronize(s));
     return FC_OK;
@@ -81,21 +81,8 @@ static fc_status batch_plain(fc_graph* const* gs, uint32_t count, double beta,
                              fc_batch_report* rep, cudaStream_t s) {
     double peel_ms = 0;
     uint32_t launches = 0, levels = 0;
-    for (uint32_t i = 0; i < count; i++) {
-        fc_graph* g = gs[i];
-        FC_TRY(upload(g, s));
-        DeviceGraph* d = g->dev;
-        d->home = s;
-        invalidate_densest(d);
-        for (uint32_t c = 0; c < d->L && d->n; c++) {
-            PeelStats st;
-            FC_TRY(peel_columns(d, c, 1, s, &st));
-            peel_ms += st.ms;
-            launches++;
-            levels += st.levels;
-        }
-        d->table_valid = true;
-    }
+    for (uint32_t i = 0; i < count; i++)
+        FC_TRY(batch_plain_one(gs[i], s, &peel_ms, &launches, &levels));
     double dms = 0;
     FC_TRY(densest_all(gs, count, beta, res, s, &dms));
     FC_TRY(copy_tables(gs, count, tables, s));
@@ -112,10 +99,11 @@ static fc_status batch_plain(fc_graph* const* gs, uint32_t count, double beta,
 // ---- batched: segments in persistent launches --------------------------------
 
 struct TuneKey {
-    uint32_t count, maxL;
+    uint32_t count, maxL, max_sms;
     uint64_t entries_mb;
     bool operator<(const TuneKey& o) const {
-        return std::tie(count, maxL, entries_mb) < std::tie(o.count, o.maxL, o.entries_mb);
+        return std::tie(count, maxL, max_sms, entries_mb) <
+               std::tie(o.count, o.maxL, o.max_sms, o.entries_mb);
     }
 };
 static std::mutex g_tune_mu;
@@ -141,7 +129,8 @@ static void plan_groups(const std::vector<PeelSegSpec>& specs, uint64_t budget,
 static fc_status run_groups(const std::vector<PeelSegSpec>& specs,
                             const std::vector<std::pair<size_t, size_t>>& groups, void* ws,
                             uint64_t ws_bytes, cudaStream_t s, uint32_t threads, uint32_t small_row,
-                            bool want_graph, double* ms, uint32_t* levels, bool* graphed) {
+                            bool want_graph, uint32_t max_sms, double* ms, uint32_t* levels,
+                            bool* graphed) {
     *ms = 0;
     *levels = 0;
     *graphed = want_graph;
@@ -151,7 +140,7 @@ static fc_status run_groups(const std::vector<PeelSegSpec>& specs,
         bool g = want_graph;
         BATCH_TRACE("peel graphs [%zu, %zu) threads %u small_row %u graph %d", gr.first,
                     gr.second, threads, small_row, (int)g);
-        FC_TRY(peel_batch(part, ws, ws_bytes, s, &st, threads, small_row, &g));
+        FC_TRY(peel_batch(part, ws, ws_bytes, s, &st, threads, small_row, &g, max_sms));
         BATCH_TRACE("  done: %.3f ms, %u levels, cuda graph %d", st.ms, st.levels, (int)g);
         *graphed = *graphed && g;
         *ms += st.ms;
@@ -160,10 +149,23 @@ static fc_status run_groups(const std::vector<PeelSegSpec>& specs,
     return FC_OK;
 }
 
-static fc_status batch_persistent(fc_graph* const* gs, uint32_t count, double beta,
-                                  uint32_t* const* tables, fc_densest_result* res,
-                                  const fc_batch_options* opt, fc_batch_report* rep,
-                                  cudaStream_t s) {
+uint64_t batch_peel_ws_bytes(fc_graph* const* gs, uint32_t count) {
+    std::vector<PeelSegSpec> specs;
+    for (uint32_t i = 0; i < count; i++) {
+        const fc_graph* g = gs[i];
+        if (!g->n || !g->L) continue;
+        PeelSegSpec sp{};
+        sp.g.n = g->n;
+        sp.g.L = g->L;
+        sp.g.entries = g->total_entries();
+        sp.ncols = g->L;
+        specs.push_back(sp);
+    }
+    return specs.empty() ? 0 : peel_batch_ws_bytes(specs);
+}
+
+fc_status batch_peel(fc_graph* const* gs, uint32_t count, const fc_batch_options* opt,
+                     uint32_t max_sms, fc_batch_report* rep, cudaStream_t s) {
     std::vector<PeelSegSpec> specs;
     uint32_t maxL = 1;
     uint64_t entries = 0;
@@ -202,7 +204,7 @@ static fc_status batch_persistent(fc_graph* const* gs, uint32_t count, double be
     bool tuned_now = false;
     fc_status rc = FC_OK;
     if (!specs.empty() && (!threads || !small_row)) {
-        TuneKey key{count, maxL, entries >> 20};
+        TuneKey key{count, maxL, max_sms, entries >> 20};
         std::pair<uint32_t, uint32_t> best{0, 0};
         {
             std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -222,7 +224,8 @@ static fc_status batch_persistent(fc_graph* const* gs, uint32_t count, double be
                     double ms;
                     uint32_t lv;
                     bool gr;
-                    rc = run_groups(sample, sg, ws, ws_bytes, s, th, sr, false, &ms, &lv, &gr);
+                    rc = run_groups(sample, sg, ws, ws_bytes, s, th, sr, false, max_sms, &ms, &lv,
+                                    &gr);
                     if (rc != FC_OK) break;
                     if (ms < best_ms) {
                         best_ms = ms;
@@ -242,17 +245,13 @@ static fc_status batch_persistent(fc_graph* const* gs, uint32_t count, double be
     uint32_t levels = 0;
     bool graphed = false;
     if (rc == FC_OK && !specs.empty())
-        rc = run_groups(specs, groups, ws, ws_bytes, s, threads, small_row, want_graph, &peel_ms,
-                        &levels, &graphed);
+        rc = run_groups(specs, groups, ws, ws_bytes, s, threads, small_row, want_graph, max_sms,
+                        &peel_ms, &levels, &graphed);
     if (ws) dev_free(ws, s);
     FC_TRY(rc);
     for (uint32_t i = 0; i < count; i++) gs[i]->dev->table_valid = true;
-    double dms = 0;
-    FC_TRY(densest_all(gs, count, beta, res, s, &dms));
-    FC_TRY(copy_tables(gs, count, tables, s));
     if (rep) {
         rep->peel_ms = peel_ms;
-        rep->densest_ms = dms;
         rep->peel_launches = (uint32_t)groups.size();
         rep->block_threads = threads;
         rep->hub_threshold = small_row;
@@ -263,13 +262,50 @@ static fc_status batch_persistent(fc_graph* const* gs, uint32_t count, double be
     return FC_OK;
 }
 
+static fc_status batch_persistent(fc_graph* const* gs, uint32_t count, double beta,
+                                  uint32_t* const* tables, fc_densest_result* res,
+                                  const fc_batch_options* opt, fc_batch_report* rep,
+                                  cudaStream_t s) {
+    FC_TRY(batch_peel(gs, count, opt, 0, rep, s));
+    double dms = 0;
+    FC_TRY(densest_all(gs, count, beta, res, s, &dms));
+    FC_TRY(copy_tables(gs, count, tables, s));
+    if (rep) rep->densest_ms = dms;
+    return FC_OK;
+}
+
+fc_status batch_plain_one(fc_graph* g, cudaStream_t s, double* peel_ms, uint32_t* launches,
+                          uint32_t* levels) {
+    FC_TRY(upload(g, s));
+    DeviceGraph* d = g->dev;
+    d->home = s;
+    invalidate_densest(d);
+    for (uint32_t c = 0; c < d->L && d->n; c++) {
+        PeelStats st;
+        FC_TRY(peel_columns(d, c, 1, s, &st));
+        *peel_ms += st.ms;
+        *launches += 1;
+        *levels += st.levels;
+    }
+    d->table_valid = true;
+    return FC_OK;
+}
+
 fc_status batch_run(fc_graph* const* gs, uint32_t count, double beta, uint32_t* const* tables,
                     fc_densest_result* res, const fc_batch_options* opt, fc_batch_report* rep,
                     cudaStream_t s) {
     if (!cuda_available()) return FC_ERR_NO_DEVICE;
     if (rep) *rep = fc_batch_report{};
-    if (opt && opt->plain) return batch_plain(gs, count, beta, tables, res, rep, s);
-    return batch_persistent(gs, count, beta, tables, res, opt, rep, s);
+    const fc_status rc = opt && opt->plain
+                             ? batch_plain(gs, count, beta, tables, res, rep, s)
+                             : batch_persistent(gs, count, beta, tables, res, opt, rep, s);
+    // nothing of these graphs is left in flight on s afterwards
+    const cudaError_t e = cudaStreamSynchronize(s);
+    for (uint32_t i = 0; i < count; i++)
+        if (gs[i]->dev) gs[i]->dev->home = nullptr;
+    if (rc != FC_OK) return rc;
+    FC_CUDA_TRY(e);
+    return FC_OK;
 }
 
 }  // namespace fc

@@ -62,7 +62,8 @@ static fc_status grow(T*& p, uint64_t& cap, uint64_t need, cudaStream_t st) {
 void free_densest_state(DeviceGraph* d) {
     DensState* s = (DensState*)d->dens;
     if (!s) return;
-    // called with the graph's work finished (release_device synchronizes)
+    // called with the graph's work finished (release_device waits for it, or
+    // its caller knows that it has completed)
     for (void* p : {(void*)s->H, (void*)s->N, (void*)s->coreT, (void*)s->d_hbase,
                     (void*)s->d_nbase, (void*)s->d_kmax, (void*)s->cells, (void*)s->powl,
                     (void*)s->d_res, (void*)s->cell_lk})
@@ -340,8 +341,7 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st) {
     count_launch();
     FC_CUDA_TRY(cudaGetLastError());
     s->kmax.assign(L, 0);
-    FC_CUDA_TRY(cudaMemcpyAsync(s->kmax.data(), s->d_kmax, L * 4, cudaMemcpyDeviceToHost, st));
-    FC_CUDA_TRY(cudaStreamSynchronize(st));
+    FC_TRY(to_host(s->kmax.data(), s->d_kmax, L * 4, st));
     d->kmax = s->kmax;
     for (uint32_t l = 0; l < L; l++)
         if (s->kmax[l] > d->max_deg) return FC_ERR_DEVICE;  // not a valid core table
@@ -368,8 +368,8 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st) {
     FC_TRY(grow(s->d_hbase, s->hbase_cap, L + 1, st));
     FC_TRY(grow(s->d_nbase, s->nbase_cap, L + 1, st));
     if (!s->coreT) FC_TRY(dev_alloc((void**)&s->coreT, (uint64_t)n * L * 4 + 4, st));
-    FC_CUDA_TRY(cudaMemcpyAsync(s->d_hbase, s->hbase.data(), L * 8, cudaMemcpyHostToDevice, st));
-    FC_CUDA_TRY(cudaMemcpyAsync(s->d_nbase, s->nbase.data(), L * 8, cudaMemcpyHostToDevice, st));
+    FC_TRY(to_device(s->d_hbase, s->hbase.data(), L * 8, st));
+    FC_TRY(to_device(s->d_nbase, s->nbase.data(), L * 8, st));
     // cell list (lambda index, k) in the reference's order, for k_cells
     s->cell_host.resize(2 * nc + 2);
     {
@@ -381,8 +381,7 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st) {
             }
     }
     if (nc)
-        FC_CUDA_TRY(cudaMemcpyAsync(s->cell_lk, s->cell_host.data(), 2 * nc * 4,
-                                    cudaMemcpyHostToDevice, st));
+        FC_TRY(to_device(s->cell_lk, s->cell_host.data(), 2 * nc * 4, st));
     FC_CUDA_TRY(cudaMemsetAsync(s->H, 0, hw * 4 + 4, st));
     FC_CUDA_TRY(cudaMemsetAsync(s->N, 0, nw * 4 + 4, st));
     if (n && L) {
@@ -438,7 +437,7 @@ static fc_status score_cells(DeviceGraph* d, double beta, cudaStream_t st) {
     if (!s->powl) FC_TRY(dev_alloc((void**)&s->powl, L * 8 + 8, st));
     std::vector<double> pw(L);
     for (uint32_t l = 0; l < L; l++) pw[l] = pow((double)(l + 1), beta);  // pow((l+1), beta)
-    FC_CUDA_TRY(cudaMemcpyAsync(s->powl, pw.data(), L * 8, cudaMemcpyHostToDevice, st));
+    FC_TRY(to_device(s->powl, pw.data(), L * 8, st));
     if (!s->ncells) return FC_OK;
     uint32_t P = 1;
     while (P < L) P <<= 1;
@@ -469,8 +468,7 @@ fc_status densest(fc_graph* g, const double* betas, uint32_t nb, fc_densest_resu
         k_fold<<<1, 32, 0, st>>>(s->cells, s->ncells, betas[b], s->d_res);
         count_launch();
         FC_CUDA_TRY(cudaGetLastError());
-        FC_CUDA_TRY(cudaMemcpyAsync(res + b, s->d_res, sizeof(fc_densest_result),
-                                    cudaMemcpyDeviceToHost, st));
+        FC_TRY(to_host(res + b, s->d_res, sizeof(fc_densest_result), st));
     }
     FC_CUDA_TRY(cudaEventRecord(e1, st));
     FC_CUDA_TRY(cudaStreamSynchronize(st));
@@ -492,7 +490,7 @@ fc_status cells(fc_graph* g, double beta, fc_cell* out, uint32_t cap, uint32_t* 
     uint64_t nc = s->ncells;
     if (count) *count = (uint32_t)nc;
     uint64_t w = nc < cap ? nc : cap;
-    if (w && out) FC_CUDA_TRY(cudaMemcpyAsync(out, s->cells, w * sizeof(fc_cell), cudaMemcpyDeviceToHost, st));
+    if (w && out) FC_TRY(to_host(out, s->cells, w * sizeof(fc_cell), st));
     FC_CUDA_TRY(cudaStreamSynchronize(st));
     return FC_OK;
 }
@@ -508,9 +506,7 @@ fc_status densest_members(fc_graph* g, const fc_densest_result* r, uint32_t* nod
     if (r->lmd < 1 || r->lmd > L || r->k > s->kmax[lam]) return FC_ERR_INVALID;
     if (nodes) {
         std::vector<uint32_t> col(n);
-        FC_CUDA_TRY(cudaMemcpyAsync(col.data(), d->table + (uint64_t)lam * n, (uint64_t)n * 4,
-                                    cudaMemcpyDeviceToHost, st));
-        FC_CUDA_TRY(cudaStreamSynchronize(st));
+        FC_TRY(to_host(col.data(), d->table + (uint64_t)lam * n, (uint64_t)n * 4, st));
         uint32_t j = 0;
         for (uint32_t v = 0; v < n; v++)
             if (col[v] >= r->k) nodes[j++] = v;
@@ -521,9 +517,7 @@ fc_status densest_members(fc_graph* g, const fc_densest_result* r, uint32_t* nod
         const uint32_t km1 = s->kmax[lam] + 1;
         std::vector<uint32_t> e(L);
         for (uint32_t l = 0; l < L; l++)
-            FC_CUDA_TRY(cudaMemcpyAsync(&e[l], s->H + s->hbase[lam] + (uint64_t)l * km1 + r->k, 4,
-                                        cudaMemcpyDeviceToHost, st));
-        FC_CUDA_TRY(cudaStreamSynchronize(st));
+            FC_TRY(to_host(&e[l], s->H + s->hbase[lam] + (uint64_t)l * km1 + r->k, 4, st));
         std::vector<uint32_t> idx(L);
         for (uint32_t l = 0; l < L; l++) idx[l] = l;
         std::stable_sort(idx.begin(), idx.end(), [&](uint32_t a, uint32_t b) { return e[a] > e[b]; });
@@ -537,6 +531,18 @@ fc_status densest_members(fc_graph* g, const fc_densest_result* r, uint32_t* nod
 void invalidate_densest(DeviceGraph* d) {
     DensState* s = (DensState*)d->dens;
     if (s) s->hist_valid = false;
+}
+
+void densest_preload() {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, k_colmax);
+    cudaFuncGetAttributes(&a, k_transpose);
+    cudaFuncGetAttributes(&a, k_node_hist);
+    cudaFuncGetAttributes(&a, k_edge_hist);
+    cudaFuncGetAttributes(&a, k_suffix);
+    cudaFuncGetAttributes(&a, k_cells);
+    cudaFuncGetAttributes(&a, k_fold);
+    cudaGetLastError();
 }
 
 }  // namespace fc

@@ -65,7 +65,7 @@ struct DeviceGraph {
     size_t ws_bytes = 0;
     uint64_t bytes = 0;            // CSR + table
     fc_stats stats{};              // diagnostics of the last computations
-    cudaStream_t home = nullptr;   // stream of the last call (device frees are ordered on it)
+    cudaStream_t home = nullptr;   // stream that may still run work on it (nullptr: none)
 };
 
 // Device memory from the device's stream-ordered pool, which keeps freed
@@ -73,6 +73,18 @@ struct DeviceGraph {
 // dropping and re-uploading a graph does not return to the driver.
 fc_status dev_alloc(void** p, size_t bytes, cudaStream_t s);
 void dev_free(void* p, cudaStream_t s);
+
+// A pinned host buffer a thread copies through (set_thread_staging); the
+// server lanes install one so that their copies do not queue behind other
+// threads' copies to pageable memory.
+struct Staging {
+    void* p = nullptr;
+    size_t cap = 0;
+};
+void set_thread_staging(Staging* st);
+// device -> host, waits for the copy; host -> device, waits only when staged
+fc_status to_host(void* h, const void* d, size_t bytes, cudaStream_t s);
+fc_status to_device(void* d, const void* h, size_t bytes, cudaStream_t s);
 
 // kernels launched by this library (fc_launch_count)
 void count_launch(uint32_t k = 1);
@@ -118,10 +130,12 @@ struct PeelSegSpec {
 uint64_t peel_batch_ws_bytes(const std::vector<PeelSegSpec>& specs);
 // All segments in one persistent launch (threads per block and the longest row
 // queued as one item: 0 = defaults).  With *use_graph set the launch is
-// captured in a CUDA graph; on return *use_graph says whether it was.
+// captured in a CUDA graph; on return *use_graph says whether it was.  The grid
+// covers at most max_sms SMs (0 = all), so that launches on other streams can
+// run beside it.
 fc_status peel_batch(const std::vector<PeelSegSpec>& specs, void* ws, size_t ws_bytes,
                      cudaStream_t s, PeelStats* st, uint32_t threads, uint32_t small_row,
-                     bool* use_graph);
+                     bool* use_graph, uint32_t max_sms = 0);
 
 // last CUDA error text, for diagnostics
 const char* last_cuda_error();

@@ -68,7 +68,9 @@ void apply_order(int order, fc_graph* g);
 // ---- device (graph.cu / peel.cu / densest.cu) --------------------------------
 bool cuda_available();
 fc_status upload(fc_graph* g, cudaStream_t s);
-void release_device(fc_graph* g);
+// frees g's device copy; waits for g's last stream first unless the caller
+// knows that its work is complete
+void release_device(fc_graph* g, bool wait_home = true);
 uint64_t device_bytes(const fc_graph* g);
 fc_status coreindex(fc_graph* g, uint32_t* out, bool out_on_device, cudaStream_t s);
 fc_status densest(fc_graph* g, const double* betas, uint32_t nb, fc_densest_result* res,
@@ -80,6 +82,23 @@ fc_status cells(fc_graph* g, double beta, fc_cell* out, uint32_t cap, uint32_t* 
 fc_status batch_run(fc_graph* const* gs, uint32_t count, double beta, uint32_t* const* tables,
                     fc_densest_result* res, const fc_batch_options* opt, fc_batch_report* rep,
                     cudaStream_t s);
+// The peel of every graph (all its columns) in persistent launches covering
+// at most max_sms SMs (0 = all) on stream s, uploading graphs as needed;
+// each graph's table is valid on the device afterwards.  rep may be NULL.
+fc_status batch_peel(fc_graph* const* gs, uint32_t count, const fc_batch_options* opt,
+                     uint32_t max_sms, fc_batch_report* rep, cudaStream_t s);
+// the peel scratch batch_peel allocates for these graphs (one launch group)
+uint64_t batch_peel_ws_bytes(fc_graph* const* gs, uint32_t count);
+// one graph, one lambda column per launch (the plain form); table valid
+// after; adds to the three counters
+fc_status batch_plain_one(fc_graph* g, cudaStream_t s, double* peel_ms, uint32_t* launches,
+                          uint32_t* levels);
+// a graph's device copy is going away: servers drop it from their records
+void residency_forget(fc_graph* g);
+// loads every kernel of the library on the current device now (once)
+void preload_kernels();
+void peel_preload();
+void densest_preload();
 
 }  // namespace fc
 

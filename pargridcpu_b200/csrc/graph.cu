@@ -3,6 +3,7 @@
 #include <cub/cub.cuh>
 
 #include <cstdio>
+#include <cstring>
 #include <mutex>
 #include <string>
 
@@ -97,6 +98,51 @@ void dev_free(void* p, cudaStream_t s) {
     if (p) cudaFreeAsync(p, s);
 }
 
+// ---- host <-> device copies through a thread's pinned staging buffer ------
+// A copy to or from pageable host memory goes through the driver's own
+// staging, which copies from every thread share: a server lane's small
+// read-back would wait behind another lane's read-back that waits for that
+// lane's long kernel.  A thread that installs a pinned staging buffer (the
+// server lanes) copies through it in pieces instead; other threads copy
+// directly.
+
+static thread_local Staging* t_staging = nullptr;
+
+void set_thread_staging(Staging* st) { t_staging = st; }
+
+fc_status to_host(void* h, const void* d, size_t bytes, cudaStream_t s) {
+    if (!bytes) return FC_OK;
+    Staging* st = t_staging;
+    if (!st || !st->p) {
+        FC_CUDA_TRY(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, s));
+        FC_CUDA_TRY(cudaStreamSynchronize(s));
+        return FC_OK;
+    }
+    for (size_t off = 0; off < bytes; off += st->cap) {
+        const size_t c = bytes - off < st->cap ? bytes - off : st->cap;
+        FC_CUDA_TRY(cudaMemcpyAsync(st->p, (const char*)d + off, c, cudaMemcpyDeviceToHost, s));
+        FC_CUDA_TRY(cudaStreamSynchronize(s));
+        memcpy((char*)h + off, st->p, c);
+    }
+    return FC_OK;
+}
+
+fc_status to_device(void* d, const void* h, size_t bytes, cudaStream_t s) {
+    if (!bytes) return FC_OK;
+    Staging* st = t_staging;
+    if (!st || !st->p) {
+        FC_CUDA_TRY(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, s));
+        return FC_OK;
+    }
+    for (size_t off = 0; off < bytes; off += st->cap) {
+        const size_t c = bytes - off < st->cap ? bytes - off : st->cap;
+        memcpy(st->p, (const char*)h + off, c);
+        FC_CUDA_TRY(cudaMemcpyAsync((char*)d + off, st->p, c, cudaMemcpyHostToDevice, s));
+        FC_CUDA_TRY(cudaStreamSynchronize(s));  // before the buffer is written again
+    }
+    return FC_OK;
+}
+
 fc_status ensure_ws(DeviceGraph* d, size_t bytes, cudaStream_t s) {
     if (d->ws_bytes >= bytes) return FC_OK;
     dev_free(d->ws, s);
@@ -168,27 +214,31 @@ fc_status upload(fc_graph* g, cudaStream_t s) {
         FC_CUDA_TRY(cudaGetLastError());
     }
     uint32_t mx[2] = {0, 0};
-    FC_CUDA_TRY(cudaMemcpyAsync(mx, d_max, 8, cudaMemcpyDeviceToHost, s));
+    FC_TRY(to_host(mx, d_max, 8, s));
     if (tmp) FC_CUDA_TRY(cudaFreeAsync(tmp, s));
     FC_CUDA_TRY(cudaFreeAsync(d_off, s));
     FC_CUDA_TRY(cudaFreeAsync(d_in, s));
     FC_CUDA_TRY(cudaFreeAsync(rowlen, s));
     FC_CUDA_TRY(cudaFreeAsync(d_max, s));
     FC_CUDA_TRY(cudaStreamSynchronize(s));
+    d->home = nullptr;
     d->max_deg = mx[0];
     d->max_row = mx[1];
     return FC_OK;
 }
 
-void release_device(fc_graph* g) {
+void release_device(fc_graph* g, bool wait_home) {
     DeviceGraph* d = g->dev;
     if (!d) return;
+    residency_forget(g);
     int cur = -1;
     cudaGetDevice(&cur);
     if (d->device >= 0 && d->device != cur) cudaSetDevice(d->device);
     // the last call's work is done before its memory returns to the pool;
     // the frees go on the legacy stream, which outlives any caller stream
-    cudaStreamSynchronize(d->home);
+    // a call that left work in flight recorded its stream; one that finished
+    // with a synchronize did not (that stream may already be destroyed)
+    if (wait_home && d->home) cudaStreamSynchronize(d->home);
     cudaGetLastError();
     free_densest_state(d);
     dev_free(d->node_ptr, 0);
@@ -204,6 +254,41 @@ void release_device(fc_graph* g) {
 uint64_t device_bytes(const fc_graph* g) {
     if (!g->dev) return 0;
     return g->dev->bytes + g->dev->ws_bytes;
+}
+
+// Kernels load on first use unless loaded before, and a load may wait for
+// the kernels already running on the device: a server lane's first batch of
+// a new kind would wait for another lane's batch.  This loads every kernel
+// of the library (the scan of the CSR build by running it once on a few
+// words) on the current device, once.
+void preload_kernels() {
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done[dev]) return;
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, k_degrees);
+    cudaFuncGetAttributes(&a, k_scatter);
+    cudaFuncGetAttributes(&a, k_max);
+    peel_preload();
+    densest_preload();
+    uint32_t* buf = nullptr;
+    void* tmp = nullptr;
+    size_t tmp_bytes = 0;
+    if (cudaMalloc(&buf, 64) == cudaSuccess &&
+        cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, buf, buf + 8, 8, (cudaStream_t)0) ==
+            cudaSuccess &&
+        cudaMalloc(&tmp, tmp_bytes + 16) == cudaSuccess) {
+        cudaMemset(buf, 0, 64);
+        cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, buf, buf + 8, 8, (cudaStream_t)0);
+        cudaDeviceSynchronize();
+    }
+    if (tmp) cudaFree(tmp);
+    if (buf) cudaFree(buf);
+    cudaGetLastError();
+    done[dev] = true;
 }
 
 }  // namespace fc

@@ -120,6 +120,7 @@ struct PeelJob {
     // optional per-level trace: [level][scan|drain] = {ns, items, alive}
     unsigned long long* trace;
     uint32_t trace_levels;
+    uint32_t max_sms;     // host side: SMs the grid may cover (0 = every SM)
 };
 
 // ---- memory-model helpers -------------------------------------------------
@@ -928,6 +929,7 @@ static fc_status launch_t(PeelJob& j, cudaStream_t s) {
     if (occ < 1) return FC_ERR_DEVICE;
     uint32_t want_occ = env_u32("FC_PEEL_BLOCKS_PER_SM", 1024 / T);
     if (want_occ >= 1 && (int)want_occ < occ) occ = (int)want_occ;
+    if (j.max_sms && (int)j.max_sms < sms) sms = (int)j.max_sms;
     dim3 grid(sms * occ), block(T);
     void* args[] = {&j};
     FC_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_peel<G, T, MULTI>, grid, block, args, 0, s));
@@ -1078,8 +1080,7 @@ static fc_status run_job(PeelJob& j, uint32_t maxL, uint32_t threads, cudaStream
     if (use_graph) *use_graph = graphed;
     count_launch();
     PeelCtl out;
-    FC_CUDA_TRY(cudaMemcpyAsync(&out, j.ctl, sizeof(out), cudaMemcpyDeviceToHost, s));
-    FC_CUDA_TRY(cudaStreamSynchronize(s));
+    FC_TRY(to_host(&out, j.ctl, sizeof(out), s));
     float ms = 0;
     if (instrument) {
         cudaEventElapsedTime(&ms, e0, e1);
@@ -1171,7 +1172,7 @@ uint64_t peel_batch_ws_bytes(const std::vector<PeelSegSpec>& specs) {
 
 fc_status peel_batch(const std::vector<PeelSegSpec>& specs, void* ws, size_t ws_bytes,
                      cudaStream_t s, PeelStats* st, uint32_t threads, uint32_t small_row,
-                     bool* use_graph) {
+                     bool* use_graph, uint32_t max_sms) {
     if (specs.empty()) return FC_OK;
     if (peel_batch_ws_bytes(specs) > ws_bytes) return FC_ERR_INVALID;
     char* w = (char*)ws;
@@ -1205,14 +1206,15 @@ fc_status peel_batch(const std::vector<PeelSegSpec>& specs, void* ws, size_t ws_
     fc_status rc;
     carve_shared(j, w, end, nx, ent, s, &rc);
     FC_TRY(rc);
-    FC_CUDA_TRY(cudaMemcpyAsync(dsegs, host.data(), nseg * sizeof(SegP), cudaMemcpyHostToDevice, s));
-    FC_CUDA_TRY(cudaMemcpyAsync(dxb, xb.data(), 4 * (nseg + 1), cudaMemcpyHostToDevice, s));
+    FC_TRY(to_device(dsegs, host.data(), nseg * sizeof(SegP), s));
+    FC_TRY(to_device(dxb, xb.data(), 4 * (nseg + 1), s));
     j.seg0 = host[0];
     j.segs = dsegs;
     j.seg_xbase = dxb;
     j.nseg = nseg;
     j.max_level = max_level;
     j.small_row = small_row;
+    j.max_sms = max_sms;
     if (!threads) threads = default_threads();
     // the segment table must be on the device before a captured launch runs
     if (use_graph && *use_graph) FC_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1222,6 +1224,19 @@ fc_status peel_batch(const std::vector<PeelSegSpec>& specs, void* ws, size_t ws_
                               use_graph);
     }
     return run_job<true>(j, maxL, threads, s, st, true, 0, 0, use_graph);
+}
+
+void peel_preload() {
+    cudaFuncAttributes a;
+    cudaFuncGetAttributes(&a, k_peel<1, 512, false>);
+    cudaFuncGetAttributes(&a, k_peel<1, 512, true>);
+    cudaFuncGetAttributes(&a, k_peel<1, 1024, false>);
+    cudaFuncGetAttributes(&a, k_peel<1, 1024, true>);
+    cudaFuncGetAttributes(&a, k_peel<32, 512, false>);
+    cudaFuncGetAttributes(&a, k_peel<32, 512, true>);
+    cudaFuncGetAttributes(&a, k_peel<32, 1024, false>);
+    cudaFuncGetAttributes(&a, k_peel<32, 1024, true>);
+    cudaGetLastError();
 }
 
 fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream_t s,

@@ -1,105 +1,360 @@
-// Request loop: admits decomposition + densest requests by device-memory
-// footprint and in-flight slots, runs them, and completes each independently.
+// Continuous-batching request loop (fc_server_*).
+//
+// Requests (a graph + beta) wait in one FIFO.  The server runs `lanes` lane
+// threads, each with its own stream; a lane that is free takes, at once,
+// every pending request that fits -- the admission test below -- and runs
+// them as one batch: one persistent peel launch over all their graphs (one
+// segment per distinct graph, every lambda column), then the densest search
+// of each request, then the table copies.  Requests that arrive while a
+// batch is on the device wait for the next free lane, so new work joins as
+// soon as a lane and memory free up, and the batches of different lanes run
+// on the device at the same time: each lane's peel grid covers only its
+// share of the SMs (SMs / lanes), which leaves the others for the other lanes.
+//
+// Admission: a request is taken while the device bytes of everything
+// admitted -- the device copies of resident graphs plus the scratch of the
+// running batches -- stay within the budget.  Graphs stay resident after
+// their requests complete (they are often asked again); when memory is
+// short, resident graphs that no running batch uses are released, least
+// recently used first.  A graph runs on one lane at a time (its table lives
+// with its device copy), so a request whose graph is running elsewhere waits.
+// A request that alone would exceed the budget fails with FC_ERR_BUDGET.
+//
+// The plain form (options.plain) is the one-at-a-time baseline: one lane, one
+// request per batch, one lambda column per launch.
+//
+// Every result equals fc_coreindex + fc_densest on the graph alone: the
+// table is the unique core index, whatever the batch, and the densest search
+// reads only the graph's own table.
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <list>
 #include <map>
 #include <mutex>
+#include <set>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
-#include "fc_internal.h"
+#include "device.h"
+
+using Clock = std::chrono::steady_clock;
+
+namespace fc {
+
+// ---- residency: device copies kept by servers ------------------------------
+// Each server keeps its own least-recently-used list of the graphs whose
+// device copies it holds, and its budget counts only those.  The index of
+// all lists is process-wide, so that release_device (a graph freed by its
+// owner, or released by any server) removes the graph from whichever list
+// holds it.  A graph is on one list at a time: the last server to use it.
+
+struct Residency {
+    std::list<fc_graph*> lru;  // front = most recently used
+    uint64_t bytes = 0;
+};
+
+struct ResEntry {
+    Residency* owner;
+    uint64_t bytes;
+    std::list<fc_graph*>::iterator pos;
+};
+
+static std::mutex g_res_mu;
+static std::unordered_map<fc_graph*, ResEntry> g_res;
+
+static void res_unlink(std::unordered_map<fc_graph*, ResEntry>::iterator it) {  // under g_res_mu
+    it->second.owner->bytes -= it->second.bytes;
+    it->second.owner->lru.erase(it->second.pos);
+    g_res.erase(it);
+}
+
+void residency_forget(fc_graph* g) {
+    std::lock_guard<std::mutex> lk(g_res_mu);
+    auto it = g_res.find(g);
+    if (it != g_res.end()) res_unlink(it);
+}
+
+static void residency_touch(Residency* r, fc_graph* g, uint64_t bytes) {
+    std::lock_guard<std::mutex> lk(g_res_mu);
+    auto it = g_res.find(g);
+    if (it != g_res.end()) res_unlink(it);
+    r->lru.push_front(g);
+    g_res[g] = ResEntry{r, bytes, r->lru.begin()};
+    r->bytes += bytes;
+}
+
+static bool residency_has(Residency* r, fc_graph* g) {
+    std::lock_guard<std::mutex> lk(g_res_mu);
+    auto it = g_res.find(g);
+    return it != g_res.end() && it->second.owner == r;
+}
+
+static uint64_t residency_bytes(Residency* r) {
+    std::lock_guard<std::mutex> lk(g_res_mu);
+    return r->bytes;
+}
+
+// The server forgets its copies (they stay on the device with their graphs).
+static void residency_drop(Residency* r) {
+    std::lock_guard<std::mutex> lk(g_res_mu);
+    while (!r->lru.empty()) res_unlink(g_res.find(r->lru.front()));
+}
+
+// Graphs of r not in `keep`, least recently used first, until their bytes
+// reach `need` (all of them when they do not).
+static std::vector<std::pair<fc_graph*, uint64_t>> residency_victims(
+    Residency* r, const std::set<fc_graph*>& keep, uint64_t need) {
+    std::lock_guard<std::mutex> lk(g_res_mu);
+    std::vector<std::pair<fc_graph*, uint64_t>> out;
+    uint64_t got = 0;
+    for (auto it = r->lru.rbegin(); it != r->lru.rend() && got < need; ++it) {
+        if (keep.count(*it)) continue;
+        const uint64_t b = g_res[*it].bytes;
+        out.push_back({*it, b});
+        got += b;
+    }
+    return out;
+}
+
+// Device bytes of a graph's resident copy: CSR, degrees, table and the
+// densest search's per-graph state (an estimate: transposed table, the
+// histograms and cell records).
+static uint64_t graph_bytes(const fc_graph* g) {
+    const uint64_t n = g->n, L = g->L, e = g->total_entries();
+    return 4 * (n + 1) + 4 * e + 8 * n * L + 4 * n * L + (16ull << 20);
+}
+
+}  // namespace fc
 
 namespace {
 
 struct Request {
-    uint64_t ticket;
-    fc_graph* g;
-    double beta;
-    uint32_t* table;
-    fc_densest_result* res;
-    uint64_t footprint;
-    std::chrono::steady_clock::time_point t_submit;
+    uint64_t ticket = 0;
+    fc_graph* g = nullptr;
+    double beta = 1.0;
+    uint32_t* table = nullptr;
+    fc_densest_result* res = nullptr;
+    Clock::time_point t_submit;
     fc_status status = FC_OK;
     double latency_ms = 0.0;
     bool done = false;
 };
 
-// Device bytes a request holds while it runs: CSR, table, peel scratch for
-// one column group and the densest histograms (an upper estimate).
-uint64_t footprint(const fc_graph* g) {
-    uint64_t n = g->n, L = g->L, e = g->total_entries();
-    uint64_t csr = 4 * (n + 1) + 4 * e + 4 * n * L;
-    uint64_t table = 8 * n * L;
-    uint64_t peel = 4 * (n * L * L + 8 * n * L);
-    return csr + table + peel + (64ull << 20);
-}
-
 }  // namespace
 
 struct fc_server {
-    uint64_t budget;
-    uint32_t max_inflight;
+    // options
+    uint64_t budget = 0;
+    uint32_t max_inflight = 0, lanes = 0, max_batch_graphs = 0, lane_sms = 0;
+    bool plain = false;
+    fc_batch_options bopt{};
+
+    fc::Residency res;  // device copies this server keeps
+
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
-    std::deque<Request*> queue;
+    std::deque<Request*> pending;
     std::map<uint64_t, Request*> all;
     uint64_t next_ticket = 1;
-    uint64_t inflight_bytes = 0;
-    uint32_t inflight = 0;
+    std::set<fc_graph*> running_graphs;  // graphs of the batches on the device
+    uint64_t running_bytes = 0;          // their scratch and not yet resident copies
+    uint32_t running_requests = 0;
     bool stop = false;
-    std::vector<std::thread> workers;
-    std::mutex gpu_mu;  // one decomposition on the device at a time
+    std::vector<std::thread> threads;
 
-    void worker() {
+    // statistics (under mu)
+    fc_server_stats st{};
+    uint32_t running_lanes = 0;
+    Clock::time_point t_mark = Clock::now();
+
+    void clock_advance() {
+        const Clock::time_point now = Clock::now();
+        const double dt = std::chrono::duration<double, std::milli>(now - t_mark).count();
+        if (running_lanes >= 1) st.busy_ms += dt;
+        if (running_lanes >= 2) st.overlap_ms += dt;
+        t_mark = now;
+    }
+
+    void finish(Request* r, fc_status status) {  // under mu
+        r->status = status;
+        r->latency_ms =
+            std::chrono::duration<double, std::milli>(Clock::now() - r->t_submit).count();
+        r->done = true;
+        st.requests_done++;
+    }
+
+    // Takes the requests of the next batch out of `pending` (under mu).
+    // Returns the distinct graphs and the bytes the batch reserves (its
+    // scratch and the copies of graphs not yet resident).  Graphs released to
+    // make room are released here, under the lock, so that no other lane can
+    // take one of them meanwhile; their last work has completed (every batch
+    // ends with a stream synchronize), so the release does not wait.
+    void form_batch(std::vector<Request*>* batch, std::vector<fc_graph*>* graphs,
+                    uint64_t* reserve) {
+        uint64_t used = fc::residency_bytes(&res) + running_bytes;
+        std::set<fc_graph*> taken;
+        for (auto it = pending.begin(); it != pending.end();) {
+            Request* r = *it;
+            if (running_graphs.count(r->g)) {  // running on another lane
+                ++it;
+                continue;
+            }
+            if (taken.count(r->g)) {  // shares the peel of a graph already taken
+                if (plain) break;
+                batch->push_back(r);
+                it = pending.erase(it);
+                continue;
+            }
+            if (graphs->size() >= max_batch_graphs ||
+                running_requests + batch->size() >= max_inflight)
+                break;
+            fc_graph* g = r->g;
+            const uint64_t gb = fc::graph_bytes(g);
+            const uint64_t wb = plain ? fc::peel_ws_bytes(g->n, g->L, g->total_entries(), 1)
+                                      : fc::batch_peel_ws_bytes(&g, 1);
+            if (gb + wb > budget) {
+                finish(r, FC_ERR_BUDGET);
+                it = pending.erase(it);
+                cv_done.notify_all();
+                continue;
+            }
+            const uint64_t need = (fc::residency_has(&res, g) ? 0 : gb) + wb;
+            if (used + need > budget) {
+                // release resident graphs that nothing running or taken uses
+                std::set<fc_graph*> keep(running_graphs);
+                keep.insert(taken.begin(), taken.end());
+                keep.insert(g);
+                auto victims = fc::residency_victims(&res, keep, used + need - budget);
+                uint64_t freed = 0;
+                for (auto& v : victims) freed += v.second;
+                if (used + need > budget + freed) break;  // wait for memory, in order
+                for (auto& v : victims) fc::release_device(v.first, false);
+                used -= freed;
+                st.evictions += victims.size();
+            }
+            used += need;
+            *reserve += need;
+            taken.insert(g);
+            graphs->push_back(g);
+            batch->push_back(r);
+            it = pending.erase(it);
+            if (plain) break;
+        }
+    }
+
+    // The device work of one batch on the lane's stream.
+    fc_status run_batch(cudaStream_t s, const std::vector<Request*>& batch,
+                        const std::vector<fc_graph*>& graphs) {
+        for (fc_graph* g : graphs) {
+            const bool had = g->dev != nullptr;
+            FC_TRY(fc::upload(g, s));
+            if (!had) {
+                std::lock_guard<std::mutex> lk(mu);
+                st.uploads++;
+            }
+        }
+        if (plain) {
+            double ms = 0;
+            uint32_t launches = 0, levels = 0;
+            FC_TRY(fc::batch_plain_one(graphs[0], s, &ms, &launches, &levels));
+        } else {
+            FC_TRY(fc::batch_peel(graphs.data(), (uint32_t)graphs.size(), &bopt, lane_sms, nullptr,
+                                  s));
+        }
+        // densest: every request's beta, one pass per graph
+        for (fc_graph* g : graphs) {
+            std::vector<double> betas;
+            std::vector<Request*> rs;
+            for (Request* r : batch)
+                if (r->g == g && r->res) {
+                    betas.push_back(r->beta);
+                    rs.push_back(r);
+                }
+            if (betas.empty()) continue;
+            std::vector<fc_densest_result> out(betas.size());
+            if (g->n && g->L) {
+                FC_TRY(fc::densest(g, betas.data(), (uint32_t)betas.size(), out.data(), s));
+            } else {
+                for (size_t i = 0; i < out.size(); i++) {
+                    out[i] = fc_densest_result{};
+                    out[i].beta = betas[i];
+                }
+            }
+            for (size_t i = 0; i < rs.size(); i++) *rs[i]->res = out[i];
+        }
+        for (Request* r : batch) {
+            const uint64_t bytes = (uint64_t)r->g->n * r->g->L * 4;
+            if (r->table && bytes)
+                FC_TRY(fc::to_host(r->table, r->g->dev->table, bytes, s));
+        }
+        FC_CUDA_TRY(cudaStreamSynchronize(s));
+        return FC_OK;
+    }
+
+    void lane_loop() {
         cudaStream_t s = nullptr;
         cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        // this lane's copies go through its own pinned buffer
+        fc::Staging stage;
+        if (cudaHostAlloc(&stage.p, 16u << 20, cudaHostAllocDefault) == cudaSuccess)
+            stage.cap = 16u << 20;
+        else
+            stage.p = nullptr;
+        cudaGetLastError();
+        fc::set_thread_staging(&stage);
         for (;;) {
-            Request* r = nullptr;
+            std::vector<Request*> batch;
+            std::vector<fc_graph*> graphs;
+            uint64_t reserve = 0;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv_work.wait(lk, [&] {
-                    if (stop) return true;
-                    if (queue.empty()) return false;
-                    Request* h = queue.front();
-                    return inflight < max_inflight &&
-                           (inflight == 0 || inflight_bytes + h->footprint <= budget);
-                });
-                if (stop && queue.empty()) break;
-                if (queue.empty()) continue;
-                r = queue.front();
-                queue.pop_front();
-                inflight++;
-                inflight_bytes += r->footprint;
-            }
-            fc_status st = FC_OK;
-            if (r->footprint > budget) st = FC_ERR_BUDGET;
-            if (st == FC_OK) st = fc::upload(r->g, s);
-            if (st == FC_OK) {
-                std::lock_guard<std::mutex> g(gpu_mu);
-                st = fc::coreindex(r->g, r->table, false, s);
-                if (st == FC_OK && r->res) {
-                    if (r->g->n && r->g->L) st = fc::densest(r->g, &r->beta, 1, r->res, s);
-                    else {
-                        memset(r->res, 0, sizeof(*r->res));
-                        r->res->beta = r->beta;
+                for (;;) {
+                    if (stop && pending.empty()) break;
+                    if (!pending.empty()) {
+                        form_batch(&batch, &graphs, &reserve);
+                        if (!batch.empty()) break;
                     }
+                    // nothing to take now: wait for an arrival or a completion
+                    cv_work.wait_for(lk, std::chrono::milliseconds(100));
                 }
+                if (batch.empty()) break;  // stopped and nothing pending
+                for (fc_graph* g : graphs) running_graphs.insert(g);
+                running_bytes += reserve;
+                running_requests += (uint32_t)batch.size();
+                st.peak_bytes = std::max(st.peak_bytes, fc::residency_bytes(&res) + running_bytes);
+                clock_advance();
+                running_lanes++;
+                st.batches++;
+                st.graphs_peeled += graphs.size();
+                st.max_batch = std::max<uint32_t>(st.max_batch, (uint32_t)batch.size());
+            }
+            const fc_status rc = run_batch(s, batch, graphs);
+            if (rc != FC_OK) cudaStreamSynchronize(s);  // what was enqueued has finished
+            // nothing is left in flight on the lane's stream, which goes away
+            // with the server while the graphs may live on
+            for (fc_graph* g : graphs) {
+                if (!g->dev) continue;
+                g->dev->home = nullptr;
+                fc::residency_touch(&res, g, fc::graph_bytes(g));
             }
             {
                 std::lock_guard<std::mutex> lk(mu);
-                r->status = st;
-                r->latency_ms = std::chrono::duration<double, std::milli>(
-                                    std::chrono::steady_clock::now() - r->t_submit)
-                                    .count();
-                r->done = true;
-                inflight--;
-                inflight_bytes -= r->footprint;
+                clock_advance();
+                running_lanes--;
+                for (fc_graph* g : graphs) running_graphs.erase(g);
+                running_bytes -= reserve;
+                running_requests -= (uint32_t)batch.size();
+                for (Request* r : batch) finish(r, rc);
             }
             cv_done.notify_all();
             cv_work.notify_all();
         }
+        fc::set_thread_staging(nullptr);
+        if (stage.p) cudaFreeHost(stage.p);
         if (s) cudaStreamDestroy(s);
     }
 };
@@ -108,11 +363,27 @@ extern "C" {
 
 fc_status fc_server_create(const fc_server_options* opt, fc_server** out) {
     if (!out) return FC_ERR_INVALID;
+    *out = nullptr;
     if (!fc::cuda_available()) return FC_ERR_NO_DEVICE;
     fc_server* s = new fc_server();
     s->budget = (opt && opt->hbm_budget_bytes) ? opt->hbm_budget_bytes : 150ull * 1000 * 1000 * 1000;
-    s->max_inflight = (opt && opt->max_inflight) ? opt->max_inflight : 16;
-    for (uint32_t i = 0; i < s->max_inflight; i++) s->workers.emplace_back([s] { s->worker(); });
+    s->max_inflight = (opt && opt->max_inflight) ? opt->max_inflight : 256;
+    s->plain = opt && opt->plain;
+    s->lanes = s->plain ? 1 : ((opt && opt->lanes) ? opt->lanes : 2);
+    s->max_batch_graphs = s->plain ? 1 : ((opt && opt->max_batch_graphs) ? opt->max_batch_graphs : 64);
+    // every kernel loaded now: a kernel's first load may wait for kernels
+    // running on other lanes
+    fc::preload_kernels();
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    s->lane_sms = s->lanes > 1 ? std::max(1u, (uint32_t)sms / s->lanes) : 0;
+    // fixed launch shape: serving does not stop to autotune every new mix
+    s->bopt.block_threads = (opt && opt->block_threads) ? opt->block_threads : 1024;
+    s->bopt.hub_threshold = (opt && opt->hub_threshold) ? opt->hub_threshold : 64;
+    s->bopt.use_cuda_graph = 0;
+    s->st.lanes = s->lanes;
+    for (uint32_t i = 0; i < s->lanes; i++) s->threads.emplace_back([s] { s->lane_loop(); });
     *out = s;
     return FC_OK;
 }
@@ -125,13 +396,16 @@ fc_status fc_server_submit(fc_server* s, fc_graph* g, double beta, uint32_t* tab
     r->beta = beta;
     r->table = table;
     r->res = res;
-    r->footprint = footprint(g);
-    r->t_submit = std::chrono::steady_clock::now();
+    r->t_submit = Clock::now();
     {
         std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stop) {
+            delete r;
+            return FC_ERR_INVALID;
+        }
         r->ticket = s->next_ticket++;
         s->all[r->ticket] = r;
-        s->queue.push_back(r);
+        s->pending.push_back(r);
     }
     if (ticket) *ticket = r->ticket;
     s->cv_work.notify_all();
@@ -156,6 +430,15 @@ fc_status fc_server_wait(fc_server* s, uint64_t ticket, int64_t timeout_ms, fc_s
     return FC_OK;
 }
 
+fc_status fc_server_query(fc_server* s, fc_server_stats* out) {
+    if (!s || !out) return FC_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->clock_advance();
+    *out = s->st;
+    out->resident_bytes = fc::residency_bytes(&s->res);
+    return FC_OK;
+}
+
 fc_status fc_server_destroy(fc_server* s) {
     if (!s) return FC_ERR_INVALID;
     {
@@ -163,7 +446,8 @@ fc_status fc_server_destroy(fc_server* s) {
         s->stop = true;
     }
     s->cv_work.notify_all();
-    for (auto& t : s->workers) t.join();
+    for (auto& t : s->threads) t.join();
+    fc::residency_drop(&s->res);
     for (auto& kv : s->all) delete kv.second;
     delete s;
     return FC_OK;

@@ -26,7 +26,7 @@ EXPORTS = [
     "fc_graph_id2vtx", "fc_graph_order", "fc_graph_csr", "fc_graph_upload",
     "fc_graph_release_device", "fc_graph_reset_results", "fc_graph_device_bytes", "fc_coreindex",
     "fc_densest", "fc_densest_members", "fc_cells", "fc_batch_run", "fc_server_create",
-    "fc_server_submit", "fc_server_wait", "fc_server_destroy", "fc_graph_stats",
+    "fc_server_submit", "fc_server_wait", "fc_server_query", "fc_server_destroy", "fc_graph_stats",
     "fc_launch_count", "fc_coreindex_fixed_scratch",
 ]
 
@@ -78,7 +78,21 @@ class Stats(C.Structure):
 
 
 class ServerOptions(C.Structure):
-    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_inflight", C.c_uint32)]
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_inflight", C.c_uint32),
+                ("lanes", C.c_uint32), ("max_batch_graphs", C.c_uint32),
+                ("block_threads", C.c_uint32), ("hub_threshold", C.c_uint32),
+                ("plain", C.c_int)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("requests_done", C.c_uint64), ("batches", C.c_uint64),
+                ("graphs_peeled", C.c_uint64), ("uploads", C.c_uint64),
+                ("evictions", C.c_uint64), ("resident_bytes", C.c_uint64),
+                ("peak_bytes", C.c_uint64), ("busy_ms", C.c_double), ("overlap_ms", C.c_double),
+                ("max_batch", C.c_uint32), ("lanes", C.c_uint32)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 _lib = None
@@ -119,6 +133,7 @@ def lib():
         "fc_server_create": ([p, pp], i32),
         "fc_server_submit": ([p, p, C.c_double, p, p, C.POINTER(u64)], i32),
         "fc_server_wait": ([p, u64, C.c_int64, C.POINTER(i32), C.POINTER(C.c_double)], i32),
+        "fc_server_query": ([p, p], i32),
         "fc_server_destroy": ([p], i32),
         "fc_graph_stats": ([p, p], i32),
         "fc_launch_count": ([], u64),
