@@ -191,10 +191,12 @@ fc_status fc_batch_run(fc_graph* const* graphs, uint32_t count, double beta,
  * A continuous-batching request loop.  Requests (a graph + beta) queue in
  * arrival order; each of `lanes` lanes (a host thread and a stream) that is
  * free takes every pending request that fits and runs them as one batch --
- * one persistent peel launch over their graphs, whose grid covers SMs/lanes
- * SMs, then their densest searches -- so requests that arrive while batches
- * are on the device join the next batch as a lane and memory free up, and
- * the batches of different lanes overlap on the device.  A request is
+ * one persistent peel launch over their graphs, then their densest searches
+ * -- so requests that arrive while batches are on the device join the next
+ * batch as a lane, SMs and memory free up.  A heavy request (heavy_visits
+ * edge visits or more) runs alone on three quarters of the SMs, one at a
+ * time, while light batches share the rest, so its work overlaps on the
+ * device with the light requests that arrive meanwhile.  A request is
  * admitted while the device bytes of resident graphs plus running batches
  * stay within the budget; graphs stay resident between requests and the
  * least recently used ones that no batch is using are released when memory
@@ -215,12 +217,14 @@ typedef struct fc_server_options {
     uint32_t block_threads;     /* peel launch shape (0 = 1024 threads, */
     uint32_t hub_threshold;     /*   rows of more than 64 entries split) */
     int plain;                  /* 1 = the one-at-a-time baseline */
+    uint64_t heavy_visits;      /* entries x L at which a request runs alone (0 = 1e9) */
 } fc_server_options;
 
 /* Counters since fc_server_create. */
 typedef struct fc_server_stats {
     uint64_t requests_done;
     uint64_t batches;
+    uint64_t heavy_batches;     /* batches of one heavy request */
     uint64_t graphs_peeled;     /* distinct graphs over all batches */
     uint64_t uploads;           /* device copies made */
     uint64_t evictions;         /* resident copies released for room */

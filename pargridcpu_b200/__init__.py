@@ -254,13 +254,14 @@ def batch_run(graphs, beta=1.0, want_tables=True, block_threads=0, hub_threshold
 class Server:
     """Continuous-batching request loop (fc_server_*): requests queue in
     arrival order, free lanes take every pending request that fits the
-    device-memory budget as one batch, and the lanes' batches overlap on the
-    device.  ``plain=True`` is the one-at-a-time baseline."""
+    device-memory budget as one batch; heavy requests run alone on three
+    quarters of the SMs while light batches share the rest, so their work
+    overlaps on the device.  ``plain=True`` is the one-at-a-time baseline."""
 
     def __init__(self, hbm_budget_bytes=0, max_inflight=0, lanes=0, max_batch_graphs=0,
-                 block_threads=0, hub_threshold=0, plain=False):
+                 block_threads=0, hub_threshold=0, plain=False, heavy_visits=0):
         opt = _n.ServerOptions(hbm_budget_bytes, max_inflight, lanes, max_batch_graphs,
-                               block_threads, hub_threshold, int(plain))
+                               block_threads, hub_threshold, int(plain), heavy_visits)
         h = C.c_void_p()
         _n.check(_n.lib().fc_server_create(C.byref(opt), C.byref(h)), "server_create")
         self._h = h

@@ -2,14 +2,15 @@
 //
 // Requests (a graph + beta) wait in one FIFO.  The server runs `lanes` lane
 // threads, each with its own stream; a lane that is free takes, at once,
-// every pending request that fits -- the admission test below -- and runs
+// every pending request that fits -- the admission tests below -- and runs
 // them as one batch: one persistent peel launch over all their graphs (one
 // segment per distinct graph, every lambda column), then the densest search
 // of each request, then the table copies.  Requests that arrive while a
 // batch is on the device wait for the next free lane, so new work joins as
-// soon as a lane and memory free up, and the batches of different lanes run
-// on the device at the same time: each lane's peel grid covers only its
-// share of the SMs (SMs / lanes), which leaves the others for the other lanes.
+// soon as a lane, SMs and memory free up.  Each batch's peel grid covers the
+// SMs it claimed (form_batch): a heavy request runs alone on three quarters
+// of them while light batches run on the rest, so the two overlap on the
+// device and light requests never queue behind a heavy one.
 //
 // Admission: a request is taken while the device bytes of everything
 // admitted -- the device copies of resident graphs plus the scratch of the
@@ -149,7 +150,11 @@ struct Request {
 struct fc_server {
     // options
     uint64_t budget = 0;
-    uint32_t max_inflight = 0, lanes = 0, max_batch_graphs = 0, lane_sms = 0;
+    uint32_t max_inflight = 0, lanes = 0, max_batch_graphs = 0;
+    uint32_t sms = 0, heavy_sms = 0, min_light_sms = 0;  // the device's SMs and the shares
+    uint64_t heavy_visits = 0;
+    size_t backlog_requests = 8;  // pending requests from which everything batches
+    Clock::time_point last_backlog = Clock::now() - std::chrono::hours(1);
     bool plain = false;
     fc_batch_options bopt{};
 
@@ -163,6 +168,8 @@ struct fc_server {
     std::set<fc_graph*> running_graphs;  // graphs of the batches on the device
     uint64_t running_bytes = 0;          // their scratch and not yet resident copies
     uint32_t running_requests = 0;
+    uint32_t free_sms = 0;               // SMs no running peel grid claims
+    bool heavy_running = false;
     bool stop = false;
     std::vector<std::thread> threads;
 
@@ -187,68 +194,148 @@ struct fc_server {
         st.requests_done++;
     }
 
-    // Takes the requests of the next batch out of `pending` (under mu).
-    // Returns the distinct graphs and the bytes the batch reserves (its
-    // scratch and the copies of graphs not yet resident).  Graphs released to
+    // Edge visits of a request (every lambda column visits every entry).
+    bool is_heavy(const Request* r) const {
+        return !plain && r->g->total_entries() * (uint64_t)r->g->L >= heavy_visits;
+    }
+
+    // Memory admission of the graph of r, not yet in the batch (under mu):
+    // 0 = admitted (`used` and the batch's `reserve` grow), 1 = can never fit
+    // (r finished with FC_ERR_BUDGET), 2 = no room now.  Graphs released to
     // make room are released here, under the lock, so that no other lane can
     // take one of them meanwhile; their last work has completed (every batch
     // ends with a stream synchronize), so the release does not wait.
-    void form_batch(std::vector<Request*>* batch, std::vector<fc_graph*>* graphs,
-                    uint64_t* reserve) {
+    int admit(Request* r, uint64_t* used, const std::set<fc_graph*>& taken, uint64_t* reserve) {
+        fc_graph* g = r->g;
+        const uint64_t gb = fc::graph_bytes(g);
+        const uint64_t wb = plain ? fc::peel_ws_bytes(g->n, g->L, g->total_entries(), 1)
+                                  : fc::batch_peel_ws_bytes(&g, 1);
+        if (gb + wb > budget) {
+            finish(r, FC_ERR_BUDGET);
+            cv_done.notify_all();
+            return 1;
+        }
+        const uint64_t need = (fc::residency_has(&res, g) ? 0 : gb) + wb;
+        if (*used + need > budget) {
+            // release resident graphs that nothing running or taken uses
+            std::set<fc_graph*> keep(running_graphs);
+            keep.insert(taken.begin(), taken.end());
+            keep.insert(g);
+            auto victims = fc::residency_victims(&res, keep, *used + need - budget);
+            uint64_t freed = 0;
+            for (auto& v : victims) freed += v.second;
+            if (*used + need > budget + freed) return 2;
+            for (auto& v : victims) fc::release_device(v.first, false);
+            *used -= freed;
+            st.evictions += victims.size();
+        }
+        *used += need;
+        *reserve += need;
+        return 0;
+    }
+
+    struct Plan {
+        std::vector<Request*> reqs;
+        std::vector<fc_graph*> graphs;
+        uint64_t reserve = 0;  // bytes: scratch and copies not yet resident
+        uint32_t sms = 0;      // SMs the peel grid may cover (0 = all)
+        bool heavy = false;
+    };
+
+    // Takes the requests of the next batch out of `pending` (under mu).
+    //   * While few requests wait (fewer than backlog_requests, and not so
+    //     for the last second either), a heavy request
+    //     (heavy_visits or more) runs alone -- with the other pending
+    //     requests of its graph -- on heavy_sms SMs, one at a time, in arrival
+    //     order among heavy requests: its latency is most of the tail.  Light
+    //     batches then leave a waiting heavy request its SMs, taking only
+    //     what is free beyond them, so it waits at most for the batches
+    //     already running.
+    //   * With a backlog, every request batches in arrival order: a batch
+    //     of many graphs shares its level loop, which is what keeps up with
+    //     the load.
+    //   * Every other batch takes at most half of the SMs (and at least a
+    //     quarter, which a running heavy request leaves), so that two
+    //     batches, their uploads and densest searches overlap on the device.
+    // The grids of concurrent batches never claim more SMs than the device
+    // has, so every persistent grid is resident as soon as it launches.
+    void form_batch(Plan* p) {
         uint64_t used = fc::residency_bytes(&res) + running_bytes;
         std::set<fc_graph*> taken;
+        Request* waiting_heavy = nullptr;
+        const Clock::time_point now = Clock::now();
+        if (pending.size() >= backlog_requests) last_backlog = now;
+        const bool backlog = now - last_backlog < std::chrono::milliseconds(1000);
+        if (!plain && !heavy_running && !backlog) {
+            for (auto it = pending.begin(); it != pending.end(); ++it)
+                if (is_heavy(*it) && !running_graphs.count((*it)->g)) {
+                    waiting_heavy = *it;
+                    break;
+                }
+        }
+        if (waiting_heavy && free_sms >= heavy_sms &&
+            running_requests < max_inflight) {
+            Request* h = waiting_heavy;
+            const int a = admit(h, &used, taken, &p->reserve);
+            if (a == 1) {
+                pending.erase(std::find(pending.begin(), pending.end(), h));
+                return;  // rejected; the lane looks again
+            }
+            if (a == 0) {
+                for (auto it = pending.begin(); it != pending.end();) {
+                    if ((*it)->g == h->g) {
+                        p->reqs.push_back(*it);
+                        it = pending.erase(it);
+                    } else {
+                        ++it;
+                    }
+                }
+                p->graphs.push_back(h->g);
+                p->sms = heavy_sms;
+                p->heavy = true;
+                return;
+            }
+        }
+        uint32_t cap = std::min(free_sms, std::max(min_light_sms, sms / 2));
+        if (!plain) {
+            if (waiting_heavy) cap = free_sms > heavy_sms ? std::min(cap, free_sms - heavy_sms) : 0;
+            if (cap < min_light_sms) return;
+        }
         for (auto it = pending.begin(); it != pending.end();) {
             Request* r = *it;
-            if (running_graphs.count(r->g)) {  // running on another lane
+            // running on another lane, or a heavy request that runs alone later
+            if (running_graphs.count(r->g) || (!backlog && is_heavy(r))) {
                 ++it;
                 continue;
             }
             if (taken.count(r->g)) {  // shares the peel of a graph already taken
                 if (plain) break;
-                batch->push_back(r);
+                p->reqs.push_back(r);
                 it = pending.erase(it);
                 continue;
             }
-            if (graphs->size() >= max_batch_graphs ||
-                running_requests + batch->size() >= max_inflight)
+            if (p->graphs.size() >= max_batch_graphs ||
+                running_requests + p->reqs.size() >= max_inflight)
                 break;
-            fc_graph* g = r->g;
-            const uint64_t gb = fc::graph_bytes(g);
-            const uint64_t wb = plain ? fc::peel_ws_bytes(g->n, g->L, g->total_entries(), 1)
-                                      : fc::batch_peel_ws_bytes(&g, 1);
-            if (gb + wb > budget) {
-                finish(r, FC_ERR_BUDGET);
+            const int a = admit(r, &used, taken, &p->reserve);
+            if (a == 1) {
                 it = pending.erase(it);
-                cv_done.notify_all();
                 continue;
             }
-            const uint64_t need = (fc::residency_has(&res, g) ? 0 : gb) + wb;
-            if (used + need > budget) {
-                // release resident graphs that nothing running or taken uses
-                std::set<fc_graph*> keep(running_graphs);
-                keep.insert(taken.begin(), taken.end());
-                keep.insert(g);
-                auto victims = fc::residency_victims(&res, keep, used + need - budget);
-                uint64_t freed = 0;
-                for (auto& v : victims) freed += v.second;
-                if (used + need > budget + freed) break;  // wait for memory, in order
-                for (auto& v : victims) fc::release_device(v.first, false);
-                used -= freed;
-                st.evictions += victims.size();
-            }
-            used += need;
-            *reserve += need;
-            taken.insert(g);
-            graphs->push_back(g);
-            batch->push_back(r);
+            if (a == 2) break;  // wait for memory, in order
+            taken.insert(r->g);
+            p->graphs.push_back(r->g);
+            p->reqs.push_back(r);
             it = pending.erase(it);
             if (plain) break;
         }
+        p->sms = plain ? 0 : cap;
     }
 
     // The device work of one batch on the lane's stream.
-    fc_status run_batch(cudaStream_t s, const std::vector<Request*>& batch,
-                        const std::vector<fc_graph*>& graphs) {
+    fc_status run_batch(cudaStream_t s, const Plan& p) {
+        const std::vector<Request*>& batch = p.reqs;
+        const std::vector<fc_graph*>& graphs = p.graphs;
         for (fc_graph* g : graphs) {
             const bool had = g->dev != nullptr;
             FC_TRY(fc::upload(g, s));
@@ -262,8 +349,7 @@ struct fc_server {
             uint32_t launches = 0, levels = 0;
             FC_TRY(fc::batch_plain_one(graphs[0], s, &ms, &launches, &levels));
         } else {
-            FC_TRY(fc::batch_peel(graphs.data(), (uint32_t)graphs.size(), &bopt, lane_sms, nullptr,
-                                  s));
+            FC_TRY(fc::batch_peel(graphs.data(), (uint32_t)graphs.size(), &bopt, p.sms, nullptr, s));
         }
         // densest: every request's beta, one pass per graph
         for (fc_graph* g : graphs) {
@@ -307,36 +393,39 @@ struct fc_server {
         cudaGetLastError();
         fc::set_thread_staging(&stage);
         for (;;) {
-            std::vector<Request*> batch;
-            std::vector<fc_graph*> graphs;
-            uint64_t reserve = 0;
+            Plan p;
             {
                 std::unique_lock<std::mutex> lk(mu);
                 for (;;) {
                     if (stop && pending.empty()) break;
                     if (!pending.empty()) {
-                        form_batch(&batch, &graphs, &reserve);
-                        if (!batch.empty()) break;
+                        form_batch(&p);
+                        if (!p.reqs.empty()) break;
                     }
                     // nothing to take now: wait for an arrival or a completion
                     cv_work.wait_for(lk, std::chrono::milliseconds(100));
                 }
-                if (batch.empty()) break;  // stopped and nothing pending
-                for (fc_graph* g : graphs) running_graphs.insert(g);
-                running_bytes += reserve;
-                running_requests += (uint32_t)batch.size();
+                if (p.reqs.empty()) break;  // stopped and nothing pending
+                for (fc_graph* g : p.graphs) running_graphs.insert(g);
+                running_bytes += p.reserve;
+                running_requests += (uint32_t)p.reqs.size();
+                if (!plain) free_sms -= p.sms;
+                if (p.heavy) {
+                    heavy_running = true;
+                    st.heavy_batches++;
+                }
                 st.peak_bytes = std::max(st.peak_bytes, fc::residency_bytes(&res) + running_bytes);
                 clock_advance();
                 running_lanes++;
                 st.batches++;
-                st.graphs_peeled += graphs.size();
-                st.max_batch = std::max<uint32_t>(st.max_batch, (uint32_t)batch.size());
+                st.graphs_peeled += p.graphs.size();
+                st.max_batch = std::max<uint32_t>(st.max_batch, (uint32_t)p.reqs.size());
             }
-            const fc_status rc = run_batch(s, batch, graphs);
+            const fc_status rc = run_batch(s, p);
             if (rc != FC_OK) cudaStreamSynchronize(s);  // what was enqueued has finished
             // nothing is left in flight on the lane's stream, which goes away
             // with the server while the graphs may live on
-            for (fc_graph* g : graphs) {
+            for (fc_graph* g : p.graphs) {
                 if (!g->dev) continue;
                 g->dev->home = nullptr;
                 fc::residency_touch(&res, g, fc::graph_bytes(g));
@@ -345,10 +434,12 @@ struct fc_server {
                 std::lock_guard<std::mutex> lk(mu);
                 clock_advance();
                 running_lanes--;
-                for (fc_graph* g : graphs) running_graphs.erase(g);
-                running_bytes -= reserve;
-                running_requests -= (uint32_t)batch.size();
-                for (Request* r : batch) finish(r, rc);
+                for (fc_graph* g : p.graphs) running_graphs.erase(g);
+                running_bytes -= p.reserve;
+                running_requests -= (uint32_t)p.reqs.size();
+                if (!plain) free_sms += p.sms;
+                if (p.heavy) heavy_running = false;
+                for (Request* r : p.reqs) finish(r, rc);
             }
             cv_done.notify_all();
             cv_work.notify_all();
@@ -374,10 +465,13 @@ fc_status fc_server_create(const fc_server_options* opt, fc_server** out) {
     // every kernel loaded now: a kernel's first load may wait for kernels
     // running on other lanes
     fc::preload_kernels();
-    int dev = 0, sms = 148;
+    int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    s->lane_sms = s->lanes > 1 ? std::max(1u, (uint32_t)sms / s->lanes) : 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    s->sms = s->free_sms = (uint32_t)(nsm > 0 ? nsm : 148);
+    s->min_light_sms = std::max(1u, s->sms / 4);
+    s->heavy_sms = s->sms - s->min_light_sms;
+    s->heavy_visits = (opt && opt->heavy_visits) ? opt->heavy_visits : 1000000000ull;
     // fixed launch shape: serving does not stop to autotune every new mix
     s->bopt.block_threads = (opt && opt->block_threads) ? opt->block_threads : 1024;
     s->bopt.hub_threshold = (opt && opt->hub_threshold) ? opt->hub_threshold : 64;

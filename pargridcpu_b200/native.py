@@ -81,12 +81,12 @@ class ServerOptions(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_inflight", C.c_uint32),
                 ("lanes", C.c_uint32), ("max_batch_graphs", C.c_uint32),
                 ("block_threads", C.c_uint32), ("hub_threshold", C.c_uint32),
-                ("plain", C.c_int)]
+                ("plain", C.c_int), ("heavy_visits", C.c_uint64)]
 
 
 class ServerStats(C.Structure):
     _fields_ = [("requests_done", C.c_uint64), ("batches", C.c_uint64),
-                ("graphs_peeled", C.c_uint64), ("uploads", C.c_uint64),
+                ("heavy_batches", C.c_uint64), ("graphs_peeled", C.c_uint64), ("uploads", C.c_uint64),
                 ("evictions", C.c_uint64), ("resident_bytes", C.c_uint64),
                 ("peak_bytes", C.c_uint64), ("busy_ms", C.c_double), ("overlap_ms", C.c_double),
                 ("max_batch", C.c_uint32), ("lanes", C.c_uint32)]
