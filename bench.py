@@ -356,15 +356,22 @@ def run_ours(args, world, rank, local):
 def run_batch(args, world, rank, local):
     """The 256-graph mix: every (graph, lambda) column in one persistent launch
     (batched form) against one graph and one column per launch (plain form),
-    same graphs, tables compared.  Each rank takes every world-th graph."""
+    same graphs, tables compared.  Under torchrun each rank takes the graphs
+    the work-balanced assignment gives it (no collective in the data path)."""
+    import multiprocessing as mp
     import torch
-    from concurrent.futures import ThreadPoolExecutor
-    from pargridcpu_b200 import MultilayerGraph, batch_run, synth
+    from concurrent.futures import ProcessPoolExecutor, ThreadPoolExecutor
+    from pargridcpu_b200 import MultilayerGraph, batch_run, shard, synth
 
     torch.cuda.set_device(local)
     t0 = time.time()
-    gens = synth.batch_mix(count=args.batch_count, seed=404,
-                           workers=os.cpu_count() or 1)[rank::world]
+    params = synth.batch_params(count=args.batch_count, seed=404)
+    works = [shard.graph_work(p["n"], p["n_layers"], 2 * p["m_per_layer"] * p["n_layers"])
+             for p in params]
+    owner = shard.assign_graphs(works, world)
+    mine = [p for p, r in zip(params, owner) if r == rank]
+    with ProcessPoolExecutor(os.cpu_count() or 1, mp_context=mp.get_context("spawn")) as ex:
+        gens = list(ex.map(synth._make, mine, chunksize=1))
     with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
         graphs = list(ex.map(lambda g: MultilayerGraph.from_pairs(g.layers), gens))
     del gens
@@ -421,7 +428,8 @@ def run_batch(args, world, rank, local):
                                    "[2,32], gamma U[2,3], copy U[0,0.6], seed 404; full fcgrid "
                                    "+ densest(beta) per graph",
                        "graphs": len(graphs), "edge_visits_per_step": visits, "beta": args.beta,
-                       "parallelism": "graphs split over ranks" if world > 1 else "single GPU"},
+                       "parallelism": ("graphs split over ranks by work (LPT)" if world > 1
+                                       else "single GPU")},
             "batched": {"ms": ms, "report": rep},
             "plain": {"ms": plain_ms, "report": plain_rep,
                       "form": "one graph and one lambda column per launch, one after another"},
