@@ -241,9 +241,16 @@ __device__ void leader_step(volatile PeelCtl* c, const PeelJob& j) {
             c->phase = PH_DONE;
         }
     };
+    // the run's deadline, checked at every phase change after the first
+    if (c->phase == PH_INIT) c->t_start = c->t_last;
+    else if (c->t_last - c->t_start > j.deadline_ns) c->err = ERR_DEADLINE;
+    if (c->err) {
+        c->err_level = c->level;
+        c->phase = PH_DONE;
+        return;
+    }
     switch (c->phase) {
         case PH_INIT:  // degree tables copied: the first scan follows
-            c->t_start = c->t_last;
             c->phase = PH_SCAN;
             break;
         case PH_SCAN:  // the first scan wrote alive[1]

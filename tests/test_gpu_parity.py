@@ -14,7 +14,7 @@ import pytest
 
 import golden_cases as G
 import oracle as O
-from pargridcpu_b200 import MultilayerGraph, synth
+from pargridcpu_b200 import MultilayerGraph, native, synth
 
 pytestmark = pytest.mark.gpu
 
@@ -135,6 +135,19 @@ C3_FIXTURE = os.path.join(os.path.dirname(__file__), "golden", "c3.npz")
 
 
 @pytest.mark.skipif(not os.path.exists(C3_FIXTURE), reason="c3 fixture not generated")
+def test_deadline_ends_the_run_with_an_error_and_the_device_stays_usable(monkeypatch):
+    """Every wait and loop of the peel kernel is bounded by the run's
+    deadline: a run past it ends with an error status (no fault, no trap),
+    and the next call on the same context gets the reference's table."""
+    g = MultilayerGraph.from_pairs(G.inputs("c1"))
+    monkeypatch.setenv("FC_PEEL_DEADLINE_MS", "0")
+    with pytest.raises(native.FcError) as e:
+        g.coreindex()
+    assert e.value.code == 6  # FC_ERR_ITER_LIMIT
+    monkeypatch.delenv("FC_PEEL_DEADLINE_MS")
+    assert np.array_equal(g.coreindex(), G.expected("c1")["table"])
+
+
 def test_c3_full_size():
     """The 2.5M-node, 34M-edge, 4-layer configuration at full size: table hash
     and densest results against the reference's own output."""
