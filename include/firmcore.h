@@ -174,7 +174,7 @@ typedef struct fc_batch_options {
 /* What a batch run did (any pointer field may be ignored). */
 typedef struct fc_batch_report {
     double peel_ms;            /* device time of the peel launch(es), CUDA events */
-    double densest_ms;         /* device time of the densest searches */
+    double densest_ms;         /* time of the densest searches (they overlap on streams) */
     uint32_t peel_launches;
     uint32_t block_threads;    /* the configuration used */
     uint32_t hub_threshold;

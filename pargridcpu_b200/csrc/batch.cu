@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <map>
 #include <mutex>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -43,20 +44,86 @@ static bool debug_on() {
         }                                         \
     } while (0)
 
+// The densest searches of a batch run on DENSE_WORKERS host threads, each
+// with its own stream and pinned staging buffer: one graph's search is a few
+// small kernels separated by host round trips, so the graphs' searches
+// overlap on the device.  The pool is per device and process-wide; batches
+// from several callers take turns on it.
+static constexpr uint32_t DENSE_WORKERS = 8;
+struct DenseWorker {
+    cudaStream_t s = nullptr;
+    Staging stage;
+};
+static std::mutex g_dw_mu, g_dw_run_mu;
+static std::map<int, std::vector<DenseWorker>> g_dw;
+
+static std::vector<DenseWorker>* dense_workers() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> lk(g_dw_mu);
+    std::vector<DenseWorker>& v = g_dw[dev];
+    if (v.empty()) {
+        v.resize(DENSE_WORKERS);
+        for (DenseWorker& w : v) {
+            if (cudaStreamCreateWithFlags(&w.s, cudaStreamNonBlocking) != cudaSuccess) w.s = nullptr;
+            if (cudaHostAlloc(&w.stage.p, 1u << 20, cudaHostAllocDefault) == cudaSuccess)
+                w.stage.cap = 1u << 20;
+            else
+                w.stage.p = nullptr;
+        }
+        cudaGetLastError();
+    }
+    for (const DenseWorker& w : v)
+        if (!w.s) return nullptr;
+    return &v;
+}
+
 static fc_status densest_all(fc_graph* const* gs, uint32_t count, double beta,
                              fc_densest_result* res, cudaStream_t s, double* ms) {
     *ms = 0;
+    if (!res) return FC_OK;
+    std::vector<uint32_t> todo;
     for (uint32_t i = 0; i < count; i++) {
-        fc_graph* g = gs[i];
-        if (!res) continue;
-        if (g->n && g->L) {
-            BATCH_TRACE("densest graph %u (n %u, L %u)", i, g->n, g->L);
-            FC_TRY(densest(g, &beta, 1, res + i, s));
-            *ms += g->dev->stats.densest_ms;
+        if (gs[i]->n && gs[i]->L) {
+            todo.push_back(i);
         } else {
             res[i] = fc_densest_result{};
             res[i].beta = beta;
         }
+    }
+    std::vector<DenseWorker>* pool = todo.size() >= 4 ? dense_workers() : nullptr;
+    if (!pool) {  // a few graphs: one after another on the caller's stream
+        for (uint32_t i : todo) {
+            BATCH_TRACE("densest graph %u (n %u, L %u)", i, gs[i]->n, gs[i]->L);
+            FC_TRY(densest(gs[i], &beta, 1, res + i, s));
+            *ms += gs[i]->dev->stats.densest_ms;
+        }
+        return FC_OK;
+    }
+    std::lock_guard<std::mutex> lk(g_dw_run_mu);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint32_t nw = (uint32_t)std::min<size_t>(pool->size(), todo.size());
+    std::vector<fc_status> rc(nw, FC_OK);
+    std::vector<double> wms(nw, 0.0);
+    std::vector<std::thread> th;
+    for (uint32_t w = 0; w < nw; w++) {
+        th.emplace_back([&, w] {
+            cudaSetDevice(dev);
+            DenseWorker& me = (*pool)[w];
+            set_thread_staging(me.stage.p ? &me.stage : nullptr);
+            for (size_t k = w; k < todo.size() && rc[w] == FC_OK; k += nw) {
+                fc_graph* g = gs[todo[k]];
+                rc[w] = densest(g, &beta, 1, res + todo[k], me.s);
+                if (rc[w] == FC_OK) wms[w] += g->dev->stats.densest_ms;
+            }
+            set_thread_staging(nullptr);
+        });
+    }
+    for (auto& t : th) t.join();
+    for (uint32_t w = 0; w < nw; w++) {
+        FC_TRY(rc[w]);
+        *ms += wms[w];
     }
     return FC_OK;
 }
@@ -84,7 +151,10 @@ static fc_status batch_plain(fc_graph* const* gs, uint32_t count, double beta,
     for (uint32_t i = 0; i < count; i++)
         FC_TRY(batch_plain_one(gs[i], s, &peel_ms, &launches, &levels));
     double dms = 0;
+    const auto t_dense = std::chrono::steady_clock::now();
     FC_TRY(densest_all(gs, count, beta, res, s, &dms));
+    dms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_dense)
+              .count();
     FC_TRY(copy_tables(gs, count, tables, s));
     if (rep) {
         rep->peel_ms = peel_ms;
@@ -268,7 +338,10 @@ static fc_status batch_persistent(fc_graph* const* gs, uint32_t count, double be
                                   cudaStream_t s) {
     FC_TRY(batch_peel(gs, count, opt, 0, rep, s));
     double dms = 0;
+    const auto t_dense = std::chrono::steady_clock::now();
     FC_TRY(densest_all(gs, count, beta, res, s, &dms));
+    dms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_dense)
+              .count();
     FC_TRY(copy_tables(gs, count, tables, s));
     if (rep) rep->densest_ms = dms;
     return FC_OK;

@@ -394,12 +394,10 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st) {
         FC_CUDA_TRY(cudaGetLastError());
         // lambda groups whose bins fit the shared-memory budget
         const uint32_t SH_WORDS = 48 * 1024;  // 192 KB
-        static bool attr_set = false;
-        if (!attr_set) {
-            FC_CUDA_TRY(cudaFuncSetAttribute(k_edge_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             SH_WORDS * 4));
-            attr_set = true;
-        }
+        // once per process (thread-safe static initialisation)
+        static const cudaError_t attr_rc = cudaFuncSetAttribute(
+            k_edge_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, SH_WORDS * 4);
+        FC_CUDA_TRY(attr_rc);
         FastDiv divL;
         divL.init(L);
         const int blocks = sm_count();
