@@ -2,6 +2,8 @@
 // (Graph/MultilayerGraph.cpp:47-166) and Graph::BuildFromEdgeLst's CSR
 // (Graph/Graph.cpp:17-50), producing fc_graph's host CSR.
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -198,6 +200,25 @@ void build_layer(uint32_t n, const std::vector<uint32_t>& dir_pairs, std::vector
     off[n] = adj.size();
 }
 
+// f(l) for every layer l, on up to one host thread per core (layers are
+// independent once their ids are assigned).
+template <class F>
+void for_each_layer(uint32_t L, F f) {
+    unsigned hw = std::thread::hardware_concurrency();
+    const uint32_t nt = std::min<uint32_t>(L, hw ? hw : 4);
+    if (nt <= 1) {
+        for (uint32_t l = 0; l < L; l++) f(l);
+        return;
+    }
+    std::atomic<uint32_t> next{0};
+    std::vector<std::thread> th;
+    for (uint32_t t = 0; t < nt; t++)
+        th.emplace_back([&] {
+            for (uint32_t l; (l = next.fetch_add(1)) < L;) f(l);
+        });
+    for (auto& t : th) t.join();
+}
+
 fc_status finish(uint32_t n, uint32_t L, std::vector<std::vector<uint32_t>>& dir_pairs, fc_graph* g) {
     g->n = n;
     g->L = L;
@@ -205,20 +226,19 @@ fc_status finish(uint32_t n, uint32_t L, std::vector<std::vector<uint32_t>>& dir
     for (uint32_t i = 0; i < L; i++) g->order[i] = i;
     std::vector<std::vector<uint64_t>> offs(L);
     std::vector<std::vector<uint32_t>> adjs(L);
-    uint64_t total = 0;
-    for (uint32_t l = 0; l < L; l++) {
+    for_each_layer(L, [&](uint32_t l) {
         build_layer(n, dir_pairs[l], offs[l], adjs[l]);
         std::vector<uint32_t>().swap(dir_pairs[l]);
-        total += adjs[l].size();
-    }
-    if (!g->off.alloc((uint64_t)L * (n + 1)) || !g->adj.alloc(total)) return FC_ERR_OOM;
-    uint64_t base = 0;
-    for (uint32_t l = 0; l < L; l++) {
+    });
+    std::vector<uint64_t> base(L + 1, 0);
+    for (uint32_t l = 0; l < L; l++) base[l + 1] = base[l] + adjs[l].size();
+    if (!g->off.alloc((uint64_t)L * (n + 1)) || !g->adj.alloc(base[L])) return FC_ERR_OOM;
+    for_each_layer(L, [&](uint32_t l) {
         uint64_t* o = g->off.p + (uint64_t)l * (n + 1);
-        for (uint32_t v = 0; v <= n; v++) o[v] = base + offs[l][v];
-        if (!adjs[l].empty()) memcpy(g->adj.p + base, adjs[l].data(), adjs[l].size() * 4);
-        base += adjs[l].size();
-    }
+        for (uint32_t v = 0; v <= n; v++) o[v] = base[l] + offs[l][v];
+        if (!adjs[l].empty()) memcpy(g->adj.p + base[l], adjs[l].data(), adjs[l].size() * 4);
+        std::vector<uint32_t>().swap(adjs[l]);
+    });
     return FC_OK;
 }
 
@@ -259,22 +279,31 @@ fc_status load_dir(const std::string& dir, int order, bool write_vtx_map, fc_gra
         }
     }
     uint32_t L = (uint32_t)files.size();
+    // read and parse the layer files in parallel; ids are then handed out in
+    // one pass in file order, as the reference's sequential load does
+    std::vector<std::vector<uint32_t>> raw(L);
+    std::vector<char> io_ok(L, 0);
+    for_each_layer(L, [&](uint32_t l) {
+        std::vector<char> text;
+        if (!read_file(dir + files[l], text)) return;
+        parse_pairs(text, raw[l]);
+        io_ok[l] = 1;
+    });
+    for (uint32_t l = 0; l < L; l++)
+        if (!io_ok[l]) return FC_ERR_IO;
     IdMap map(&g->id2vtx);
     std::vector<std::vector<uint32_t>> dir_pairs(L);
-    std::vector<char> text;
-    std::vector<uint32_t> raw;
     for (uint32_t l = 0; l < L; l++) {
-        if (!read_file(dir + files[l], text)) return FC_ERR_IO;
-        parse_pairs(text, raw);
         auto& d = dir_pairs[l];
-        d.reserve(raw.size() * 2);
-        for (size_t i = 0; i < raw.size(); i += 2) {
-            uint32_t a = map.get(raw[i]), b = map.get(raw[i + 1]);
+        d.reserve(raw[l].size() * 2);
+        for (size_t i = 0; i < raw[l].size(); i += 2) {
+            uint32_t a = map.get(raw[l][i]), b = map.get(raw[l][i + 1]);
             d.push_back(a);
             d.push_back(b);
             d.push_back(b);
             d.push_back(a);
         }
+        std::vector<uint32_t>().swap(raw[l]);
     }
     if (write_vtx_map) {
         // `u uid` per new id, in assignment order (MultilayerGraph.cpp:131,139)
