@@ -147,6 +147,14 @@ fc_status fc_densest(fc_graph* g, const double* betas, uint32_t n_betas, fc_dens
  * on the same graph.  Either pointer may be NULL. */
 fc_status fc_densest_members(fc_graph* g, const fc_densest_result* res, uint32_t* nodes,
                              uint32_t* layers, void* stream);
+/* Node set of any cell, C_{k,lambda} = {v : core_lambda(v) >= k}, in
+ * ascending internal ids: the query of `-m kpe -k K -lmd L` (main.cpp:
+ * 197-225) that FCTree::saveCoreToLocal writes out (Core/FCTree.cpp:138-153).
+ * Writes min(cap, count) ids; *count receives |C|.  k = 0 gives every node;
+ * lmd must be in 1..L.  Runs fc_coreindex first when the table is not
+ * resident. */
+fc_status fc_cell_members(fc_graph* g, uint32_t k, uint32_t lmd, uint32_t* nodes, uint32_t cap,
+                          uint32_t* count, void* stream);
 /* Every non-empty cell with its best density for `beta`, in the reference's
  * order (lambda-major, k ascending), as its fcgrid trees hold them
  * (coreNode / coreNodeP: k, lmd, length, layer_density, num_select_layer).

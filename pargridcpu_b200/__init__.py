@@ -187,6 +187,15 @@ class MultilayerGraph:
                                              None), "densest_members")
         return nodes[:r.length], layers[:r.lstar]
 
+    def cell_members(self, k, lmd, stream=None):
+        """C_{k,lmd} = {v : core_lmd(v) >= k}, ascending internal ids (the
+        `-m kpe -k -lmd` query, FCTree::saveCoreToLocal)."""
+        nodes = np.zeros(max(self.n, 1), np.uint32)
+        cnt = C.c_uint32()
+        _n.check(_n.lib().fc_cell_members(self._h, int(k), int(lmd), _n.ptr(nodes), self.n,
+                                          C.byref(cnt), _n.stream_handle(stream)), "cell_members")
+        return nodes[:cnt.value].copy()
+
     def cells(self, beta=1.0):
         cnt = C.c_uint32()
         _n.check(_n.lib().fc_cells(self._h, float(beta), None, 0, C.byref(cnt), None), "cells")

@@ -203,6 +203,18 @@ fc_status fc_densest_members(fc_graph* g, const fc_densest_result* res, uint32_t
     return densest_members(g, res, nodes, layers, (cudaStream_t)stream);
 }
 
+fc_status fc_cell_members(fc_graph* g, uint32_t k, uint32_t lmd, uint32_t* nodes, uint32_t cap,
+                          uint32_t* count, void* stream) {
+    if (!g) return FC_ERR_INVALID;
+    if (!cuda_available()) return FC_ERR_NO_DEVICE;
+    if (lmd < 1 || lmd > g->L) return FC_ERR_INVALID;
+    if (!g->n) {
+        if (count) *count = 0;
+        return FC_OK;
+    }
+    return cell_members(g, k, lmd, nodes, cap, count, (cudaStream_t)stream);
+}
+
 fc_status fc_cells(fc_graph* g, double beta, fc_cell* cells_out, uint32_t cap, uint32_t* count,
                    void* stream) {
     if (!g) return FC_ERR_INVALID;

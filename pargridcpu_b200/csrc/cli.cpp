@@ -177,9 +177,13 @@ int main(int argc, char* argv[]) {
         if (k != 0 && lmd != 0) {
             cout << k << " " << lmd << endl;
             std::vector<uint32_t> cell;
-            if (lmd <= L)
-                for (uint32_t v = 0; v < n; v++)
-                    if (table[(size_t)(lmd - 1) * n + v] >= k) cell.push_back(v);
+            if (lmd >= 1 && (uint32_t)lmd <= L) {
+                cell.resize(n);
+                uint32_t cnt = 0;
+                s = fc_cell_members(g, (uint32_t)k, (uint32_t)lmd, cell.data(), n, &cnt, nullptr);
+                if (s != FC_OK) return fail(method.c_str(), s);
+                cell.resize(cnt);
+            }
             if (cell.empty()) {
                 cout << "No statisfy result" << endl;
             } else {

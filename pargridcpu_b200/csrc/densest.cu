@@ -16,6 +16,10 @@
 // maximum (Core/FCTree.cpp:69-82, main.cpp:406).  pow(l, beta) comes from the
 // host's libm, as in the reference; every other step is IEEE FP32/FP64
 // arithmetic in the same order, so densities are bit-identical.
+#include <thrust/iterator/counting_iterator.h>
+
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -529,6 +533,51 @@ fc_status densest_members(fc_graph* g, const fc_densest_result* r, uint32_t* nod
 void invalidate_densest(DeviceGraph* d) {
     DensState* s = (DensState*)d->dens;
     if (s) s->hist_valid = false;
+}
+
+// C_{k,lambda} = {v : core_lambda(v) >= k} in ascending ids, by an
+// order-preserving stream compaction of the lambda column on the device (the
+// query of -m kpe -k -lmd, main.cpp:197-225 and FCTree::saveCoreToLocal,
+// Core/FCTree.cpp:138-153).
+struct InCell {
+    const uint32_t* col;
+    uint32_t k;
+    __host__ __device__ __forceinline__ bool operator()(uint32_t v) const { return col[v] >= k; }
+};
+
+fc_status cell_members(fc_graph* g, uint32_t k, uint32_t lmd, uint32_t* nodes, uint32_t cap,
+                       uint32_t* count, cudaStream_t st) {
+    if (lmd < 1 || lmd > g->L) return FC_ERR_INVALID;
+    FC_TRY(coreindex(g, nullptr, false, st));
+    DeviceGraph* d = g->dev;
+    const uint32_t n = d->n;
+    uint32_t* out = nullptr;
+    uint32_t* num = nullptr;
+    void* tmp = nullptr;
+    size_t tb = 0;
+    const InCell pred{d->table + (uint64_t)(lmd - 1) * n, k};
+    thrust::counting_iterator<uint32_t> ids(0);
+    FC_CUDA_TRY(cub::DeviceSelect::If(nullptr, tb, ids, out, num, (int)n, pred, st));
+    fc_status rc = dev_alloc((void**)&out, (uint64_t)n * 4 + 4, st);
+    if (rc == FC_OK) rc = dev_alloc((void**)&num, 8, st);
+    if (rc == FC_OK) rc = dev_alloc(&tmp, tb + 16, st);
+    uint32_t total = 0;
+    if (rc == FC_OK) {
+        const cudaError_t e = cub::DeviceSelect::If(tmp, tb, ids, out, num, (int)n, pred, st);
+        count_launch(1);
+        if (e != cudaSuccess) {
+            set_last_cuda_error(e, "DeviceSelect::If", __FILE__, __LINE__);
+            rc = FC_ERR_DEVICE;
+        }
+    }
+    if (rc == FC_OK) rc = to_host(&total, num, 4, st);
+    if (rc == FC_OK && nodes && total)
+        rc = to_host(nodes, out, (size_t)std::min(total, cap) * 4, st);
+    dev_free(tmp, st);
+    dev_free(num, st);
+    dev_free(out, st);
+    if (count) *count = total;
+    return rc;
 }
 
 void densest_preload() {

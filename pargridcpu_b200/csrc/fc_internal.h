@@ -79,6 +79,8 @@ fc_status densest_members(fc_graph* g, const fc_densest_result* r, uint32_t* nod
                           uint32_t* layers, cudaStream_t s);
 fc_status cells(fc_graph* g, double beta, fc_cell* out, uint32_t cap, uint32_t* count,
                 cudaStream_t s);
+fc_status cell_members(fc_graph* g, uint32_t k, uint32_t lmd, uint32_t* nodes, uint32_t cap,
+                       uint32_t* count, cudaStream_t s);
 fc_status batch_run(fc_graph* const* gs, uint32_t count, double beta, uint32_t* const* tables,
                     fc_densest_result* res, const fc_batch_options* opt, fc_batch_report* rep,
                     cudaStream_t s);

@@ -135,6 +135,22 @@ C3_FIXTURE = os.path.join(os.path.dirname(__file__), "golden", "c3.npz")
 
 
 @pytest.mark.skipif(not os.path.exists(C3_FIXTURE), reason="c3 fixture not generated")
+@pytest.mark.parametrize("name", ["c1", "layers33", "hubs"])
+def test_cell_members(name):
+    """Any cell's node set from the device table equals {v : core >= k} of
+    the reference's table, for k across the column's range and beyond."""
+    exp = G.expected(name)["table"]
+    g = MultilayerGraph.from_pairs(G.inputs(name))
+    for lmd in sorted({1, 2, g.L // 2 + 1, g.L}):
+        col = exp[lmd - 1]
+        kmax = int(col.max())
+        for k in sorted({0, 1, kmax // 2, kmax, kmax + 1}):
+            want = np.nonzero(col >= k)[0].astype(np.uint32)
+            assert np.array_equal(g.cell_members(k, lmd), want), (lmd, k)
+    with pytest.raises(native.FcError):
+        g.cell_members(1, g.L + 1)
+
+
 def test_deadline_ends_the_run_with_an_error_and_the_device_stays_usable(monkeypatch):
     """Every wait and loop of the peel kernel is bounded by the run's
     deadline: a run past it ends with an error status (no fault, no trap),
