@@ -207,70 +207,79 @@ __device__ __forceinline__ SegP seg_load(const PeelJob& j, uint32_t s) {
 
 // ---- leader step: phase transitions (one thread, all blocks parked) -------
 
-__device__ void leader_step(volatile PeelCtl* c, const PeelJob& j) {
-    {
-        uint64_t now = global_ns();
-        uint32_t kind = c->phase == PH_DRAIN ? 1 : 0;
-        if (c->t_last) c->ph_ns[kind] += now - c->t_last;
-        const uint32_t q = c->q_cur;
-        if (j.trace && c->t_last && c->level < j.trace_levels && c->phase != PH_INIT) {
-            unsigned long long* r = j.trace + 3ull * (2ull * c->level + kind);
-            r[0] = now - c->t_last;
-            r[1] = c->tail[q][QS].v + c->tail[q][QC].v;
-            r[2] = c->alive_cnt[c->alive_cur ^ (kind == 0 ? 1u : 0u)];
-        }
-        c->t_last = now;
+// The serial step between phases, run by the last block to arrive at a
+// grid barrier while all others wait.  Every field it reads is loaded in one
+// round of independent L2 loads and every result stored once: the step is on
+// the critical path of every level, twice.
+__device__ void leader_step(PeelCtl* c, const PeelJob& j) {
+    const uint64_t now = global_ns();
+    const uint32_t phase = ld_l2(&c->phase), q = ld_l2(&c->q_cur), level = ld_l2(&c->level);
+    uint32_t ac = ld_l2(&c->alive_cur);
+    uint32_t err = ld_l2(&c->err);
+    const uint32_t levels = ld_l2(&c->levels), items = ld_l2(&c->items);
+    const uint64_t t_last = ld_l2_64(&c->t_last), t_start0 = ld_l2_64(&c->t_start);
+    const uint32_t kind = phase == PH_DRAIN ? 1 : 0;
+    const uint64_t ph = ld_l2_64(&c->ph_ns[kind]);
+    const uint32_t t00 = ld_l2(&c->tail[0][QS].v), t01 = ld_l2(&c->tail[0][QC].v);
+    const uint32_t t10 = ld_l2(&c->tail[1][QS].v), t11 = ld_l2(&c->tail[1][QC].v);
+    const uint32_t ac0 = ld_l2(&c->alive_cnt[0]), ac1 = ld_l2(&c->alive_cnt[1]);
+    const uint32_t ts = q ? t10 : t00, tc = q ? t11 : t01;  // this level's reservations
+    if (t_last) __stcg((unsigned long long*)&c->ph_ns[kind], ph + (now - t_last));
+    if (j.trace && t_last && level < j.trace_levels && phase != PH_INIT) {
+        unsigned long long* r = j.trace + 3ull * (2ull * level + kind);
+        r[0] = now - t_last;
+        r[1] = ts + tc;
+        r[2] = (ac ^ (kind == 0 ? 1u : 0u)) ? ac1 : ac0;
     }
-    auto next_level = [&]() {
-        // the queues of this level are done: the other parity becomes current
-        const uint32_t q = c->q_cur;
-        c->prev_tail[QS] = c->tail[q][QS].v;
-        c->prev_tail[QC] = c->tail[q][QC].v;
-        c->q_cur = q ^ 1;
-        for (uint32_t s = 0; s < 2; s++) {
-            c->tail[q ^ 1][s].v = 0;
-            c->head[q ^ 1][s].v = 0;
-            c->processed[q ^ 1][s].v = 0;
-        }
-        c->level = c->level + 1;
-        c->levels = c->levels + 1;
-        c->alive_cnt[c->alive_cur ^ 1] = 0;
-        c->phase = PH_SCAN;
-        if (c->level > j.max_level) {
-            c->err = ERR_LIMIT;
-            c->phase = PH_DONE;
-        }
-    };
+    __stcg((unsigned long long*)&c->t_last, now);
     // the run's deadline, checked at every phase change after the first
-    if (c->phase == PH_INIT) c->t_start = c->t_last;
-    else if (c->t_last - c->t_start > j.deadline_ns) c->err = ERR_DEADLINE;
-    if (c->err) {
-        c->err_level = c->level;
-        c->phase = PH_DONE;
-        return;
+    uint32_t next = PH_DONE;
+    if (phase == PH_INIT) __stcg((unsigned long long*)&c->t_start, now);
+    else if (now - t_start0 > j.deadline_ns) err = ERR_DEADLINE;
+    bool advance = false;
+    if (!err) {
+        switch (phase) {
+            case PH_INIT:  // degree tables copied: the first scan follows
+                next = PH_SCAN;
+                break;
+            case PH_SCAN:  // the scan wrote the other alive list
+                ac ^= 1;
+                __stcg(&c->alive_cur, ac);
+                if (ts + tc > 0) next = PH_DRAIN;
+                else if ((ac ? ac1 : ac0) == 0) next = PH_DONE;
+                else advance = true;
+                break;
+            case PH_DRAIN:
+                __stcg(&c->items, items + ts + tc);
+                if ((ac ? ac1 : ac0) == 0) next = PH_DONE;
+                else advance = true;
+                break;
+            default:
+                next = PH_DONE;
+        }
     }
-    switch (c->phase) {
-        case PH_INIT:  // degree tables copied: the first scan follows
-            c->phase = PH_SCAN;
-            break;
-        case PH_SCAN:  // the first scan wrote alive[1]
-            c->alive_cur ^= 1;
-            if (c->tail[c->q_cur][QS].v + c->tail[c->q_cur][QC].v > 0) c->phase = PH_DRAIN;
-            else if (c->alive_cnt[c->alive_cur] == 0) c->phase = PH_DONE;
-            else next_level();
-            break;
-        case PH_DRAIN:
-            c->items = c->items + c->tail[c->q_cur][QS].v + c->tail[c->q_cur][QC].v;
-            if (c->alive_cnt[c->alive_cur] == 0) c->phase = PH_DONE;
-            else next_level();
-            break;
-        default:
-            c->phase = PH_DONE;
+    if (advance) {
+        // the queues of this level are done: the other parity becomes current
+        __stcg(&c->prev_tail[QS], ts);
+        __stcg(&c->prev_tail[QC], tc);
+        __stcg(&c->q_cur, q ^ 1);
+        for (uint32_t s = 0; s < 2; s++) {
+            __stcg(&c->tail[q ^ 1][s].v, 0u);
+            __stcg(&c->head[q ^ 1][s].v, 0u);
+            __stcg(&c->processed[q ^ 1][s].v, 0u);
+        }
+        __stcg(&c->level, level + 1);
+        __stcg(&c->levels, levels + 1);
+        __stcg(&c->alive_cnt[ac ^ 1], 0u);
+        next = PH_SCAN;
+        if (level + 1 > j.max_level) err = ERR_LIMIT;
     }
-    if (c->err) {
-        c->err_level = c->level;
-        c->phase = PH_DONE;
+    if (err) {
+        __stcg(&c->err, err);
+        __stcg(&c->err_level, advance ? level + 1 : level);
+        next = PH_DONE;
     }
+    __stcg(&c->phase, next);
 }
 
 // Grid barrier with a bounded wait.  Returns false once any block has
@@ -283,10 +292,10 @@ __device__ bool grid_barrier(const PeelJob& j) {
         __threadfence();
         uint32_t arrived = atom_add_acq_rel(&c->bar_count, 1);
         if (arrived == gridDim.x - 1) {
+            // the release store of the new generation orders every store of
+            // the step before it
             c->bar_count = 0;
-            __threadfence();
             leader_step(c, j);
-            __threadfence();
             st_release(&c->bar_gen, gen + 1);
         } else {
             uint64_t t0 = global_ns();
