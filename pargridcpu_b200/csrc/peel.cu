@@ -332,10 +332,11 @@ __device__ __forceinline__ void write_short(const PeelJob& j, uint32_t q, uint32
         atomicExch(&j.ctl->err, ERR_QUEUE);
 }
 
+// Chunk items c_begin .. c_end-1 of x at queue slots first, first+1, ...
 __device__ __forceinline__ void write_chunks(const PeelJob& j, uint32_t q, uint32_t first,
-                                             uint32_t x, uint32_t nch) {
-    for (uint32_t c = 0; c < nch; c++) {
-        const uint32_t idx = first + c;
+                                             uint32_t x, uint32_t c_begin, uint32_t c_end) {
+    for (uint32_t c = c_begin; c < c_end; c++) {
+        const uint32_t idx = first + (c - c_begin);
         if (idx < j.qc_cap) {
             const unsigned long long it = (unsigned long long)x | ((unsigned long long)c << 32);
             asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(j.qc[q] + idx), "l"(it)
@@ -379,19 +380,53 @@ __device__ __forceinline__ uint32_t group_count_ge(const uint32_t* row, uint32_t
     return cnt;
 }
 
+// A removed node that the warp which removed it expands next itself instead
+// of queueing it -- its whole row when short, its first chunk when long (the
+// other chunks are queued): a removal cascade then takes no queue round trip
+// per step along the warp's own chain, while the warp's other removals go to
+// the queues for the other warps.  Warp-uniform.  Such an item is never
+// reserved, so it never counts as processed; the warp must not flush its
+// processed counts while it holds one (the level could otherwise end first).
+struct Local {
+    uint32_t x;      // launch index, EMPTY32 when none
+    uint32_t chunk;  // 1: x's first chunk; 0: x's whole short row
+};
+
 // Queues the nodes this warp's lanes removed (rem[i]: launch index yg[i],
 // nch[i] chunk items or one short item when 0), with one reservation per
-// queue for the whole warp.  my_s / my_c are the lane's short / chunk item
-// counts.  All 32 lanes call it together.
+// queue for the whole warp -- except one, kept in `loc` when it is empty.
+// my_s / my_c are the lane's short / chunk item counts.  All 32 lanes call it
+// together.
 template <int N>
 __device__ __forceinline__ void enqueue_removed(const PeelJob& j, uint32_t q, const bool (&rem)[N],
                                                 const uint32_t (&yg)[N], const uint32_t (&nch)[N],
-                                                uint32_t my_s, uint32_t my_c) {
+                                                uint32_t my_s, uint32_t my_c, Local& loc) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t any = __ballot_sync(0xffffffffu, (my_s | my_c) != 0);
+    if (!any) return;
+    int keep = -1;  // on the lane that gives up an entry: that entry
+    if (loc.x == EMPTY32) {
+        const uint32_t src = __ffs(any) - 1;
+        uint32_t px = 0, pn = 0;
+        if (lane == src) {
+#pragma unroll
+            for (int i = 0; i < N; i++)
+                if (keep < 0 && rem[i]) {
+                    keep = i;
+                    px = yg[i];
+                    pn = nch[i];
+                }
+            if (pn == 0) my_s -= 1;
+            else my_c -= 1;  // its first chunk stays with the warp
+        }
+        loc.x = __shfl_sync(0xffffffffu, px, src);
+        loc.chunk = __shfl_sync(0xffffffffu, pn, src) ? 1u : 0u;
+    }
     if (!__any_sync(0xffffffffu, (my_s | my_c) != 0)) return;
     const uint32_t is = warp_incl_scan(my_s);
     const uint32_t ic = warp_incl_scan(my_c);
     uint32_t bs = 0, bc = 0;
-    if ((threadIdx.x & 31) == 31) {
+    if (lane == 31) {
         if (is) bs = atomicAdd(&j.ctl->tail[q][QS].v, is);
         if (ic) bc = atomicAdd(&j.ctl->tail[q][QC].v, ic);
     }
@@ -400,10 +435,13 @@ __device__ __forceinline__ void enqueue_removed(const PeelJob& j, uint32_t q, co
 #pragma unroll
     for (int i = 0; i < N; i++) {
         if (rem[i]) {
-            if (nch[i] == 0) write_short(j, q, bs++, yg[i]);
-            else {
-                write_chunks(j, q, bc, yg[i], nch[i]);
-                bc += nch[i];
+            const bool kept = i == keep;
+            if (nch[i] == 0) {
+                if (!kept) write_short(j, q, bs++, yg[i]);
+            } else {
+                const uint32_t c0 = kept ? 1u : 0u;
+                write_chunks(j, q, bc, yg[i], c0, nch[i]);
+                bc += nch[i] - c0;
             }
         }
     }
@@ -421,7 +459,7 @@ __device__ __forceinline__ void enqueue_removed(const PeelJob& j, uint32_t q, co
 template <bool MULTI>
 __device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&seg)[4],
                                        const uint32_t (&col)[4], const uint32_t (&slot)[4],
-                                       const bool (&ok)[4], uint32_t k, uint32_t q) {
+                                       const bool (&ok)[4], uint32_t k, uint32_t q, Local& loc) {
     uint32_t yl[4], yg[4], cy[4], old[4], lmd[4];
 #pragma unroll
     for (int i = 0; i < 4; i++) {
@@ -455,7 +493,7 @@ __device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&seg)[4
             my_c += nch[i];
         }
     }
-    enqueue_removed<4>(j, q, rem, yg, nch, my_s, my_c);
+    enqueue_removed<4>(j, q, rem, yg, nch, my_s, my_c, loc);
 }
 
 // The same for N entries per lane that all belong to one node (a chunk of a
@@ -464,7 +502,7 @@ __device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&seg)[4
 template <int N>
 __device__ __forceinline__ void visit_node(const PeelJob& j, const SegP& g, uint32_t col,
                                            const uint32_t (&slot)[N], const bool (&ok)[N],
-                                           uint32_t k, uint32_t q) {
+                                           uint32_t k, uint32_t q, Local& loc) {
     const uint32_t lmd = g.col0 + col + 1;
     const uint32_t cb = col * g.n;
     uint32_t* const deg = g.deg + (uint64_t)col * g.nL;
@@ -492,7 +530,7 @@ __device__ __forceinline__ void visit_node(const PeelJob& j, const SegP& g, uint
             my_c += nch[i];
         }
     }
-    enqueue_removed<N>(j, q, rem, yg, nch, my_s, my_c);
+    enqueue_removed<N>(j, q, rem, yg, nch, my_s, my_c, loc);
 }
 
 // ---- phases ---------------------------------------------------------------
@@ -561,7 +599,7 @@ __device__ __forceinline__ void scan_nodes(const PeelJob& j, const uint32_t* src
         __syncthreads();
         if (keep) out[s_kbase + s_keep[warp] + kin - 1] = x;
         if (ns) write_short(j, q, s_sbase + s_short[warp] + sin - 1, x);
-        if (nch) write_chunks(j, q, s_cbase + s_chunk[warp] + cin - nch, x, nch);
+        if (nch) write_chunks(j, q, s_cbase + s_chunk[warp] + cin - nch, x, 0, nch);
         __syncthreads();
     }
 }
@@ -668,7 +706,7 @@ __device__ __forceinline__ void flush_processed(PeelCtl* c, uint32_t q, uint32_t
 // search over the warp's exclusive scan of row lengths.
 template <bool MULTI>
 __device__ __forceinline__ void expand_short(const PeelJob& j, uint32_t k, uint32_t q, uint32_t x,
-                                             bool ready) {
+                                             bool ready, Local& loc) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t s = seg_of<MULTI>(j, x);
     const SegP g = seg_load<MULTI>(j, s);
@@ -711,7 +749,7 @@ __device__ __forceinline__ void expand_short(const PeelJob& j, uint32_t k, uint3
             ok[i] = qq < total;
             slot[i] = ok[i] ? __ldg(oadj + ob + (qq - oe)) : 0u;
         }
-        visit4<MULTI>(j, segs, cols, slot, ok, k, q);
+        visit4<MULTI>(j, segs, cols, slot, ok, k, q, loc);
     }
 }
 
@@ -719,7 +757,7 @@ __device__ __forceinline__ void expand_short(const PeelJob& j, uint32_t k, uint3
 // per lane).
 template <bool MULTI>
 __device__ __forceinline__ void expand_chunk(const PeelJob& j, uint32_t k, uint32_t q,
-                                             unsigned long long it) {
+                                             unsigned long long it, Local& loc) {
     constexpr int PER_LANE = CHUNK / 32;
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t x = (uint32_t)it, ch = (uint32_t)(it >> 32);
@@ -742,7 +780,7 @@ __device__ __forceinline__ void expand_chunk(const PeelJob& j, uint32_t k, uint3
         ok[i] = p < ce;
         slot[i] = ok[i] ? __ldg(g.adj + p) : 0u;
     }
-    visit_node<PER_LANE>(j, g, col, slot, ok, k, q);
+    visit_node<PER_LANE>(j, g, col, slot, ok, k, q, loc);
 }
 
 // Per-block drain state in shared memory: `done` is set when the level is
@@ -800,8 +838,19 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j, volatile DrainBloc
     uint32_t idle = 0;          // consecutive polls without work
     uint32_t busy = 0;          // polls with work (lane 0's count)
     uint32_t pend_s = 0, pend_c = 0;  // processed items not yet flushed
+    Local loc{EMPTY32, 0};            // a removal this warp expands itself next
     for (;;) {
         bool progress = false;
+        if (loc.x != EMPTY32) {
+            // the warp's own removal first: the next step of its cascade
+            const Local cur = loc;
+            loc.x = EMPTY32;
+            if (cur.chunk) expand_chunk<MULTI>(j, k, q, (unsigned long long)cur.x, loc);
+            else expand_short<MULTI>(j, k, q, lane == 0 ? cur.x : 0u, lane == 0, loc);
+            progress = true;
+            goto done_work;
+        }
+        {
         // new claims, decided by lane 0
         uint32_t want = 0, cb = NONE, sbase = NONE;
         const bool hold_s = __any_sync(0xffffffffu, sidx != NONE);
@@ -828,7 +877,7 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j, volatile DrainBloc
             if (lane == 0 && cidx < j.qc_cap) it = ld_relaxed64(j.qc[q] + cidx);
             it = __shfl_sync(0xffffffffu, it, 0);
             if (it != EMPTY) {
-                if ((uint32_t)it < j.nx) expand_chunk<MULTI>(j, k, q, it);
+                if ((uint32_t)it < j.nx) expand_chunk<MULTI>(j, k, q, it, loc);
                 else if (lane == 0) record_bad(j, (uint32_t)it, 3);
                 pend_c += 1;
                 cidx = NONE;
@@ -844,14 +893,18 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j, volatile DrainBloc
             if (bad) record_bad(j, x, 4);
             const uint32_t rmask = __ballot_sync(0xffffffffu, ready);
             if (rmask) {
-                expand_short<MULTI>(j, k, q, ready && !bad ? x : 0u, ready && !bad);
+                expand_short<MULTI>(j, k, q, ready && !bad ? x : 0u, ready && !bad, loc);
                 if (ready) sidx = NONE;
                 pend_s += (uint32_t)__popc(rmask);
                 progress = true;
             }
         }
+        }
+    done_work:
         if (progress) {
-            if (pend_s + pend_c >= 16) flush_processed(c, q, pend_s, pend_c);
+            // never while a kept removal is pending: its parent must not count
+            // as processed before the removal's row is visited
+            if (pend_s + pend_c >= 16 && loc.x == EMPTY32) flush_processed(c, q, pend_s, pend_c);
             t0 = global_ns();
             ns = 32;
             idle = 0;
