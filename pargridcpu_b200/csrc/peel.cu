@@ -26,7 +26,7 @@
 // (CoreIndexParallel/CoreIndex.cpp:62-109) and ParGrid's per-cell PeelSync:
 // core_lambda is the unique fixpoint, whatever the removal order.
 //
-// Long rows (more than `small_row` entries, 32 by default; the batch
+// Long rows (more than `small_row` entries, 64 by default; the batch
 // autotuner picks it) are queued as CHUNK-entry items so that hubs spread over
 // many warps.  SCAN and DRAIN are separated by a grid
 // barrier whose last arriving block runs the serial "leader" step (level
@@ -62,7 +62,7 @@ enum : uint32_t { QS = 0, QC = 1 };
 
 // rows longer than the job's small_row entries are expanded as CHUNK-entry
 // work items
-constexpr uint32_t SMALL_ROW_DEFAULT = 32;
+constexpr uint32_t SMALL_ROW_DEFAULT = 64;
 constexpr uint32_t CHUNK = 256;
 
 // A counter alone on its 128-byte line: the queue counters are hit by atomics
@@ -1019,7 +1019,7 @@ static fc_status launch(PeelJob& j, uint32_t maxL, uint32_t threads, cudaStream_
     return launch_g<32, MULTI>(j, threads, s);
 }
 
-static uint32_t default_threads() { return env_u32("FC_PEEL_THREADS", 512) == 1024 ? 1024 : 512; }
+static uint32_t default_threads() { return env_u32("FC_PEEL_THREADS", 1024) == 512 ? 512 : 1024; }
 
 // Queue capacities: a level removes each node at most once; short rows take
 // one qs item, long rows at most entries/CHUNK + 1 qc items.
