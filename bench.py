@@ -73,11 +73,13 @@ def describe(name):
             f"seed={c['seed']}; full fcgrid + densest(beta)")
 
 
-def dist_setup():
+def dist_setup(init=True):
+    """Rank and world from the torchrun environment; with init, the NCCL
+    process group (one rank per GPU)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
+    if world > 1 and init:
         import datetime
         import torch
         import torch.distributed as dist
@@ -539,7 +541,9 @@ def run_serve(args, world, rank, local):
 
 def main():
     args = parse_args()
-    world, rank, local = dist_setup()
+    # the reference arm runs on rank 0's host cores alone: no process group
+    grouped = args.impl != "reference"
+    world, rank, local = dist_setup(init=grouped)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     try:
         if args.impl == "reference":
@@ -551,7 +555,7 @@ def main():
         else:
             run_ours(args, world, rank, local)
     finally:
-        if world > 1:
+        if world > 1 and grouped:
             import torch.distributed as dist
             dist.destroy_process_group()
 
