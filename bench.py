@@ -151,11 +151,13 @@ def peaks():
 
 
 def committed_traffic(workload):
-    """DRAM bytes per peel launch from the committed ncu summary, if any."""
+    """DRAM bytes and L2 atomic sectors per peel launch from the committed
+    ncu summary, if any."""
     p = os.path.join(ROOT, "profiles", f"peel_{workload}_traffic.json")
     if os.path.exists(p):
-        return json.load(open(p)).get("dram_bytes_per_launch")
-    return None
+        j = json.load(open(p))
+        return j.get("dram_bytes_per_launch"), j.get("l2_atomic_sectors_per_launch")
+    return None, None
 
 
 def cpu_baseline(layers, L, visits, beta, steps=1, warmup=0):
@@ -319,7 +321,7 @@ def run_ours(args, world, rank, local):
     launch_ms = statistics.mean(p / max(1, q) for p, q in zip(peel_ms, peel_launches))
     achieved = bytes_per_launch / (launch_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
-    traffic = committed_traffic(args.workload)
+    traffic, atom_sectors = committed_traffic(args.workload)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
@@ -333,7 +335,11 @@ def run_ours(args, world, rank, local):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "k_peel", "peak_kind": peak_kind,
-                         "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms},
+                         "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms,
+                         # atomics are reported beside the bytes, not folded in
+                         "l2_atomic_sectors_per_launch": atom_sectors,
+                         "l2_atomic_gsectors_per_s": (atom_sectors / (launch_ms / 1e3) / 1e9
+                                                      if atom_sectors else None)},
             "e2e": e2e, "gpu_launches": launches, "clocks": clk,
             "detail": {"peel_ms_per_step": statistics.mean(peel_ms),
                        "densest_ms_per_step": statistics.mean(dens_ms),
