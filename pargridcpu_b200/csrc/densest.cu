@@ -404,7 +404,12 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st) {
         FC_CUDA_TRY(attr_rc);
         FastDiv divL;
         divL.init(L);
-        const int blocks = sm_count();
+        // about 16K entries per block, at most one block per SM: a block
+        // clears and flushes all of its group's bins, which small graphs
+        // should not pay on every SM (and graphs searched on other streams
+        // get the SMs this one leaves)
+        const uint64_t want = (d->entries + 16383) / 16384;
+        const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>(sm_count(), want));
         uint32_t lam = 0;
         while (lam < L) {
             uint32_t words = 0, nl = 0;
