@@ -84,3 +84,23 @@ def test_batch_same_as_alone():
         a = alone.densest([1.0])[0]
         assert (a["k"], a["lmd"], a["length"], a["density"]) == (r["k"], r["lmd"], r["length"],
                                                                  r["density"])
+
+
+def test_batch_with_empty_graph_and_empty_layer():
+    """A graph without edges and a graph with an empty layer, between ordinary
+    ones: every result equals the oracle's, the empty graph's is all zero."""
+    ordinary = synth.chung_lu_graph(2000, 3, 5000, 2.3, 0.3, 350).layers
+    empty = [np.zeros((0, 2), np.uint32), np.zeros((0, 2), np.uint32)]
+    gap = [ordinary[0], np.zeros((0, 2), np.uint32), ordinary[1]]
+    layers = [ordinary, empty, gap]
+    graphs = [MultilayerGraph.from_pairs(ls) for ls in layers]
+    tables, results, _ = batch_run(graphs, beta=1.0)
+    assert graphs[1].n == 0 and tables[1].size == 0
+    assert (results[1]["k"], results[1]["lmd"], results[1]["length"]) == (0, 0, 0)
+    for i in (0, 2):
+        og = O.OracleGraph(layers[i])
+        t = og.coreindex()
+        o = og.densest(t, 1.0, with_cells=False)
+        assert np.array_equal(tables[i], t)
+        assert (results[i]["k"], results[i]["lmd"], results[i]["length"], results[i]["density"]) == \
+            (o["k"], o["lmd"], o["length"], o["density"])

@@ -154,3 +154,13 @@ def test_server_evicts_resident_graphs_for_room():
         srv.close()
     print(st)
     assert st["evictions"] > 0 and st["uploads"] > len(graphs)
+
+
+def test_server_empty_graph():
+    g = MultilayerGraph.from_pairs([np.zeros((0, 2), np.uint32)])
+    srv = Server()
+    try:
+        table, res, _ = srv.wait(srv.submit(g, 1.0), timeout_ms=60000)
+    finally:
+        srv.close()
+    assert table.size == 0 and (res["k"], res["lmd"], res["length"]) == (0, 0, 0)
