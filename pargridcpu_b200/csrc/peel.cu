@@ -1094,7 +1094,7 @@ template <bool MULTI>
 static fc_status run_job(PeelJob& j, uint32_t maxL, uint32_t threads, cudaStream_t s,
                          PeelStats* st, bool instrument, uint32_t col0, uint32_t ncols,
                          bool* use_graph = nullptr) {
-    j.idle_polls = env_u32("FC_PEEL_IDLE_POLLS", 8);
+    j.idle_polls = env_u32("FC_PEEL_IDLE_POLLS", 2);
     if (!j.small_row) j.small_row = env_u32("FC_PEEL_SMALL_ROW", SMALL_ROW_DEFAULT);
     j.timeout_ns = (uint64_t)env_u32("FC_BARRIER_TIMEOUT_MS", 10000) * 1000000ull;
     j.deadline_ns = (uint64_t)env_u32("FC_PEEL_DEADLINE_MS", 60000) * 1000000ull;
