@@ -147,6 +147,26 @@ fc_status fc_densest(fc_graph* g, const double* betas, uint32_t n_betas, fc_dens
  * on the same graph.  Either pointer may be NULL. */
 fc_status fc_densest_members(fc_graph* g, const fc_densest_result* res, uint32_t* nodes,
                              uint32_t* layers, void* stream);
+/* ---- one graph split by lambda range --------------------------------------
+ * The lambda columns of a graph are independent given the graph, so a
+ * graph's fcgrid can be split over processes or GPUs by lambda range: each
+ * computes its columns lmd_lo .. lmd_hi-1 (1 <= lmd_lo < lmd_hi <= L+1) and
+ * their cells, and the cells of all ranges, folded in the reference's order
+ * with its float running maximum (FCTree::WeightDenestSubgraph,
+ * Core/FCTree.cpp:69-82), give the whole graph's densest result
+ * (pargridcpu_b200/shard.py, merge_cells).  The reference computes every
+ * column in one process; these have no direct counterpart there. */
+/* out[(lambda - lmd_lo)*n + v] = core_lambda(v) for the range; only its
+ * columns are peeled unless the whole table (or a covering range) is
+ * resident.  out may be NULL; out_on_device as for fc_coreindex. */
+fc_status fc_coreindex_range(fc_graph* g, uint32_t lmd_lo, uint32_t lmd_hi, uint32_t* out,
+                             int out_on_device, void* stream);
+/* The range's non-empty cells with their best density for `beta`, lambda-major
+ * and k ascending, as fc_cells gives them for the whole graph.  Writes
+ * min(cap, count) cells; *count receives the total. */
+fc_status fc_cells_range(fc_graph* g, uint32_t lmd_lo, uint32_t lmd_hi, double beta,
+                         fc_cell* cells, uint32_t cap, uint32_t* count, void* stream);
+
 /* Node set of any cell, C_{k,lambda} = {v : core_lambda(v) >= k}, in
  * ascending internal ids: the query of `-m kpe -k K -lmd L` (main.cpp:
  * 197-225) that FCTree::saveCoreToLocal writes out (Core/FCTree.cpp:138-153).

@@ -196,6 +196,27 @@ class MultilayerGraph:
                                           C.byref(cnt), _n.stream_handle(stream)), "cell_members")
         return nodes[:cnt.value].copy()
 
+    def coreindex_range(self, lmd_lo, lmd_hi, stream=None):
+        """Columns lmd_lo .. lmd_hi-1 of the core table, (lmd_hi - lmd_lo, n):
+        one process's share when a graph is split by lambda range."""
+        out = np.zeros((lmd_hi - lmd_lo, self.n), np.uint32)
+        _n.check(_n.lib().fc_coreindex_range(self._h, int(lmd_lo), int(lmd_hi), _n.ptr(out), 0,
+                                             _n.stream_handle(stream)), "coreindex_range")
+        return out
+
+    def cells_range(self, lmd_lo, lmd_hi, beta=1.0):
+        """The cells of lambda lmd_lo .. lmd_hi-1 as (k, lmd, length, lstar,
+        density) tuples, the form shard.merge_cells folds."""
+        cnt = C.c_uint32()
+        _n.check(_n.lib().fc_cells_range(self._h, int(lmd_lo), int(lmd_hi), float(beta), None, 0,
+                                         C.byref(cnt), None), "cells_range")
+        buf = (_n.Cell * max(cnt.value, 1))()
+        _n.check(_n.lib().fc_cells_range(self._h, int(lmd_lo), int(lmd_hi), float(beta),
+                                         C.cast(buf, C.c_void_p), cnt.value, C.byref(cnt), None),
+                 "cells_range")
+        return [(int(c.k), int(c.lmd), int(c.length), int(c.lstar), float(c.density))
+                for c in buf[:cnt.value]]
+
     def cells(self, beta=1.0):
         cnt = C.c_uint32()
         _n.check(_n.lib().fc_cells(self._h, float(beta), None, 0, C.byref(cnt), None), "cells")

@@ -12,29 +12,36 @@ namespace fc {
 static std::atomic<uint64_t> g_launches{0};
 void count_launch(uint32_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 
+// The peel of columns [lo, hi) in launches of up to peel_columns_per_group
+// columns each, with the launches' statistics.
+static fc_status peel_range(DeviceGraph* d, uint32_t lo, uint32_t hi, cudaStream_t s) {
+    invalidate_densest(d);
+    d->stats.peel_ms = 0;
+    d->stats.peel_launches = d->stats.levels = d->stats.subrounds = 0;
+    for (int i = 0; i < 3; i++) d->stats.phase_ms[i] = 0;
+    if (!d->n || lo >= hi) return FC_OK;
+    const uint32_t per = peel_columns_per_group(d);
+    d->stats.columns_per_launch = per;
+    for (uint32_t c0 = lo; c0 < hi; c0 += per) {
+        const uint32_t nc = hi - c0 < per ? hi - c0 : per;
+        PeelStats st;
+        FC_TRY(peel_columns(d, c0, nc, s, &st));
+        d->stats.peel_ms += st.ms;
+        d->stats.peel_launches++;
+        d->stats.levels += st.levels;
+        d->stats.subrounds += st.subrounds;
+        for (int i = 0; i < 3; i++) d->stats.phase_ms[i] += st.phase_ms[i];
+    }
+    return FC_OK;
+}
+
 fc_status coreindex(fc_graph* g, uint32_t* out, bool out_on_device, cudaStream_t s) {
     FC_TRY(upload(g, s));
     DeviceGraph* d = g->dev;
     d->home = s;
     if (!d->table_valid) {
-        invalidate_densest(d);
-        d->stats.peel_ms = 0;
-        d->stats.peel_launches = d->stats.levels = d->stats.subrounds = 0;
-        for (int i = 0; i < 3; i++) d->stats.phase_ms[i] = 0;
-        if (d->n && d->L) {
-            const uint32_t per = peel_columns_per_group(d);
-            d->stats.columns_per_launch = per;
-            for (uint32_t c0 = 0; c0 < d->L; c0 += per) {
-                uint32_t nc = d->L - c0 < per ? d->L - c0 : per;
-                PeelStats st;
-                FC_TRY(peel_columns(d, c0, nc, s, &st));
-                d->stats.peel_ms += st.ms;
-                d->stats.peel_launches++;
-                d->stats.levels += st.levels;
-                d->stats.subrounds += st.subrounds;
-                for (int i = 0; i < 3; i++) d->stats.phase_ms[i] += st.phase_ms[i];
-            }
-        }
+        d->cols_lo = d->cols_hi = 0;
+        FC_TRY(peel_range(d, 0, d->L, s));
         d->table_valid = true;
     }
     if (out) {
@@ -48,6 +55,33 @@ fc_status coreindex(fc_graph* g, uint32_t* out, bool out_on_device, cudaStream_t
     }
     // every peel launch ended with a synchronize; only a device-to-device
     // copy of the table may still be in flight
+    if (!out || !out_on_device) d->home = nullptr;
+    return FC_OK;
+}
+
+// Columns [lo, hi) of the table (0-based); out (may be NULL) receives them,
+// (hi - lo) rows of n.  Peels only those columns unless the whole table, or
+// a range covering them, is already resident.
+fc_status coreindex_range(fc_graph* g, uint32_t lo, uint32_t hi, uint32_t* out, bool out_on_device,
+                          cudaStream_t s) {
+    if (lo >= hi || hi > g->L) return FC_ERR_INVALID;
+    FC_TRY(upload(g, s));
+    DeviceGraph* d = g->dev;
+    d->home = s;
+    if (!d->table_valid && !(d->cols_lo <= lo && hi <= d->cols_hi)) {
+        d->cols_lo = d->cols_hi = 0;
+        FC_TRY(peel_range(d, lo, hi, s));
+        d->cols_lo = lo;
+        d->cols_hi = hi;
+    }
+    const uint64_t bytes = (uint64_t)d->n * (hi - lo) * 4;
+    if (out && bytes) {
+        const uint32_t* src = d->table + (uint64_t)lo * d->n;
+        if (out_on_device)
+            FC_CUDA_TRY(cudaMemcpyAsync(out, src, bytes, cudaMemcpyDeviceToDevice, s));
+        else
+            FC_TRY(to_host(out, src, bytes, s));
+    }
     if (!out || !out_on_device) d->home = nullptr;
     return FC_OK;
 }
@@ -172,6 +206,7 @@ fc_status fc_graph_reset_results(fc_graph* g) {
     if (!g) return FC_ERR_INVALID;
     if (g->dev) {
         g->dev->table_valid = false;
+        g->dev->cols_lo = g->dev->cols_hi = 0;
         invalidate_densest(g->dev);
     }
     return FC_OK;
@@ -213,6 +248,27 @@ fc_status fc_cell_members(fc_graph* g, uint32_t k, uint32_t lmd, uint32_t* nodes
         return FC_OK;
     }
     return cell_members(g, k, lmd, nodes, cap, count, (cudaStream_t)stream);
+}
+
+fc_status fc_coreindex_range(fc_graph* g, uint32_t lmd_lo, uint32_t lmd_hi, uint32_t* out,
+                             int out_on_device, void* stream) {
+    if (!g || lmd_lo < 1 || lmd_lo >= lmd_hi || lmd_hi > g->L + 1) return FC_ERR_INVALID;
+    if (!cuda_available()) return FC_ERR_NO_DEVICE;
+    if (!g->n) return FC_OK;
+    return coreindex_range(g, lmd_lo - 1, lmd_hi - 1, out, out_on_device != 0,
+                           (cudaStream_t)stream);
+}
+
+fc_status fc_cells_range(fc_graph* g, uint32_t lmd_lo, uint32_t lmd_hi, double beta,
+                         fc_cell* cells_out, uint32_t cap, uint32_t* count, void* stream) {
+    if (!g || lmd_lo < 1 || lmd_lo >= lmd_hi || lmd_hi > g->L + 1) return FC_ERR_INVALID;
+    if (!cuda_available()) return FC_ERR_NO_DEVICE;
+    if (!g->n) {
+        if (count) *count = 0;
+        return FC_OK;
+    }
+    return cells_range(g, lmd_lo - 1, lmd_hi - 1, beta, cells_out, cap, count,
+                       (cudaStream_t)stream);
 }
 
 fc_status fc_cells(fc_graph* g, double beta, fc_cell* cells_out, uint32_t cap, uint32_t* count,

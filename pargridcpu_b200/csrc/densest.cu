@@ -49,6 +49,7 @@ struct DensState {
     std::vector<uint32_t> cell_host;
     uint64_t H_cap = 0, N_cap = 0, cells_cap = 0, cell_lk_cap = 0, hbase_cap = 0, nbase_cap = 0;
     bool hist_valid = false;
+    uint32_t lo = 0, hi = 0;           // the lambda columns (0-based) the histograms cover
 };
 
 template <class T>
@@ -326,10 +327,12 @@ static int sm_count() {
     return sms;
 }
 
-// Histograms for the resident table (beta-independent).
-static fc_status build_hist(DeviceGraph* d, cudaStream_t st) {
+// Histograms for the resident table (beta-independent), over the lambda
+// columns [lo, hi): the other columns count as empty (kmax 0, no cells), and
+// no kernel reads them, since they may not have been computed.
+static fc_status build_hist(DeviceGraph* d, cudaStream_t st, uint32_t lo, uint32_t hi) {
     DensState* s = (DensState*)d->dens;
-    if (s && s->hist_valid) return FC_OK;
+    if (s && s->hist_valid && s->lo == lo && s->hi == hi) return FC_OK;
     if (!s) {
         s = new DensState();
         d->dens = s;
@@ -339,9 +342,9 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st) {
     // per-lambda maxima
     if (!s->d_kmax) FC_TRY(dev_alloc((void**)&s->d_kmax, (L + 1) * 4, st));
     FC_CUDA_TRY(cudaMemsetAsync(s->d_kmax, 0, (L + 1) * 4, st));
-    dim3 g((n + 255) / 256 < 64 ? (n + 255) / 256 : 64, L);
+    dim3 g((n + 255) / 256 < 64 ? (n + 255) / 256 : 64, hi - lo);
     if (g.x == 0) g.x = 1;
-    k_colmax<<<g, 256, 0, st>>>(d->table, n, L, s->d_kmax);
+    k_colmax<<<g, 256, 0, st>>>(d->table + (uint64_t)lo * n, n, L, s->d_kmax + lo);
     count_launch();
     FC_CUDA_TRY(cudaGetLastError());
     s->kmax.assign(L, 0);
@@ -392,8 +395,9 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st) {
         dim3 tg((n + 31) / 32, (L + 31) / 32);
         k_transpose<<<tg, dim3(32, 8), 0, st>>>(d->table, n, L, s->coreT);
         FC_CUDA_TRY(cudaGetLastError());
-        dim3 ng((n + 255) / 256 < 32 ? (n + 255) / 256 : 32, L);
-        k_node_hist<<<ng, 256, 12288 * 4, st>>>(d->table, n, s->d_nbase, s->d_kmax, s->N);
+        dim3 ng((n + 255) / 256 < 32 ? (n + 255) / 256 : 32, hi - lo);
+        k_node_hist<<<ng, 256, 12288 * 4, st>>>(d->table + (uint64_t)lo * n, n, s->d_nbase + lo,
+                                               s->d_kmax + lo, s->N);
         count_launch(2);
         FC_CUDA_TRY(cudaGetLastError());
         // lambda groups whose bins fit the shared-memory budget
@@ -410,10 +414,10 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st) {
         // get the SMs this one leaves)
         const uint64_t want = (d->entries + 16383) / 16384;
         const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>(sm_count(), want));
-        uint32_t lam = 0;
-        while (lam < L) {
+        uint32_t lam = lo;
+        while (lam < hi) {
             uint32_t words = 0, nl = 0;
-            while (lam + nl < L && nl < 64) {
+            while (lam + nl < hi && nl < 64) {
                 uint32_t w = L * (s->kmax[lam + nl] + 1);
                 if (nl > 0 && words + w > SH_WORDS) break;
                 words += w;
@@ -435,6 +439,8 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st) {
         FC_CUDA_TRY(cudaGetLastError());
     }
     s->hist_valid = true;
+    s->lo = lo;
+    s->hi = hi;
     return FC_OK;
 }
 
@@ -467,7 +473,7 @@ fc_status densest(fc_graph* g, const double* betas, uint32_t nb, fc_densest_resu
     FC_CUDA_TRY(cudaEventCreate(&e0));
     FC_CUDA_TRY(cudaEventCreate(&e1));
     FC_CUDA_TRY(cudaEventRecord(e0, st));
-    FC_TRY(build_hist(d, st));
+    FC_TRY(build_hist(d, st, 0, d->L));
     DensState* s = (DensState*)d->dens;
     if (!s->d_res) FC_TRY(dev_alloc((void**)&s->d_res, sizeof(fc_densest_result), st));
     for (uint32_t b = 0; b < nb; b++) {
@@ -491,7 +497,7 @@ fc_status cells(fc_graph* g, double beta, fc_cell* out, uint32_t cap, uint32_t* 
                 cudaStream_t st) {
     FC_TRY(coreindex(g, nullptr, false, st));
     DeviceGraph* d = g->dev;
-    FC_TRY(build_hist(d, st));
+    FC_TRY(build_hist(d, st, 0, d->L));
     DensState* s = (DensState*)d->dens;
     FC_TRY(score_cells(d, beta, st));
     uint64_t nc = s->ncells;
@@ -502,12 +508,30 @@ fc_status cells(fc_graph* g, double beta, fc_cell* out, uint32_t cap, uint32_t* 
     return FC_OK;
 }
 
+// The cells of the lambda columns [lo, hi) (0-based), computing those
+// columns first when they are not resident.
+fc_status cells_range(fc_graph* g, uint32_t lo, uint32_t hi, double beta, fc_cell* out, uint32_t cap,
+                      uint32_t* count, cudaStream_t st) {
+    FC_TRY(coreindex_range(g, lo, hi, nullptr, false, st));
+    DeviceGraph* d = g->dev;
+    FC_TRY(build_hist(d, st, lo, hi));
+    DensState* s = (DensState*)d->dens;
+    FC_TRY(score_cells(d, beta, st));
+    const uint64_t nc = s->ncells;
+    if (count) *count = (uint32_t)nc;
+    const uint64_t w = nc < cap ? nc : cap;
+    if (w && out) FC_TRY(to_host(out, s->cells, w * sizeof(fc_cell), st));
+    FC_CUDA_TRY(cudaStreamSynchronize(st));
+    d->home = nullptr;
+    return FC_OK;
+}
+
 fc_status densest_members(fc_graph* g, const fc_densest_result* r, uint32_t* nodes,
                           uint32_t* layers, cudaStream_t st) {
     if (!r || r->k == 0) return FC_OK;
     FC_TRY(coreindex(g, nullptr, false, st));
     DeviceGraph* d = g->dev;
-    FC_TRY(build_hist(d, st));
+    FC_TRY(build_hist(d, st, 0, d->L));
     DensState* s = (DensState*)d->dens;
     const uint32_t n = d->n, L = d->L, lam = r->lmd - 1;
     if (r->lmd < 1 || r->lmd > L || r->k > s->kmax[lam]) return FC_ERR_INVALID;

@@ -57,6 +57,9 @@ struct DeviceGraph {
     // resident results
     uint32_t* table = nullptr;     // L * n, lambda-major
     bool table_valid = false;
+    // when the table is not all valid: columns [cols_lo, cols_hi) are
+    // (fc_coreindex_range); an empty range when none
+    uint32_t cols_lo = 0, cols_hi = 0;
     std::vector<uint32_t> kmax;    // per lambda, max core (host copy)
     // densest state for the resident table (histograms, cell records)
     void* dens = nullptr;

@@ -81,6 +81,11 @@ fc_status cells(fc_graph* g, double beta, fc_cell* out, uint32_t cap, uint32_t* 
                 cudaStream_t s);
 fc_status cell_members(fc_graph* g, uint32_t k, uint32_t lmd, uint32_t* nodes, uint32_t cap,
                        uint32_t* count, cudaStream_t s);
+// lambda columns [lo, hi), 0-based (fc_coreindex_range / fc_cells_range)
+fc_status coreindex_range(fc_graph* g, uint32_t lo, uint32_t hi, uint32_t* out, bool out_on_device,
+                          cudaStream_t s);
+fc_status cells_range(fc_graph* g, uint32_t lo, uint32_t hi, double beta, fc_cell* out, uint32_t cap,
+                      uint32_t* count, cudaStream_t s);
 fc_status batch_run(fc_graph* const* gs, uint32_t count, double beta, uint32_t* const* tables,
                     fc_densest_result* res, const fc_batch_options* opt, fc_batch_report* rep,
                     cudaStream_t s);

@@ -25,7 +25,8 @@ EXPORTS = [
     "fc_graph_from_adjbuf", "fc_graph_free", "fc_graph_n", "fc_graph_layers", "fc_graph_layer_m",
     "fc_graph_id2vtx", "fc_graph_order", "fc_graph_csr", "fc_graph_upload",
     "fc_graph_release_device", "fc_graph_reset_results", "fc_graph_device_bytes", "fc_coreindex",
-    "fc_densest", "fc_densest_members", "fc_cell_members", "fc_cells", "fc_batch_run", "fc_server_create",
+    "fc_densest", "fc_densest_members", "fc_cell_members", "fc_cells", "fc_coreindex_range",
+    "fc_cells_range", "fc_batch_run", "fc_server_create",
     "fc_server_submit", "fc_server_wait", "fc_server_query", "fc_server_destroy", "fc_graph_stats",
     "fc_launch_count", "fc_coreindex_fixed_scratch",
 ]
@@ -130,6 +131,8 @@ def lib():
         "fc_densest_members": ([p, p, p, p, p], i32),
         "fc_cell_members": ([p, u32, u32, p, u32, C.POINTER(u32), p], i32),
         "fc_cells": ([p, C.c_double, p, u32, C.POINTER(u32), p], i32),
+        "fc_coreindex_range": ([p, u32, u32, p, i32, p], i32),
+        "fc_cells_range": ([p, u32, u32, C.c_double, p, u32, C.POINTER(u32), p], i32),
         "fc_batch_run": ([p, u32, C.c_double, p, p, p, p, p], i32),
         "fc_server_create": ([p, pp], i32),
         "fc_server_submit": ([p, p, C.c_double, p, p, C.POINTER(u64)], i32),

@@ -167,6 +167,18 @@ def test_no_device_fails_loudly():
     assert e.value.code == 9
 
 
+def test_lambda_range_bounds_checked_on_host():
+    """fc_coreindex_range / fc_cells_range reject a range outside
+    1 <= lo < hi <= L+1 before touching a device."""
+    g = MultilayerGraph.from_pairs(G.inputs("tiny_dirty"))
+    for lo, hi in [(0, 1), (2, 2), (3, 2), (1, g.L + 2)]:
+        rc = native.lib().fc_coreindex_range(g._h, lo, hi, None, 0, None)
+        assert rc == 7
+        with pytest.raises(native.FcError) as e:
+            g.cells_range(lo, hi)
+        assert e.value.code == 7
+
+
 def test_cli_help_runs_without_gpu():
     """The drop-in CLI loads a dataset and prints the reference's header lines
     before any device work."""
