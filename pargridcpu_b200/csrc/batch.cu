@@ -247,7 +247,8 @@ fc_status batch_peel(fc_graph* const* gs, uint32_t count, const fc_batch_options
         invalidate_densest(d);
         if (d->n && d->L) {
             PeelSegSpec sp;
-            sp.g = PeelGraph{d->n, d->L, d->entries, d->node_ptr, d->adj, d->deg0, d->max_deg + 1};
+            sp.g = PeelGraph{d->n, d->L, d->entries, d->node_ptr, d->adj, d->deg0, d->max_deg + 1,
+                             d->big_id, d->ptab};
             sp.col0 = 0;
             sp.ncols = d->L;
             sp.table = d->table;

@@ -9,6 +9,14 @@
 //                                   to decrement
 //   deg0[v * L + l] = |N_l(v)|      the full per-layer degrees
 // Core tables are lambda-major: table[(lambda-1) * n + v].
+//
+// Rows longer than ORDER_MIN_ROW entries are ordered by bound bucket,
+// highest first: the bound of neighbour u is its largest layer degree, which
+// is at least core_lambda(u) for every lambda, so at level K every entry
+// whose bound is below K names a removed node.  For such a row,
+// ptab[big_id[v] * BUCKETS + b] counts its entries of bucket >= b, and a
+// removal at level K needs only the chunks covering the first
+// ptab[.. + bucket_of(K)] entries.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -45,6 +53,33 @@ struct FastDiv {
     }
 };
 
+// Bound buckets: 0..15 hold the values 0..15, buckets 16..63 eight per
+// octave from 16 (lower ends 16 * 2^(i/8), rounded down); bucket 63 is
+// unbounded above.
+constexpr uint32_t BUCKETS = 64;
+constexpr uint32_t ORDER_MIN_ROW = 256;
+constexpr uint32_t NO_BIG_ROW = 0xFFFFFFFFu;
+__host__ __device__ __forceinline__ uint32_t bucket_lo(uint32_t b) {
+    if (b < 16) return b;
+    const uint32_t t = b - 16;
+    // 256 * 2^(i/8), i = 0..7, rounded down
+    const uint32_t f = t & 7;
+    const uint32_t frac = f == 0 ? 256u : f == 1 ? 279u : f == 2 ? 304u : f == 3 ? 331u
+                        : f == 4 ? 362u : f == 5 ? 394u : f == 6 ? 430u : 469u;
+    return ((16u << (t >> 3)) * frac) >> 8;
+}
+// the bucket holding value x: the largest b with bucket_lo(b) <= x
+__host__ __device__ __forceinline__ uint32_t bucket_of(uint32_t x) {
+    if (x < 16) return x;
+    uint32_t lo = 16, hi = BUCKETS - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (bucket_lo(mid) <= x) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
 struct DeviceGraph {
     int device = -1;
     uint32_t n = 0, L = 0;
@@ -54,6 +89,10 @@ struct DeviceGraph {
     uint32_t* node_ptr = nullptr;  // n + 1
     uint32_t* adj = nullptr;       // entries (slots)
     uint32_t* deg0 = nullptr;      // n * L
+    // ordered long rows: big_id[v] (NO_BIG_ROW for other rows), BUCKETS counts each
+    uint32_t* big_id = nullptr;    // n
+    uint32_t* ptab = nullptr;      // nbig * BUCKETS
+    uint32_t nbig = 0;
     // resident results
     uint32_t* table = nullptr;     // L * n, lambda-major
     bool table_valid = false;
@@ -115,6 +154,9 @@ struct PeelGraph {
     const uint32_t* adj;
     const uint32_t* deg0;
     uint32_t max_level;  // bound on the level count (largest degree + 1, or n + 1)
+    // ordered long rows (both null when the rows are in any order)
+    const uint32_t* big_id = nullptr;
+    const uint32_t* ptab = nullptr;
 };
 // scratch bytes one peel launch over `ncols` columns needs
 uint64_t peel_ws_bytes(uint32_t n, uint32_t L, uint64_t entries, uint32_t ncols);

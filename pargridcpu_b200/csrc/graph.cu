@@ -47,7 +47,8 @@ __global__ void k_degrees(const uint64_t* __restrict__ off, uint32_t n, uint32_t
     }
 }
 
-// One warp per node: copy its L layer rows into its node-major range as slots.
+// One warp per node: copy its L layer rows into its node-major range as
+// slots; the rows longer than ORDER_MIN_ROW are left to the ordering kernels.
 __global__ void k_scatter(const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj_in,
                           const uint32_t* __restrict__ node_ptr, uint32_t n, uint32_t L,
                           uint32_t* __restrict__ adj_out) {
@@ -55,12 +56,168 @@ __global__ void k_scatter(const uint64_t* __restrict__ off, const uint32_t* __re
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
         uint32_t dst = node_ptr[v];
+        if (node_ptr[v + 1] - dst > ORDER_MIN_ROW) continue;  // written ordered (k_order_scatter)
         for (uint32_t l = 0; l < L; l++) {
             const uint64_t* o = off + (uint64_t)l * (n + 1);
             uint64_t b = o[v], e = o[v + 1];
             for (uint64_t j = b + lane; j < e; j += 32) adj_out[dst + (j - b)] = adj_in[j] * L + l;
             dst += (uint32_t)(e - b);
         }
+    }
+}
+
+// ---- ordering of long rows by bound bucket (layout in device.h) ----------
+// Each row longer than ORDER_MIN_ROW is cut into tiles of ORDER_TILE
+// entries.  A tile's bucket histogram goes to hist at the row's base
+// (first tile * BUCKETS) + (BUCKETS-1-b) * tiles + tile, so one exclusive scan
+// over all rows lists, per row, the buckets highest first and each bucket's
+// tiles in order: the scan minus its value at the row's base is where a
+// tile's first entry of bucket b goes.  Entries keep their order within a
+// bucket (a stable counting sort), so the layout is deterministic.
+constexpr uint32_t ORDER_TILE = 1024;
+
+// the bound of every node and, per row, whether it is ordered and its tiles
+__global__ void k_order_flags(const uint32_t* __restrict__ deg0, const uint32_t* __restrict__ rowlen,
+                              uint32_t n, uint32_t L, uint32_t* __restrict__ ub,
+                              uint32_t* __restrict__ fbig, uint32_t* __restrict__ ftiles) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v <= n; v += gridDim.x * blockDim.x) {
+        if (v == n) {
+            fbig[n] = 0;
+            ftiles[n] = 0;
+            continue;
+        }
+        uint32_t m = 0;
+        for (uint32_t l = 0; l < L; l++) m = max(m, deg0[(uint64_t)v * L + l]);
+        ub[v] = m;
+        const uint32_t len = rowlen[v];
+        const bool big = len > ORDER_MIN_ROW;
+        fbig[v] = big ? 1u : 0u;
+        ftiles[v] = big ? (len + ORDER_TILE - 1) / ORDER_TILE : 0u;
+    }
+}
+
+// big_id of every node; the node of every ordered row and of every tile
+__global__ void k_order_index(const uint32_t* __restrict__ fbig, const uint32_t* __restrict__ bscan,
+                              const uint32_t* __restrict__ tscan, uint32_t n,
+                              uint32_t* __restrict__ big_id, uint32_t* __restrict__ big_v,
+                              uint32_t* __restrict__ tile_row) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        if (!fbig[v]) {
+            big_id[v] = NO_BIG_ROW;
+            continue;
+        }
+        const uint32_t id = bscan[v];
+        big_id[v] = id;
+        big_v[id] = v;
+        for (uint32_t t = tscan[v]; t < tscan[v + 1]; t++) tile_row[t] = v;
+    }
+}
+
+// The entries of tile i of node v's row (row positions [i*ORDER_TILE, ...)),
+// read from the per-layer input CSR: f(valid, lane's u, l) is called by the
+// whole warp for 32 consecutive positions at a time, in row order; a call
+// never spans two layers.
+template <class F>
+__device__ __forceinline__ void for_tile_entries(const uint64_t* __restrict__ off,
+                                                 const uint32_t* __restrict__ adj_in,
+                                                 const uint32_t* __restrict__ deg0, uint32_t n,
+                                                 uint32_t L, uint32_t v, uint32_t len, uint32_t i,
+                                                 F&& f) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t p0 = i * ORDER_TILE;
+    const uint32_t p1 = min(len, p0 + ORDER_TILE);
+    uint32_t s = 0;  // row position of layer l's first entry
+    for (uint32_t l = 0; l < L && s < p1; l++) {
+        const uint32_t d = deg0[(uint64_t)v * L + l];
+        const uint32_t a = max(s, p0), b = min(s + d, p1);
+        if (a < b) {
+            const uint64_t ob = off[(uint64_t)l * (n + 1) + v] - s;
+            for (uint32_t p = a; p < b; p += 32) {
+                const bool valid = p + lane < b;
+                const uint32_t u = valid ? adj_in[ob + p + lane] : 0u;
+                f(valid, u, l);
+            }
+        }
+        s += d;
+    }
+}
+
+// One warp per tile: its bucket histogram.
+__global__ void k_order_hist(const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj_in,
+                             const uint32_t* __restrict__ deg0, const uint32_t* __restrict__ node_ptr,
+                             uint32_t n, uint32_t L, const uint32_t* __restrict__ ub,
+                             const uint32_t* __restrict__ tile_row, const uint32_t* __restrict__ tscan,
+                             uint32_t ntiles, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t h[8][BUCKETS];  // 256 threads
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntiles; t += warps) {
+        const uint32_t v = tile_row[t];
+        const uint32_t t0 = tscan[v], nt = tscan[v + 1] - t0, i = t - t0;
+        h[w][lane] = 0;
+        h[w][lane + 32] = 0;
+        __syncwarp();
+        for_tile_entries(off, adj_in, deg0, n, L, v, node_ptr[v + 1] - node_ptr[v], i,
+                         [&](bool valid, uint32_t u, uint32_t) {
+                             if (valid) atomicAdd(&h[w][bucket_of(ub[u])], 1u);
+                         });
+        __syncwarp();
+        const uint64_t base = (uint64_t)t0 * BUCKETS;
+        for (uint32_t b = lane; b < BUCKETS; b += 32)
+            hist[base + (uint64_t)(BUCKETS - 1 - b) * nt + i] = h[w][b];
+        __syncwarp();
+    }
+}
+
+// Per ordered row r and bucket b: entries of bucket >= b.
+__global__ void k_order_ptab(const uint32_t* __restrict__ big_v, const uint32_t* __restrict__ tscan,
+                             const uint32_t* __restrict__ G, uint32_t nbig, uint32_t* __restrict__ ptab) {
+    const uint64_t total = (uint64_t)nbig * BUCKETS;
+    for (uint64_t x = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; x < total;
+         x += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t r = (uint32_t)(x / BUCKETS), b = (uint32_t)(x % BUCKETS);
+        const uint32_t v = big_v[r];
+        const uint32_t t0 = tscan[v], nt = tscan[v + 1] - t0;
+        const uint64_t base = (uint64_t)t0 * BUCKETS;
+        ptab[x] = G[base + (uint64_t)(BUCKETS - b) * nt] - G[base];
+    }
+}
+
+// One warp per tile: its entries as slots to their ordered places in the
+// row, ranked in row order within each bucket.
+__global__ void k_order_scatter(const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj_in,
+                                const uint32_t* __restrict__ deg0, const uint32_t* __restrict__ node_ptr,
+                                uint32_t n, uint32_t L, const uint32_t* __restrict__ ub,
+                                const uint32_t* __restrict__ tile_row, const uint32_t* __restrict__ tscan,
+                                const uint32_t* __restrict__ G, uint32_t ntiles,
+                                uint32_t* __restrict__ adj) {
+    __shared__ uint32_t cur[8][BUCKETS];  // 256 threads
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    for (uint32_t t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntiles; t += warps) {
+        const uint32_t v = tile_row[t];
+        const uint32_t t0 = tscan[v], nt = tscan[v + 1] - t0, i = t - t0;
+        const uint64_t base = (uint64_t)t0 * BUCKETS;
+        const uint32_t g0 = G[base];
+        for (uint32_t b = lane; b < BUCKETS; b += 32)
+            cur[w][b] = G[base + (uint64_t)(BUCKETS - 1 - b) * nt + i] - g0;
+        __syncwarp();
+        const uint32_t rs = node_ptr[v];
+        for_tile_entries(off, adj_in, deg0, n, L, v, node_ptr[v + 1] - rs, i,
+                         [&](bool valid, uint32_t u, uint32_t l) {
+                             const uint32_t mask = __ballot_sync(0xffffffffu, valid);
+                             if (valid) {
+                                 const uint32_t b = bucket_of(ub[u]);
+                                 const uint32_t peers = __match_any_sync(mask, b);
+                                 const uint32_t rank = __popc(peers & lt);
+                                 adj[rs + cur[w][b] + rank] = u * L + l;
+                                 __syncwarp(mask);
+                                 if (rank == 0) cur[w][b] += __popc(peers);
+                             }
+                             __syncwarp();
+                         });
+        __syncwarp();
     }
 }
 
@@ -165,6 +322,82 @@ static int num_sms() {
     return sms;
 }
 
+// Stream-ordered temporaries of one call, returned when it ends (on every path).
+struct TempBufs {
+    cudaStream_t s;
+    void* p[12] = {};
+    int k = 0;
+    explicit TempBufs(cudaStream_t st) : s(st) {}
+    ~TempBufs() {
+        for (int i = 0; i < k; i++) cudaFreeAsync(p[i], s);
+    }
+    template <class T>
+    cudaError_t alloc(T** out, size_t bytes) {
+        *out = nullptr;
+        if (k == 12) return cudaErrorMemoryAllocation;
+        cudaError_t e = cudaMallocAsync((void**)out, bytes, s);
+        if (e == cudaSuccess) p[k++] = *out;
+        return e;
+    }
+};
+
+// Writes the rows longer than ORDER_MIN_ROW, ordered by bound bucket, from
+// the per-layer input CSR (off, adj_in), and builds big_id and ptab
+// (device.h).
+static fc_status order_rows(DeviceGraph* d, const uint32_t* rowlen, const uint64_t* off,
+                            const uint32_t* adj_in, cudaStream_t s) {
+    const uint32_t n = d->n, L = d->L;
+    const int blocks = num_sms() * 8;
+    TempBufs tb(s);
+    uint32_t *ub, *fbig, *ftiles, *bscan, *tscan;
+    FC_CUDA_TRY(tb.alloc(&ub, (uint64_t)n * 4 + 4));
+    FC_CUDA_TRY(tb.alloc(&fbig, ((uint64_t)n + 1) * 4));
+    FC_CUDA_TRY(tb.alloc(&ftiles, ((uint64_t)n + 1) * 4));
+    FC_CUDA_TRY(tb.alloc(&bscan, ((uint64_t)n + 1) * 4));
+    FC_CUDA_TRY(tb.alloc(&tscan, ((uint64_t)n + 1) * 4));
+    k_order_flags<<<blocks, 256, 0, s>>>(d->deg0, rowlen, n, L, ub, fbig, ftiles);
+    count_launch();
+    FC_CUDA_TRY(cudaGetLastError());
+    size_t tmp_bytes = 0;
+    FC_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, fbig, bscan, n + 1, s));
+    void* tmp;
+    FC_CUDA_TRY(tb.alloc(&tmp, tmp_bytes + 16));
+    FC_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, fbig, bscan, n + 1, s));
+    FC_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, ftiles, tscan, n + 1, s));
+    uint32_t nbig = 0, ntiles = 0;
+    FC_TRY(to_host(&nbig, bscan + n, 4, s));
+    FC_TRY(to_host(&ntiles, tscan + n, 4, s));
+    if (!nbig) return FC_OK;
+    FC_TRY(dev_alloc((void**)&d->big_id, (uint64_t)n * 4 + 4, s));
+    FC_TRY(dev_alloc((void**)&d->ptab, (uint64_t)nbig * BUCKETS * 4, s));
+    d->nbig = nbig;
+    d->bytes += (uint64_t)n * 4 + (uint64_t)nbig * BUCKETS * 4;
+    const uint64_t hwords = (uint64_t)ntiles * BUCKETS + 1;
+    if (hwords >= (1ull << 31)) return FC_ERR_TOO_LARGE;
+    uint32_t *big_v, *tile_row, *hist, *G;
+    FC_CUDA_TRY(tb.alloc(&big_v, (uint64_t)nbig * 4));
+    FC_CUDA_TRY(tb.alloc(&tile_row, (uint64_t)ntiles * 4));
+    FC_CUDA_TRY(tb.alloc(&hist, hwords * 4));
+    FC_CUDA_TRY(tb.alloc(&G, hwords * 4));
+    k_order_index<<<blocks, 256, 0, s>>>(fbig, bscan, tscan, n, d->big_id, big_v, tile_row);
+    FC_CUDA_TRY(cudaGetLastError());
+    FC_CUDA_TRY(cudaMemsetAsync(hist + hwords - 1, 0, 4, s));
+    k_order_hist<<<blocks, 256, 0, s>>>(off, adj_in, d->deg0, d->node_ptr, n, L, ub, tile_row, tscan,
+                                        ntiles, hist);
+    FC_CUDA_TRY(cudaGetLastError());
+    size_t tmp2 = 0;
+    FC_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp2, hist, G, (int)hwords, s));
+    if (tmp2 > tmp_bytes) FC_CUDA_TRY(tb.alloc(&tmp, tmp2 + 16));
+    FC_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp2, hist, G, (int)hwords, s));
+    k_order_ptab<<<blocks, 256, 0, s>>>(big_v, tscan, G, nbig, d->ptab);
+    FC_CUDA_TRY(cudaGetLastError());
+    k_order_scatter<<<blocks, 256, 0, s>>>(off, adj_in, d->deg0, d->node_ptr, n, L, ub, tile_row,
+                                           tscan, G, ntiles, d->adj);
+    count_launch(4);
+    FC_CUDA_TRY(cudaGetLastError());
+    return FC_OK;
+}
+
 fc_status upload(fc_graph* g, cudaStream_t s) {
     if (!cuda_available()) return FC_ERR_NO_DEVICE;
     if (g->dev) return FC_OK;
@@ -212,6 +445,7 @@ fc_status upload(fc_graph* g, cudaStream_t s) {
         k_max<<<blocks, 256, 0, s>>>(rowlen, n, d_max + 1);
         count_launch(4);
         FC_CUDA_TRY(cudaGetLastError());
+        FC_TRY(order_rows(d, rowlen, d_off, d_in, s));
     }
     uint32_t mx[2] = {0, 0};
     FC_TRY(to_host(mx, d_max, 8, s));
@@ -244,6 +478,8 @@ void release_device(fc_graph* g, bool wait_home) {
     dev_free(d->node_ptr, 0);
     dev_free(d->adj, 0);
     dev_free(d->deg0, 0);
+    dev_free(d->big_id, 0);
+    dev_free(d->ptab, 0);
     dev_free(d->table, 0);
     dev_free(d->ws, 0);
     if (cur >= 0 && d->device != cur) cudaSetDevice(cur);
@@ -272,6 +508,11 @@ void preload_kernels() {
     cudaFuncGetAttributes(&a, k_degrees);
     cudaFuncGetAttributes(&a, k_scatter);
     cudaFuncGetAttributes(&a, k_max);
+    cudaFuncGetAttributes(&a, k_order_flags);
+    cudaFuncGetAttributes(&a, k_order_index);
+    cudaFuncGetAttributes(&a, k_order_hist);
+    cudaFuncGetAttributes(&a, k_order_ptab);
+    cudaFuncGetAttributes(&a, k_order_scatter);
     peel_preload();
     densest_preload();
     uint32_t* buf = nullptr;

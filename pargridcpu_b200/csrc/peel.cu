@@ -97,6 +97,8 @@ struct SegP {
     const uint32_t* deg0;
     uint32_t* deg;             // ncols * n * L, degrees inside the alive set
     uint32_t* t;               // table + col0 * n: UNSET while alive, then the core
+    const uint32_t* big_id;    // ordered long rows (device.h), or null
+    const uint32_t* ptab;
     uint32_t ncols, pad;
 };
 
@@ -201,6 +203,8 @@ __device__ __forceinline__ SegP seg_load(const PeelJob& j, uint32_t s) {
     g.deg0 = (const uint32_t*)__ldg((const unsigned long long*)&p->deg0);
     g.deg = (uint32_t*)__ldg((const unsigned long long*)&p->deg);
     g.t = (uint32_t*)__ldg((const unsigned long long*)&p->t);
+    g.big_id = (const uint32_t*)__ldg((const unsigned long long*)&p->big_id);
+    g.ptab = (const uint32_t*)__ldg((const unsigned long long*)&p->ptab);
     g.ncols = __ldg(&p->ncols);
     return g;
 }
@@ -317,12 +321,21 @@ __device__ bool grid_barrier(const PeelJob& j) {
 
 // ---- queues -----------------------------------------------------------------
 
-// A removed node is queued as one short item when its row has at most
-// small_row entries, else as ceil(len / CHUNK) chunk items; returns the chunk
-// count (0 for a short row).
-__device__ __forceinline__ uint32_t chunks_of(const SegP& g, uint32_t v, uint32_t small_row) {
+// A node removed at level k is queued as one short item when its row has at
+// most small_row entries, else as chunk items; returns the chunk count (0 for
+// a short row).  An ordered row (device.h) needs only the chunks covering its
+// entries of bucket >= bucket_of(k): every later entry names a neighbour whose
+// bound is below k, removed at an earlier level.  At least one chunk is
+// queued, so that every removal of a long row is one or more chunk items.
+__device__ __forceinline__ uint32_t chunks_of(const SegP& g, uint32_t v, uint32_t small_row,
+                                              uint32_t k) {
+    // the three loads are independent: one round trip
+    const uint32_t id = g.big_id ? __ldg(g.big_id + v) : NO_BIG_ROW;
     const uint32_t len = __ldg(g.node_ptr + v + 1) - __ldg(g.node_ptr + v);
-    return len <= small_row ? 0u : (len + CHUNK - 1) / CHUNK;
+    if (len <= small_row) return 0u;
+    uint32_t need = len;
+    if (id != NO_BIG_ROW) need = min(len, __ldg(g.ptab + (uint64_t)id * BUCKETS + bucket_of(k)));
+    return need ? (need + CHUNK - 1) / CHUNK : 1u;
 }
 
 __device__ __forceinline__ void write_short(const PeelJob& j, uint32_t q, uint32_t idx, uint32_t x) {
@@ -333,12 +346,27 @@ __device__ __forceinline__ void write_short(const PeelJob& j, uint32_t q, uint32
 }
 
 // Chunk items c_begin .. c_end-1 of x at queue slots first, first+1, ...
+// The high word of chunk item c of a row queued as nch chunks at level k.
+// From level 16 on (where the ordered rows' pruning acts) a row of 2 .. 32767
+// chunks is visited strided: chunk c takes the 8-entry groups c, c + nch,
+// c + 2 nch, ... (one group per lane), so that the front of an ordered row --
+// the neighbours that may still be alive -- is spread over all of its chunks
+// rather than loading its first one.  Otherwise chunk c is the CHUNK entries
+// from c * CHUNK.  Either way the row's first 256 * nch entries (clipped to
+// the row) are visited once each.
+constexpr uint32_t STRIDED = 0x80000000u;
+__device__ __forceinline__ uint32_t chunk_word(uint32_t c, uint32_t nch, uint32_t k) {
+    return (k >= 16 && nch > 1 && nch < 32768) ? (STRIDED | (nch << 16) | c) : c;
+}
+
 __device__ __forceinline__ void write_chunks(const PeelJob& j, uint32_t q, uint32_t first,
-                                             uint32_t x, uint32_t c_begin, uint32_t c_end) {
+                                             uint32_t x, uint32_t c_begin, uint32_t c_end,
+                                             uint32_t k) {
     for (uint32_t c = c_begin; c < c_end; c++) {
         const uint32_t idx = first + (c - c_begin);
         if (idx < j.qc_cap) {
-            const unsigned long long it = (unsigned long long)x | ((unsigned long long)c << 32);
+            const unsigned long long it =
+                (unsigned long long)x | ((unsigned long long)chunk_word(c, c_end, k) << 32);
             asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(j.qc[q] + idx), "l"(it)
                          : "memory");
         } else {
@@ -389,7 +417,7 @@ __device__ __forceinline__ uint32_t group_count_ge(const uint32_t* row, uint32_t
 // processed counts while it holds one (the level could otherwise end first).
 struct Local {
     uint32_t x;      // launch index, EMPTY32 when none
-    uint32_t chunk;  // 1: x's first chunk; 0: x's whole short row
+    uint32_t chunk;  // n > 0: x's first chunk of n; 0: x's whole short row
 };
 
 // Queues the nodes this warp's lanes removed (rem[i]: launch index yg[i],
@@ -398,9 +426,10 @@ struct Local {
 // my_s / my_c are the lane's short / chunk item counts.  All 32 lanes call it
 // together.
 template <int N>
-__device__ __forceinline__ void enqueue_removed(const PeelJob& j, uint32_t q, const bool (&rem)[N],
-                                                const uint32_t (&yg)[N], const uint32_t (&nch)[N],
-                                                uint32_t my_s, uint32_t my_c, Local& loc) {
+__device__ __forceinline__ void enqueue_removed(const PeelJob& j, uint32_t q, uint32_t k,
+                                                const bool (&rem)[N], const uint32_t (&yg)[N],
+                                                const uint32_t (&nch)[N], uint32_t my_s,
+                                                uint32_t my_c, Local& loc) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t any = __ballot_sync(0xffffffffu, (my_s | my_c) != 0);
     if (!any) return;
@@ -420,7 +449,7 @@ __device__ __forceinline__ void enqueue_removed(const PeelJob& j, uint32_t q, co
             else my_c -= 1;  // its first chunk stays with the warp
         }
         loc.x = __shfl_sync(0xffffffffu, px, src);
-        loc.chunk = __shfl_sync(0xffffffffu, pn, src) ? 1u : 0u;
+        loc.chunk = __shfl_sync(0xffffffffu, pn, src);
     }
     if (!__any_sync(0xffffffffu, (my_s | my_c) != 0)) return;
     const uint32_t is = warp_incl_scan(my_s);
@@ -440,7 +469,7 @@ __device__ __forceinline__ void enqueue_removed(const PeelJob& j, uint32_t q, co
                 if (!kept) write_short(j, q, bs++, yg[i]);
             } else {
                 const uint32_t c0 = kept ? 1u : 0u;
-                write_chunks(j, q, bc, yg[i], c0, nch[i]);
+                write_chunks(j, q, bc, yg[i], c0, nch[i], k);
                 bc += nch[i] - c0;
             }
         }
@@ -488,12 +517,12 @@ __device__ __forceinline__ void visit4(const PeelJob& j, const uint32_t (&seg)[4
             const SegP g = seg_load<MULTI>(j, seg[i]);
             clear_alive(j, yg[i]);
             g.t[yl[i]] = k;
-            nch[i] = chunks_of(g, yl[i] - col[i] * g.n, j.small_row);
+            nch[i] = chunks_of(g, yl[i] - col[i] * g.n, j.small_row, k);
             my_s += nch[i] == 0;
             my_c += nch[i];
         }
     }
-    enqueue_removed<4>(j, q, rem, yg, nch, my_s, my_c, loc);
+    enqueue_removed<4>(j, q, k, rem, yg, nch, my_s, my_c, loc);
 }
 
 // The same for N entries per lane that all belong to one node (a chunk of a
@@ -525,12 +554,12 @@ __device__ __forceinline__ void visit_node(const PeelJob& j, const SegP& g, uint
             const uint32_t yl = yg[i] - g.xbase;
             clear_alive(j, yg[i]);
             g.t[yl] = k;
-            nch[i] = chunks_of(g, yl - cb, j.small_row);
+            nch[i] = chunks_of(g, yl - cb, j.small_row, k);
             my_s += nch[i] == 0;
             my_c += nch[i];
         }
     }
-    enqueue_removed<N>(j, q, rem, yg, nch, my_s, my_c, loc);
+    enqueue_removed<N>(j, q, k, rem, yg, nch, my_s, my_c, loc);
 }
 
 // ---- phases ---------------------------------------------------------------
@@ -563,7 +592,7 @@ __device__ __forceinline__ void scan_nodes(const PeelJob& j, const uint32_t* src
         const bool lead = live && (lane & (G - 1)) == 0;
         const bool remove = lead && cnt < g.col0 + c + 1;
         const bool keep = lead && !remove;
-        const uint32_t nch = remove ? chunks_of(g, v, j.small_row) : 0u;
+        const uint32_t nch = remove ? chunks_of(g, v, j.small_row, k) : 0u;
         const uint32_t ns = (remove && nch == 0) ? 1u : 0u;
         if (remove) {
             clear_alive(j, x);
@@ -599,7 +628,7 @@ __device__ __forceinline__ void scan_nodes(const PeelJob& j, const uint32_t* src
         __syncthreads();
         if (keep) out[s_kbase + s_keep[warp] + kin - 1] = x;
         if (ns) write_short(j, q, s_sbase + s_short[warp] + sin - 1, x);
-        if (nch) write_chunks(j, q, s_cbase + s_chunk[warp] + cin - nch, x, 0, nch);
+        if (nch) write_chunks(j, q, s_cbase + s_chunk[warp] + cin - nch, x, 0, nch, k);
         __syncthreads();
     }
 }
@@ -753,32 +782,38 @@ __device__ __forceinline__ void expand_short(const PeelJob& j, uint32_t k, uint3
     }
 }
 
-// One CHUNK-entry piece of a long row, by the whole warp (CHUNK / 32 entries
-// per lane).
+// One chunk of a long row (chunk_word), by the whole warp (CHUNK / 32
+// entries per lane).
 template <bool MULTI>
 __device__ __forceinline__ void expand_chunk(const PeelJob& j, uint32_t k, uint32_t q,
                                              unsigned long long it, Local& loc) {
     constexpr int PER_LANE = CHUNK / 32;
     const uint32_t lane = threadIdx.x & 31;
-    const uint32_t x = (uint32_t)it, ch = (uint32_t)(it >> 32);
+    const uint32_t x = (uint32_t)it, w = (uint32_t)(it >> 32);
     const SegP g = seg_load<MULTI>(j, seg_of<MULTI>(j, x));
     const uint32_t xl = x - g.xbase;
     const uint32_t col = g.divN.div(xl);
     const uint32_t v = xl - col * g.n;
     const uint32_t rb = __ldg(g.node_ptr + v), re = __ldg(g.node_ptr + v + 1);
-    if (ch >= (re - rb + CHUNK - 1) / CHUNK) {  // no such chunk of the row
+    const uint32_t len = re - rb, full = (len + CHUNK - 1) / CHUNK;
+    const bool strided = (w & STRIDED) != 0;
+    const uint32_t nch = strided ? (w >> 16) & 0x7FFFu : 0u;
+    const uint32_t ch = strided ? (w & 0xFFFFu) : w;
+    if (strided ? (ch >= nch || nch > full) : ch >= full) {  // no such chunk of the row
         if (lane == 0) record_bad(j, x, 2);
         return;
     }
-    const uint32_t cb = rb + ch * CHUNK;
-    const uint32_t ce = min(re, cb + CHUNK);
+    // row offset of this lane's first entry and the step between its entries;
+    // offsets stay below 256 * full, under 2^24 when strided
+    const uint32_t o0 = strided ? 8u * (ch + lane * nch) : ch * CHUNK + lane;
+    const uint32_t step = strided ? 1u : 32u;
     uint32_t slot[PER_LANE];
     bool ok[PER_LANE];
 #pragma unroll
     for (int i = 0; i < PER_LANE; i++) {
-        const uint32_t p = cb + lane + 32 * i;
-        ok[i] = p < ce;
-        slot[i] = ok[i] ? __ldg(g.adj + p) : 0u;
+        const uint32_t o = o0 + step * i;
+        ok[i] = o < len && (strided || o < (ch + 1) * CHUNK);
+        slot[i] = ok[i] ? __ldg(g.adj + rb + o) : 0u;
     }
     visit_node<PER_LANE>(j, g, col, slot, ok, k, q, loc);
 }
@@ -845,7 +880,11 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j, volatile DrainBloc
             // the warp's own removal first: the next step of its cascade
             const Local cur = loc;
             loc.x = EMPTY32;
-            if (cur.chunk) expand_chunk<MULTI>(j, k, q, (unsigned long long)cur.x, loc);
+            if (cur.chunk)
+                expand_chunk<MULTI>(j, k, q,
+                                    (unsigned long long)cur.x |
+                                        ((unsigned long long)chunk_word(0, cur.chunk, k) << 32),
+                                    loc);
             else expand_short<MULTI>(j, k, q, lane == 0 ? cur.x : 0u, lane == 0, loc);
             progress = true;
             goto done_work;
@@ -1201,6 +1240,8 @@ static SegP make_seg(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t
     p.deg0 = g.deg0;
     p.deg = deg;
     p.t = table + (uint64_t)col0 * g.n;
+    p.big_id = g.big_id;
+    p.ptab = g.ptab;
     p.ncols = ncols;
     return p;
 }
@@ -1312,7 +1353,7 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
                        PeelStats* st) {
     const uint64_t bytes = peel_ws_bytes(d->n, d->L, d->entries, ncols);
     FC_TRY(ensure_ws(d, bytes, s));
-    PeelGraph g{d->n, d->L, d->entries, d->node_ptr, d->adj, d->deg0, d->max_deg + 1};
+    PeelGraph g{d->n, d->L, d->entries, d->node_ptr, d->adj, d->deg0, d->max_deg + 1, d->big_id, d->ptab};
     return peel_run(g, col0, ncols, d->table, d->ws, d->ws_bytes, s, st, true);
 }
 

@@ -121,12 +121,14 @@ static std::vector<std::pair<fc_graph*, uint64_t>> residency_victims(
     return out;
 }
 
-// Device bytes of a graph's resident copy: CSR, degrees, table and the
+// Device bytes of a graph's resident copy: CSR, degrees, table, the
+// ordered rows' index (at most one per ORDER_MIN_ROW + 1 entries) and the
 // densest search's per-graph state (an estimate: transposed table, the
 // histograms and cell records).
 static uint64_t graph_bytes(const fc_graph* g) {
     const uint64_t n = g->n, L = g->L, e = g->total_entries();
-    return 4 * (n + 1) + 4 * e + 8 * n * L + 4 * n * L + (16ull << 20);
+    const uint64_t order = 4 * n + (e / (ORDER_MIN_ROW + 1) + 1) * BUCKETS * 4;
+    return 4 * (n + 1) + 4 * e + 8 * n * L + 4 * n * L + order + (16ull << 20);
 }
 
 }  // namespace fc
