@@ -67,6 +67,9 @@ def test_golden_text(name):
 RANDOM = [
     ("cl_L1", lambda: synth.chung_lu_graph(3000, 1, 9000, 2.2, 0.0, 71)),
     ("cl_L3_hubs", lambda: synth.chung_lu_graph(20000, 3, 80000, 2.02, 0.5, 72)),
+    # cores up to 69, 392 rows over 512 entries: ordered rows, pruned and
+    # strided chunk visits
+    ("cl_deep", lambda: synth.chung_lu_graph(30000, 4, 240000, 2.1, 0.5, 9092)),
     ("cl_L12", lambda: synth.chung_lu_graph(5000, 12, 12000, 2.5, 0.4, 73)),
     ("er_L40", lambda: synth.erdos_renyi_graph(150, 40, 0.01, 0.08, 74)),
     ("er_L600", lambda: synth.erdos_renyi_graph(60, 600, 0.02, 0.1, 75)),

@@ -70,6 +70,25 @@ def test_fixed_scratch_matches_allocating_path():
         assert np.array_equal(got, ref), f"call {call}"
 
 
+def test_fixed_scratch_deep_graph_with_long_rows():
+    """Cores up to 69 and rows of up to 42,012 entries in the caller's own
+    (unordered) layout: past level 16 long rows are visited strided, which
+    must not depend on the rows being ordered."""
+    import torch
+    gen = synth.chung_lu_graph(30_000, 4, 240_000, 2.1, 0.5, 9092)
+    g = MultilayerGraph.from_pairs(gen.layers)
+    ref = g.coreindex()
+    assert ref.max() > 16
+    node_ptr, slots, deg0 = node_major(g)
+    assert np.diff(node_ptr.astype(np.int64)).max() > 512
+    d_ptr, d_adj, d_deg0 = _dev(node_ptr), _dev(slots), _dev(deg0)
+    out = torch.empty((g.L, g.n), dtype=torch.int32, device="cuda")
+    rc = _call(g.n, g.L, len(slots), d_ptr, d_adj, d_deg0, out)
+    torch.cuda.synchronize()
+    assert rc == FC_OK, native.STATUS.get(rc, rc)
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), ref)
+
+
 def test_fixed_scratch_small_graph_twice():
     import torch
     gen = synth.erdos_renyi_graph(120, 40, 0.02, 0.1, 9091)
