@@ -162,8 +162,10 @@ struct PeelGraph {
 uint64_t peel_ws_bytes(uint32_t n, uint32_t L, uint64_t entries, uint32_t ncols);
 // columns [col0, col0 + ncols) of `table` (lambda-major), scratch in `ws`;
 // allocates nothing unless `instrument` (events; a trace when FC_PEEL_TRACE)
+// or `endgame` (the last levels in one block per column; a temporary buffer
+// when the survivors' subgraphs outgrow the spent queues)
 fc_status peel_run(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* table, void* ws,
-                   size_t ws_bytes, cudaStream_t s, PeelStats* st, bool instrument);
+                   size_t ws_bytes, cudaStream_t s, PeelStats* st, bool instrument, bool endgame);
 
 // One segment of a batched launch: columns [col0, col0 + ncols) of graph g,
 // written to table (lambda-major, L*n).

@@ -76,7 +76,7 @@ extern "C" fc_status fc_coreindex_fixed_scratch(uint32_t n, uint32_t n_layers, u
     for (uint32_t c0 = 0; c0 < n_layers; c0 += cols) {
         const uint32_t nc = n_layers - c0 < cols ? n_layers - c0 : cols;
         PeelStats st;
-        FC_TRY(peel_run(g, c0, nc, table, ws, FIXED_SCRATCH_BYTES, s, &st, false));
+        FC_TRY(peel_run(g, c0, nc, table, ws, FIXED_SCRATCH_BYTES, s, &st, false, false));
     }
     return FC_OK;
 }

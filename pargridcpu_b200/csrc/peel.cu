@@ -73,7 +73,7 @@ struct alignas(128) Hot {
 
 struct PeelCtl {
     uint32_t bar_count, bar_gen, err, phase;
-    uint32_t level, alive_cur, q_cur, pad0;
+    uint32_t level, alive_cur, q_cur, stopped;  // stopped: left the rest to the endgame
     uint32_t prev_tail[2];       // per kind: items the previous level's queues held
     uint32_t alive_cnt[2];
     uint32_t levels, items, pad1, pad2;
@@ -84,6 +84,10 @@ struct PeelCtl {
     Hot tail[2][2];       // [q][s] items reserved
     Hot head[2][2];       // [q][s] items claimed
     Hot processed[2][2];  // [q][s] items fully processed
+    // endgame (one block per column): survivors, subgraph entries, levels run
+    uint32_t eg_cnt[64], eg_tot[64], eg_levels[64];
+    uint32_t eg_err, eg_pad[3];
+    uint64_t eg_base[64];  // first entry of each column's subgraph
 };
 
 // One segment: a graph's group of columns, as the kernel reads it.
@@ -123,6 +127,9 @@ struct PeelJob {
     unsigned long long* trace;
     uint32_t trace_levels;
     uint32_t max_sms;     // host side: SMs the grid may cover (0 = every SM)
+    // stop after a level's DRAIN once at most this many (column, node) pairs
+    // are alive, for the endgame to finish (0: run to the end)
+    uint32_t stop_alive;
 };
 
 // ---- memory-model helpers -------------------------------------------------
@@ -255,8 +262,16 @@ __device__ void leader_step(PeelCtl* c, const PeelJob& j) {
                 break;
             case PH_DRAIN:
                 __stcg(&c->items, items + ts + tc);
-                if ((ac ? ac1 : ac0) == 0) next = PH_DONE;
-                else advance = true;
+                if ((ac ? ac1 : ac0) == 0) {
+                    next = PH_DONE;
+                } else if ((ac ? ac1 : ac0) <= j.stop_alive) {
+                    // every removal up to this level is done: the survivors
+                    // are the nodes whose core exceeds it
+                    __stcg(&c->stopped, 1u);
+                    next = PH_DONE;
+                } else {
+                    advance = true;
+                }
                 break;
             default:
                 next = PH_DONE;
@@ -1132,7 +1147,7 @@ static fc_status reset_job(const PeelJob& j, cudaStream_t s) {
 template <bool MULTI>
 static fc_status run_job(PeelJob& j, uint32_t maxL, uint32_t threads, cudaStream_t s,
                          PeelStats* st, bool instrument, uint32_t col0, uint32_t ncols,
-                         bool* use_graph = nullptr) {
+                         bool* use_graph = nullptr, PeelCtl* ctl_out = nullptr) {
     j.idle_polls = env_u32("FC_PEEL_IDLE_POLLS", 2);
     if (!j.small_row) j.small_row = env_u32("FC_PEEL_SMALL_ROW", SMALL_ROW_DEFAULT);
     j.timeout_ns = (uint64_t)env_u32("FC_BARRIER_TIMEOUT_MS", 10000) * 1000000ull;
@@ -1189,6 +1204,7 @@ static fc_status run_job(PeelJob& j, uint32_t maxL, uint32_t threads, cudaStream
     count_launch();
     PeelCtl out;
     FC_TRY(to_host(&out, j.ctl, sizeof(out), s));
+    if (ctl_out) *ctl_out = out;
     float ms = 0;
     if (instrument) {
         cudaEventElapsedTime(&ms, e0, e1);
@@ -1225,6 +1241,391 @@ static fc_status run_job(PeelJob& j, uint32_t maxL, uint32_t threads, cudaStream
     return FC_OK;
 }
 
+// ---- endgame: each column's last levels inside one block --------------------
+//
+// Near the end of a peel the grid-wide levels cost their barriers, not their
+// work.  After level K the nodes still alive are exactly those whose core
+// exceeds K, and for k > K the (k, lambda)-cores of the graph are those of the
+// subgraph they induce.  So k_peel stops once few nodes are alive
+// (stop_alive), each column's survivors are given local ids and their
+// subgraph is compacted (k_eg_index, k_eg_scan, k_eg_fill), and one block per
+// column runs the remaining levels on it (k_endgame) with the same rules:
+// degrees, counts, alive flags, lists and queue in shared memory, rounds
+// separated by __syncthreads instead of grid barriers.  Every loop is bounded
+// (levels by the level cap, rounds by the survivors); no block waits on
+// another.
+
+constexpr uint32_t EG_THREADS = 1024;
+constexpr uint32_t EG_MAX_COLS = 64;
+constexpr uint32_t EG_SMEM = 220u * 1024u;  // dynamic shared memory of k_endgame
+constexpr uint32_t EG_FILL_SPLIT = 4096;    // longer rows are filled by a whole block
+
+// shared bytes per survivor: degrees (L halves), count (a half), alive flag,
+// two alive lists and the queue (16-bit local ids)
+static uint32_t eg_node_bytes(uint32_t L) { return 2 * L + 9; }
+// survivors one column's block can hold (0: the endgame is off for this L)
+static uint32_t eg_capacity(uint32_t L) {
+    const uint64_t fixed = 8ull * EG_THREADS + 256;  // batch prefixes and row starts + alignment
+    uint64_t cap = (EG_SMEM - fixed) / eg_node_bytes(L);
+    if (cap > 65535) cap = 65535;
+    return cap >= 1024 ? (uint32_t)cap : 0u;
+}
+
+// Local ids of the survivors, per column; their subgraph row lengths are
+// the alive-neighbour degrees the peel maintained.
+__global__ void k_eg_index(const uint32_t* __restrict__ alive, uint32_t nalive,
+                           const uint32_t* __restrict__ bits, FastDiv divN, uint32_t n, uint32_t L,
+                           const uint32_t* __restrict__ deg, uint32_t cap,
+                           uint32_t* __restrict__ map, uint32_t* __restrict__ ecnt,
+                           uint32_t* __restrict__ l2g, uint32_t* __restrict__ rowlen) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nalive;
+         i += gridDim.x * blockDim.x) {
+        const uint32_t x = alive[i];
+        if (!((bits[x >> 5] >> (x & 31)) & 1u)) continue;
+        const uint32_t c = divN.div(x), v = x - c * n;
+        const uint32_t lid = atomicAdd(ecnt + c, 1u);
+        if (lid >= cap) continue;  // the host sees the count and fails the run
+        map[x] = lid;
+        l2g[(uint64_t)c * cap + lid] = v;
+        const uint32_t* d = deg + (uint64_t)c * n * L + (uint64_t)v * L;
+        uint32_t sum = 0;
+        for (uint32_t l = 0; l < L; l++) sum += d[l];
+        rowlen[(uint64_t)c * (cap + 1) + lid] = sum;
+    }
+}
+
+// Block-wide exclusive scan of the 1024 threads' values; returns the total.
+__device__ __forceinline__ uint32_t eg_block_scan(uint32_t v, uint32_t* excl, uint32_t* s_warp) {
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t in = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, in, d);
+        if (lane >= (uint32_t)d) in += t;
+    }
+    __syncthreads();
+    if (lane == 31) s_warp[w] = in;
+    __syncthreads();
+    if (w == 0) {
+        uint32_t x = s_warp[lane];
+        uint32_t y = x;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, y, d);
+            if (lane >= (uint32_t)d) y += t;
+        }
+        s_warp[lane] = y - x;  // exclusive
+        if (lane == 31) s_warp[32] = y;
+    }
+    __syncthreads();
+    *excl = s_warp[w] + in - v;
+    const uint32_t total = s_warp[32];
+    __syncthreads();
+    return total;
+}
+
+// One block per column: row offsets of its subgraph (exclusive scan of the
+// row lengths, m + 1 values) and its entry count.
+__global__ void __launch_bounds__(EG_THREADS) k_eg_scan(const uint32_t* __restrict__ rowlen,
+                                                        uint32_t* __restrict__ rowptr, uint32_t cap,
+                                                        const uint32_t* __restrict__ ecnt,
+                                                        uint32_t* __restrict__ etot) {
+    __shared__ uint32_t s_warp[33];
+    const uint32_t c = blockIdx.x;
+    const uint32_t m = min(ecnt[c], cap);
+    const uint32_t* in = rowlen + (uint64_t)c * (cap + 1);
+    uint32_t* out = rowptr + (uint64_t)c * (cap + 1);
+    const uint32_t per = (m + EG_THREADS - 1) / EG_THREADS;
+    const uint32_t b = threadIdx.x * per, e = min(m, b + per);
+    uint32_t sum = 0;
+    for (uint32_t i = b; i < e; i++) sum += in[i];
+    uint32_t base;
+    const uint32_t total = eg_block_scan(sum, &base, s_warp);
+    for (uint32_t i = b; i < e; i++) {
+        out[i] = base;
+        base += in[i];
+    }
+    if (threadIdx.x == 0) {
+        out[m] = total;
+        etot[c] = total;
+    }
+}
+
+// The part of survivor v's row that can name survivors: an ordered row is read
+// only as far as its entries of bucket >= bucket_of(K+1), the rest name nodes
+// whose bound, hence core, is at most K.
+__device__ __forceinline__ uint32_t eg_need(const uint32_t* __restrict__ node_ptr,
+                                            const uint32_t* __restrict__ big_id,
+                                            const uint32_t* __restrict__ ptab, uint32_t v,
+                                            uint32_t k1, uint32_t* rb) {
+    *rb = node_ptr[v];
+    const uint32_t len = node_ptr[v + 1] - *rb;
+    uint32_t need = len;
+    if (big_id && len > ORDER_MIN_ROW) {
+        const uint32_t id = big_id[v];
+        if (id != NO_BIG_ROW) need = min(len, ptab[(uint64_t)id * BUCKETS + bucket_of(k1)]);
+    }
+    return need;
+}
+
+// One warp per survivor whose row part is at most EG_FILL_SPLIT entries: its
+// subgraph row, the alive neighbours in row order, as local slots lid * L + l.
+// Rows whose alive-neighbour count differs from the degrees the peel kept
+// flag an error.
+__global__ void k_eg_fill(const uint32_t* __restrict__ alive, uint32_t nalive,
+                          const uint32_t* __restrict__ bits, FastDiv divN, FastDiv divL, uint32_t n,
+                          uint32_t L, const uint32_t* __restrict__ node_ptr,
+                          const uint32_t* __restrict__ adj, const uint32_t* __restrict__ big_id,
+                          const uint32_t* __restrict__ ptab, uint32_t k1,
+                          const uint32_t* __restrict__ map, uint32_t cap,
+                          const uint32_t* __restrict__ rowptr, const uint64_t* __restrict__ base,
+                          uint32_t* __restrict__ H, uint32_t* __restrict__ err) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < nalive; i += warps) {
+        const uint32_t x = alive[i];
+        if (!((bits[x >> 5] >> (x & 31)) & 1u)) continue;
+        const uint32_t c = divN.div(x), v = x - c * n;
+        const uint32_t lid = map[x];
+        if (lid >= cap) continue;
+        const uint32_t* rp = rowptr + (uint64_t)c * (cap + 1);
+        const uint32_t o0 = rp[lid], want = rp[lid + 1] - o0;
+        uint32_t* dst = H + base[c] + o0;
+        uint32_t rb;
+        const uint32_t need = eg_need(node_ptr, big_id, ptab, v, k1, &rb);
+        if (need > EG_FILL_SPLIT) continue;  // k_eg_fill_big
+        uint32_t got = 0;
+        for (uint32_t p0 = 0; p0 < need; p0 += 32) {
+            const uint32_t p = p0 + lane;
+            uint32_t u = 0, l = 0;
+            bool al = false;
+            if (p < need) {
+                const uint32_t slot = adj[rb + p];
+                u = divL.div(slot);
+                l = slot - u * L;
+                const uint32_t y = c * n + u;
+                al = (bits[y >> 5] >> (y & 31)) & 1u;
+            }
+            const uint32_t mk = __ballot_sync(0xffffffffu, al);
+            if (al) {
+                const uint32_t pos = got + __popc(mk & lt);
+                if (pos < want) dst[pos] = map[c * n + u] * L + l;
+            }
+            got += __popc(mk);
+        }
+        if (lane == 0 && got != want) atomicExch(err, 1u);
+    }
+}
+
+// One block per survivor whose row part exceeds EG_FILL_SPLIT entries, in
+// tiles of 4 * EG_THREADS entries: each thread counts its four, a block scan
+// places them (thread-major within a tile; deterministic).
+__global__ void __launch_bounds__(EG_THREADS) k_eg_fill_big(
+    const uint32_t* __restrict__ alive, uint32_t nalive, const uint32_t* __restrict__ bits,
+    FastDiv divN, FastDiv divL, uint32_t n, uint32_t L, const uint32_t* __restrict__ node_ptr,
+    const uint32_t* __restrict__ adj, const uint32_t* __restrict__ big_id,
+    const uint32_t* __restrict__ ptab, uint32_t k1, const uint32_t* __restrict__ map, uint32_t cap,
+    const uint32_t* __restrict__ rowptr, const uint64_t* __restrict__ base,
+    uint32_t* __restrict__ H, uint32_t* __restrict__ err) {
+    __shared__ uint32_t s_warp[33];
+    for (uint32_t i = blockIdx.x; i < nalive; i += gridDim.x) {
+        const uint32_t x = alive[i];
+        if (!((bits[x >> 5] >> (x & 31)) & 1u)) continue;
+        const uint32_t c = divN.div(x), v = x - c * n;
+        const uint32_t lid = map[x];
+        if (lid >= cap) continue;
+        uint32_t rb;
+        const uint32_t need = eg_need(node_ptr, big_id, ptab, v, k1, &rb);
+        if (need <= EG_FILL_SPLIT) continue;  // k_eg_fill
+        const uint32_t* rp = rowptr + (uint64_t)c * (cap + 1);
+        const uint32_t o0 = rp[lid], want = rp[lid + 1] - o0;
+        uint32_t* dst = H + base[c] + o0;
+        uint32_t got = 0;
+        for (uint32_t p0 = 0; p0 < need; p0 += 4 * EG_THREADS) {
+            uint32_t val[4], cnt = 0;
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const uint32_t p = p0 + r * EG_THREADS + threadIdx.x;
+                val[r] = UNSET;
+                if (p < need) {
+                    const uint32_t slot = adj[rb + p];
+                    const uint32_t u = divL.div(slot), l = slot - u * L;
+                    const uint32_t y = c * n + u;
+                    if ((bits[y >> 5] >> (y & 31)) & 1u) {
+                        val[r] = map[y] * L + l;
+                        cnt++;
+                    }
+                }
+            }
+            uint32_t off;
+            const uint32_t total = eg_block_scan(cnt, &off, s_warp);
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+                if (val[r] != UNSET) {
+                    const uint32_t pos = got + off++;
+                    if (pos < want) dst[pos] = val[r];
+                }
+            got += total;
+        }
+        if (threadIdx.x == 0 && got != want) atomicExch(err, 1u);
+    }
+}
+
+__device__ __forceinline__ uint32_t eg_get16(const uint32_t* w, uint32_t i) {
+    return (w[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
+}
+// decrements half i of w; returns its old value.  A half is only decremented
+// while it is at least 1 (every decrement stands for a neighbour it counts),
+// so no borrow reaches the other half.
+__device__ __forceinline__ uint32_t eg_dec16(uint32_t* w, uint32_t i) {
+    const uint32_t sh = (i & 1) * 16;
+    return (atomicSub(w + (i >> 1), 1u << sh) >> sh) & 0xFFFFu;
+}
+
+// One block per column: the levels k0, k0+1, ... of the column's subgraph
+// until no survivor is left (or the level cap, an error).
+__global__ void __launch_bounds__(EG_THREADS) k_endgame(
+    uint32_t cap, const uint32_t* __restrict__ ecnt, const uint32_t* __restrict__ rowptr,
+    const uint64_t* __restrict__ base, const uint32_t* __restrict__ H,
+    const uint32_t* __restrict__ l2g, const uint32_t* __restrict__ deg, uint32_t n, uint32_t L,
+    FastDiv divL, uint32_t* __restrict__ t, uint32_t col0, uint32_t k0, uint32_t max_level,
+    uint32_t* __restrict__ levels, uint32_t* __restrict__ err) {
+    extern __shared__ __align__(16) uint32_t sm[];
+    __shared__ uint32_t s_warp[33];
+    __shared__ uint32_t s_nalive, s_next, s_tail;
+    const uint32_t c = blockIdx.x;
+    const uint32_t m = min(ecnt[c], cap);
+    if (m == 0) return;
+    const uint32_t lmd = col0 + c + 1;
+    const uint32_t* rp = rowptr + (uint64_t)c * (cap + 1);
+    const uint32_t* Hc = H + base[c];
+    const uint32_t* g_of = l2g + (uint64_t)c * cap;
+    uint32_t* tc = t + (uint64_t)c * n;
+    // shared layout: degrees | counts | batch prefixes | batch row starts |
+    // alive | lists | queue
+    uint32_t* dw = sm;                                   // (m * L + 1) / 2 words
+    uint32_t* cw = dw + ((uint64_t)m * L + 1) / 2;       // (m + 1) / 2 words
+    uint32_t* pre = cw + (m + 1) / 2;                    // EG_THREADS words
+    uint32_t* rs = pre + EG_THREADS;                     // EG_THREADS words
+    uint8_t* alive = (uint8_t*)(rs + EG_THREADS);        // m bytes
+    uint16_t* list0 = (uint16_t*)(((uintptr_t)(alive + m) + 3) & ~(uintptr_t)3);
+    uint16_t* list1 = list0 + m;
+    uint16_t* queue = list1 + m;
+    for (uint32_t i = threadIdx.x; i < ((uint64_t)m * L + 1) / 2; i += blockDim.x) dw[i] = 0;
+    for (uint32_t i = threadIdx.x; i < (m + 1) / 2; i += blockDim.x) cw[i] = 0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < m * L; i += blockDim.x) {
+        const uint32_t lid = i / L, l = i - lid * L;
+        const uint32_t d = deg[(uint64_t)c * n * L + (uint64_t)g_of[lid] * L + l];
+        atomicOr(dw + (i >> 1), (d & 0xFFFFu) << ((i & 1) * 16));
+    }
+    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+        alive[i] = 1;
+        list0[i] = (uint16_t)i;
+    }
+    if (threadIdx.x == 0) s_nalive = m;
+    __syncthreads();
+    uint16_t* cur = list0;
+    uint16_t* nxt = list1;
+    uint32_t k = k0;
+    for (;;) {
+        const uint32_t na = s_nalive;
+        if (na == 0) break;
+        if (k > max_level) {
+            if (threadIdx.x == 0) atomicExch(err, 2u);
+            break;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_next = 0;
+            s_tail = 0;
+        }
+        __syncthreads();
+        // SCAN(k)
+        for (uint32_t i = threadIdx.x; i < na; i += blockDim.x) {
+            const uint32_t x = cur[i];
+            if (!alive[x]) continue;
+            uint32_t cnt = 0;
+            for (uint32_t l = 0; l < L; l++) cnt += eg_get16(dw, x * L + l) >= k + 1;
+            if (cnt < lmd) {
+                alive[x] = 0;
+                tc[g_of[x]] = k;
+                queue[atomicAdd(&s_tail, 1u)] = (uint16_t)x;
+            } else {
+                atomicOr(cw + (x >> 1), cnt << ((x & 1) * 16));  // the half was 0
+                nxt[atomicAdd(&s_next, 1u)] = (uint16_t)x;
+            }
+        }
+        __syncthreads();
+        // DRAIN(k): rounds over the queue, each round's rows flattened over
+        // the block in batches of EG_THREADS items
+        uint32_t qb = 0;
+        for (uint32_t round = 0; round <= m; round++) {
+            const uint32_t qe = s_tail;
+            __syncthreads();
+            if (qb >= qe) break;
+            for (uint32_t b0 = qb; b0 < qe; b0 += EG_THREADS) {
+                const uint32_t nb = min(EG_THREADS, qe - b0);
+                uint32_t len = 0, start = 0;
+                if (threadIdx.x < nb) {
+                    const uint32_t x = queue[b0 + threadIdx.x];
+                    start = rp[x];
+                    len = rp[x + 1] - start;
+                }
+                uint32_t ex;
+                const uint32_t total = eg_block_scan(len, &ex, s_warp);
+                pre[threadIdx.x] = ex;
+                rs[threadIdx.x] = start;
+                __syncthreads();
+                // four entries per thread at a time, their loads first
+                uint32_t lo0 = 0;  // this thread's entries only move forward
+                for (uint32_t e0 = threadIdx.x; e0 < total; e0 += 4 * blockDim.x) {
+                    uint32_t slot[4];
+#pragma unroll
+                    for (int r = 0; r < 4; r++) {
+                        const uint32_t e = e0 + r * blockDim.x;
+                        slot[r] = UNSET;
+                        if (e < total) {
+                            uint32_t lo = lo0, hi = nb - 1;  // last item whose prefix is <= e
+                            while (lo < hi) {
+                                const uint32_t mid = (lo + hi + 1) >> 1;
+                                if (pre[mid] <= e) lo = mid;
+                                else hi = mid - 1;
+                            }
+                            lo0 = lo;
+                            slot[r] = Hc[rs[lo] + (e - pre[lo])];
+                        }
+                    }
+#pragma unroll
+                    for (int r = 0; r < 4; r++) {
+                        if (slot[r] == UNSET) continue;
+                        const uint32_t u = divL.div(slot[r]);
+                        if (u >= m || !alive[u]) continue;
+                        const uint32_t old = eg_dec16(dw, slot[r]);
+                        if (old == k + 1 && eg_dec16(cw, u) == lmd) {
+                            alive[u] = 0;
+                            tc[g_of[u]] = k;
+                            queue[atomicAdd(&s_tail, 1u)] = (uint16_t)u;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+            qb = qe;
+        }
+        // counts are rebuilt by the next SCAN: clear the kept ones
+        for (uint32_t i = threadIdx.x; i < (m + 1) / 2; i += blockDim.x) cw[i] = 0;
+        if (threadIdx.x == 0) s_nalive = s_next;
+        uint16_t* tmp = cur;
+        cur = nxt;
+        nxt = tmp;
+        k++;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) levels[c] = k - k0;
+}
+
 static SegP make_seg(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* table,
                      uint32_t* deg, uint32_t xbase) {
     SegP p{};
@@ -1246,8 +1647,123 @@ static SegP make_seg(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t
     return p;
 }
 
+static int peel_sms() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
+// The endgame after a k_peel launch that stopped (see k_endgame): the
+// survivors' subgraphs are built in buffers the peel no longer needs (its
+// count array holds the local ids, the other alive list the local-to-global
+// map, the node queues the row offsets and the chunk queues the entries, or
+// a temporary buffer when they do not fit), then one block per column.
+static fc_status endgame_run(const PeelJob& j, const PeelGraph& g, const PeelCtl& out, uint32_t col0,
+                             uint32_t ncols, uint32_t cap, cudaStream_t s, PeelStats* st,
+                             bool instrument) {
+    const uint32_t K = out.level, ac = out.alive_cur & 1u;
+    const uint32_t nalive = out.alive_cnt[ac];
+    const uint32_t capE = cap < g.n ? cap : g.n;
+    if (ncols > EG_MAX_COLS || (uint64_t)ncols * capE > j.nx ||
+        (uint64_t)ncols * (capE + 1) > j.qs_cap)
+        return FC_ERR_INVALID;
+    PeelCtl* c = j.ctl;
+    const uint32_t* alive = j.alive[ac];
+    uint32_t* map = j.cnt;
+    uint32_t* l2g = j.alive[ac ^ 1];
+    uint32_t* rowlen = j.qs[1];
+    uint32_t* rowptr = j.qs[0];
+    const uint32_t* deg = j.seg0.deg;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (instrument) {
+        FC_CUDA_TRY(cudaEventCreate(&e0));
+        FC_CUDA_TRY(cudaEventCreate(&e1));
+        FC_CUDA_TRY(cudaEventRecord(e0, s));
+    }
+    FastDiv divN, divL;
+    divN.init(g.n);
+    divL.init(g.L);
+    const int blocks = peel_sms() * 8;
+    k_eg_index<<<blocks, 256, 0, s>>>(alive, nalive, j.bits, divN, g.n, g.L, deg, capE, map,
+                                      c->eg_cnt, l2g, rowlen);
+    FC_CUDA_TRY(cudaGetLastError());
+    uint32_t cnts[EG_MAX_COLS], tots[EG_MAX_COLS];
+    FC_TRY(to_host(cnts, c->eg_cnt, 4ull * ncols, s));
+    uint32_t mmax = 0;
+    for (uint32_t i = 0; i < ncols; i++) {
+        if (cnts[i] > capE) return FC_ERR_DEVICE;  // more survivors than the stop rule allows
+        mmax = cnts[i] > mmax ? cnts[i] : mmax;
+    }
+    k_eg_scan<<<ncols, EG_THREADS, 0, s>>>(rowlen, rowptr, capE, c->eg_cnt, c->eg_tot);
+    FC_CUDA_TRY(cudaGetLastError());
+    FC_TRY(to_host(tots, c->eg_tot, 4ull * ncols, s));
+    uint64_t bases[EG_MAX_COLS], total = 0;
+    for (uint32_t i = 0; i < ncols; i++) {
+        bases[i] = total;
+        total += tots[i];
+    }
+    uint32_t* H = (uint32_t*)j.qc[0];  // both parities' chunk queues: 4 * qc_cap words
+    uint32_t* temp = nullptr;
+    if (total > 4ull * j.qc_cap) {
+        FC_TRY(dev_alloc((void**)&temp, total * 4 + 4, s));
+        H = temp;
+    }
+    fc_status rc = to_device(c->eg_base, bases, 8ull * ncols, s);
+    if (rc == FC_OK) {
+        k_eg_fill<<<blocks, 256, 0, s>>>(alive, nalive, j.bits, divN, divL, g.n, g.L, g.node_ptr,
+                                         g.adj, g.big_id, g.ptab, K + 1, map, capE, rowptr,
+                                         c->eg_base, H, &c->eg_err);
+        k_eg_fill_big<<<peel_sms() * 2, EG_THREADS, 0, s>>>(
+            alive, nalive, j.bits, divN, divL, g.n, g.L, g.node_ptr, g.adj, g.big_id, g.ptab, K + 1,
+            map, capE, rowptr, c->eg_base, H, &c->eg_err);
+        static const cudaError_t attr_rc = cudaFuncSetAttribute(
+            k_endgame, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)EG_SMEM);
+        const uint64_t smem =
+            4ull * (((uint64_t)mmax * g.L + 1) / 2 + (mmax + 1) / 2 + 2ull * EG_THREADS) + mmax + 4 +
+            6ull * mmax + 16;
+        if (attr_rc != cudaSuccess || smem > EG_SMEM) {
+            rc = FC_ERR_DEVICE;
+        } else {
+            k_endgame<<<ncols, EG_THREADS, (size_t)smem, s>>>(
+                capE, c->eg_cnt, rowptr, c->eg_base, H, l2g, deg, g.n, g.L, divL, j.seg0.t, col0,
+                K + 1, j.max_level, c->eg_levels, &c->eg_err);
+            count_launch(5);
+            const cudaError_t le = cudaGetLastError();
+            if (le != cudaSuccess) {
+                set_last_cuda_error(le, "k_endgame", __FILE__, __LINE__);
+                rc = FC_ERR_DEVICE;
+            }
+        }
+    }
+    uint32_t tail[EG_MAX_COLS + 1];  // eg_levels then eg_err
+    if (rc == FC_OK) rc = to_host(tail, c->eg_levels, 4ull * (EG_MAX_COLS + 1), s);
+    if (temp) dev_free(temp, s);
+    if (instrument) {
+        float ms = 0;
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (st) st->ms += ms;
+    }
+    FC_TRY(rc);
+    if (tail[EG_MAX_COLS]) return tail[EG_MAX_COLS] == 2 ? FC_ERR_ITER_LIMIT : FC_ERR_DEVICE;
+    if (st) {
+        uint32_t lv = 0;
+        for (uint32_t i = 0; i < ncols; i++) lv = tail[i] > lv ? tail[i] : lv;
+        st->levels += lv;
+    }
+    return FC_OK;
+}
+
 fc_status peel_run(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* table, void* ws,
-                   size_t ws_bytes, cudaStream_t s, PeelStats* st, bool instrument) {
+                   size_t ws_bytes, cudaStream_t s, PeelStats* st, bool instrument, bool endgame) {
     const uint64_t nx = (uint64_t)ncols * g.n;
     if (peel_ws_bytes(g.n, g.L, g.entries, ncols) > ws_bytes) return FC_ERR_INVALID;
     PeelJob j{};
@@ -1265,7 +1781,13 @@ fc_status peel_run(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* 
     j.seg_xbase = nullptr;
     j.nseg = 1;
     j.max_level = g.max_level;
-    return run_job<false>(j, g.L, default_threads(), s, st, instrument, col0, ncols);
+    const uint32_t cap = (endgame && ncols <= EG_MAX_COLS && env_u32("FC_PEEL_ENDGAME", 1))
+                             ? eg_capacity(g.L) : 0u;
+    j.stop_alive = cap;
+    PeelCtl out;
+    FC_TRY(run_job<false>(j, g.L, default_threads(), s, st, instrument, col0, ncols, nullptr, &out));
+    if (!out.stopped) return FC_OK;
+    return endgame_run(j, g, out, col0, ncols, cap, s, st, instrument);
 }
 
 uint64_t peel_batch_ws_bytes(const std::vector<PeelSegSpec>& specs) {
@@ -1346,6 +1868,11 @@ void peel_preload() {
     cudaFuncGetAttributes(&a, k_peel<32, 512, true>);
     cudaFuncGetAttributes(&a, k_peel<32, 1024, false>);
     cudaFuncGetAttributes(&a, k_peel<32, 1024, true>);
+    cudaFuncGetAttributes(&a, k_eg_index);
+    cudaFuncGetAttributes(&a, k_eg_scan);
+    cudaFuncGetAttributes(&a, k_eg_fill);
+    cudaFuncGetAttributes(&a, k_eg_fill_big);
+    cudaFuncGetAttributes(&a, k_endgame);
     cudaGetLastError();
 }
 
@@ -1354,7 +1881,7 @@ fc_status peel_columns(DeviceGraph* d, uint32_t col0, uint32_t ncols, cudaStream
     const uint64_t bytes = peel_ws_bytes(d->n, d->L, d->entries, ncols);
     FC_TRY(ensure_ws(d, bytes, s));
     PeelGraph g{d->n, d->L, d->entries, d->node_ptr, d->adj, d->deg0, d->max_deg + 1, d->big_id, d->ptab};
-    return peel_run(g, col0, ncols, d->table, d->ws, d->ws_bytes, s, st, true);
+    return peel_run(g, col0, ncols, d->table, d->ws, d->ws_bytes, s, st, true, true);
 }
 
 }  // namespace fc
