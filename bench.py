@@ -312,9 +312,10 @@ def run_ours(args, world, rank, local):
 
     if rank != 0:
         return
-    # roofline of the dominant kernel (the peel): algorithmic bytes per launch
-    # (per lambda column: 4*2M adjacency + 4*L*(n+1) offsets + 2*4*L*n degree
-    # table + 4*n core output) over the mean CUDA-event launch time
+    # roofline of the dominant stage (the peel: k_peel and, when it stops
+    # early, the endgame kernels that finish the columns): algorithmic bytes
+    # per peel group (per lambda column: 4*2M adjacency + 4*L*(n+1) offsets +
+    # 2*4*L*n degree table + 4*n core output) over the mean CUDA-event time
     cols = stats["columns_per_launch"] or L
     per_col = 4 * m2 + 4 * L * (n + 1) + 8 * L * n + 4 * n
     bytes_per_launch = cols * per_col
@@ -334,7 +335,8 @@ def run_ours(args, world, rank, local):
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "k_peel", "peak_kind": peak_kind,
+                         "kernel": "k_peel + endgame (k_eg_index, k_eg_scan, k_eg_fill, "
+                                   "k_eg_fill_big, k_endgame)", "peak_kind": peak_kind,
                          "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms,
                          # atomics are reported beside the bytes, not folded in
                          "l2_atomic_sectors_per_launch": atom_sectors,
