@@ -1679,11 +1679,17 @@ static fc_status endgame_run(const PeelJob& j, const PeelGraph& g, const PeelCtl
     uint32_t* rowlen = j.qs[1];
     uint32_t* rowptr = j.qs[0];
     const uint32_t* deg = j.seg0.deg;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    struct Events {  // destroyed on every return
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        ~Events() {
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+        }
+    } ev;
     if (instrument) {
-        FC_CUDA_TRY(cudaEventCreate(&e0));
-        FC_CUDA_TRY(cudaEventCreate(&e1));
-        FC_CUDA_TRY(cudaEventRecord(e0, s));
+        FC_CUDA_TRY(cudaEventCreate(&ev.e0));
+        FC_CUDA_TRY(cudaEventCreate(&ev.e1));
+        FC_CUDA_TRY(cudaEventRecord(ev.e0, s));
     }
     FastDiv divN, divL;
     divN.init(g.n);
@@ -1745,11 +1751,9 @@ static fc_status endgame_run(const PeelJob& j, const PeelGraph& g, const PeelCtl
     if (temp) dev_free(temp, s);
     if (instrument) {
         float ms = 0;
-        cudaEventRecord(e1, s);
-        cudaEventSynchronize(e1);
-        cudaEventElapsedTime(&ms, e0, e1);
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
+        cudaEventRecord(ev.e1, s);
+        cudaEventSynchronize(ev.e1);
+        cudaEventElapsedTime(&ms, ev.e0, ev.e1);
         if (st) st->ms += ms;
     }
     FC_TRY(rc);
