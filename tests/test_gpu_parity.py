@@ -98,6 +98,18 @@ def test_random_vs_oracle(name, make):
         assert np.array_equal(nodes, o["nodes"]) and np.array_equal(layers, o["layers"])
 
 
+@pytest.mark.parametrize("name", ["cl_L3_hubs", "cl_deep", "cl_L12"])
+def test_endgame_on_and_off_agree(name, monkeypatch):
+    """The peel's endgame (the last levels of each column in one block on the
+    survivors' subgraph) gives the table the grid-wide peel gives alone."""
+    gen = dict(RANDOM)[name]()
+    ref = O.OracleGraph(gen.layers).coreindex()
+    with_eg = MultilayerGraph.from_pairs(gen.layers).coreindex()
+    monkeypatch.setenv("FC_PEEL_ENDGAME", "0")
+    without = MultilayerGraph.from_pairs(gen.layers).coreindex()
+    assert np.array_equal(with_eg, ref) and np.array_equal(without, ref)
+
+
 def test_repeatable_and_reset():
     gen = synth.chung_lu_graph(30000, 4, 60000, 2.1, 0.5, 81)
     g = MultilayerGraph.from_pairs(gen.layers)
