@@ -47,8 +47,9 @@ namespace {
 // Open-addressing map raw id -> internal id; ids are handed out in order of
 // first sight (MultilayerGraph.cpp:127-143: u is looked up before v).
 struct IdMap {
-    std::vector<uint32_t> key, val;
-    std::vector<uint8_t> used;
+    // open addressing, one 8-byte slot per entry: key in the high half, id + 1
+    // in the low half (0: empty), so a probe touches one cache line
+    std::vector<uint64_t> tab;
     uint64_t mask = 0, size = 0;
     std::vector<uint64_t>* id2vtx;
     explicit IdMap(std::vector<uint64_t>* out) : id2vtx(out) { rehash(1 << 16); }
@@ -57,32 +58,25 @@ struct IdMap {
         return z ^ (z >> 29);
     }
     void rehash(uint64_t cap) {
-        std::vector<uint32_t> k2(cap), v2(cap);
-        std::vector<uint8_t> u2(cap, 0);
-        uint64_t m2 = cap - 1;
-        for (uint64_t i = 0; i < used.size(); i++) {
-            if (!used[i]) continue;
-            uint64_t j = h(key[i]) & m2;
-            while (u2[j]) j = (j + 1) & m2;
-            u2[j] = 1;
-            k2[j] = key[i];
-            v2[j] = val[i];
+        std::vector<uint64_t> t2(cap, 0);
+        const uint64_t m2 = cap - 1;
+        for (uint64_t s : tab) {
+            if (!s) continue;
+            uint64_t j = h((uint32_t)(s >> 32)) & m2;
+            while (t2[j]) j = (j + 1) & m2;
+            t2[j] = s;
         }
-        key.swap(k2);
-        val.swap(v2);
-        used.swap(u2);
+        tab.swap(t2);
         mask = m2;
     }
+    // the lookup of x is about to come: bring its first slot in
+    void prefetch(uint32_t x) const { __builtin_prefetch(tab.data() + (h(x) & mask)); }
     uint32_t get(uint32_t x) {
         uint64_t j = h(x) & mask;
-        while (used[j]) {
-            if (key[j] == x) return val[j];
-            j = (j + 1) & mask;
-        }
-        uint32_t id = (uint32_t)size++;
-        used[j] = 1;
-        key[j] = x;
-        val[j] = id;
+        for (uint64_t s; (s = tab[j]) != 0; j = (j + 1) & mask)
+            if ((uint32_t)(s >> 32) == x) return (uint32_t)s - 1;
+        const uint32_t id = (uint32_t)size++;
+        tab[j] = ((uint64_t)x << 32) | ((uint64_t)id + 1);
         id2vtx->push_back(x);
         if (size * 2 > mask) rehash((mask + 1) * 2);
         return id;
@@ -177,14 +171,17 @@ void parse_pairs(const std::vector<char>& text, std::vector<uint32_t>& out) {
 
 // Per-layer CSR from remapped directed pairs: rows ascending, duplicates
 // dropped (Graph.cpp:27-47).  Counting sort by source, then each row sorted.
-void build_layer(uint32_t n, const std::vector<uint32_t>& dir_pairs, std::vector<uint64_t>& off,
-                 std::vector<uint32_t>& adj) {
+// C: the count type, 32-bit when the layer's entries fit (half the bytes of
+// the two randomly written count arrays)
+template <class C>
+void build_layer_t(uint32_t n, const std::vector<uint32_t>& dir_pairs, std::vector<uint64_t>& off,
+                   std::vector<uint32_t>& adj) {
     uint64_t m = dir_pairs.size() / 2;
-    std::vector<uint64_t> cnt((size_t)n + 1, 0);
+    std::vector<C> cnt((size_t)n + 1, 0);
     for (uint64_t i = 0; i < m; i++) cnt[dir_pairs[2 * i] + 1]++;
     for (uint32_t v = 0; v < n; v++) cnt[v + 1] += cnt[v];
     std::vector<uint32_t> tgt(m);
-    std::vector<uint64_t> pos(cnt.begin(), cnt.end() - 1);
+    std::vector<C> pos(cnt.begin(), cnt.end() - 1);
     for (uint64_t i = 0; i < m; i++) tgt[pos[dir_pairs[2 * i]]++] = dir_pairs[2 * i + 1];
     off.assign((size_t)n + 1, 0);
     adj.clear();
@@ -198,6 +195,12 @@ void build_layer(uint32_t n, const std::vector<uint32_t>& dir_pairs, std::vector
             if (q == b || *q != q[-1]) adj.push_back(*q);
     }
     off[n] = adj.size();
+}
+
+void build_layer(uint32_t n, const std::vector<uint32_t>& dir_pairs, std::vector<uint64_t>& off,
+                 std::vector<uint32_t>& adj) {
+    if (dir_pairs.size() / 2 < (1ull << 32)) build_layer_t<uint32_t>(n, dir_pairs, off, adj);
+    else build_layer_t<uint64_t>(n, dir_pairs, off, adj);
 }
 
 // f(l) for every layer l, on up to one host thread per core (layers are
@@ -251,6 +254,10 @@ fc_status build_from_pairs(uint32_t L, const uint64_t* m, const uint32_t* pairs,
     for (uint32_t l = 0; l < L; l++) {
         dir[l].reserve(2 * m[l] * 2);
         for (uint64_t i = 0; i < m[l]; i++, p += 2) {
+            if (i + 8 < m[l]) {  // the slots 8 pairs ahead
+                map.prefetch(p[16]);
+                map.prefetch(p[17]);
+            }
             uint32_t u = p[0], v = p[1];
             if (u == v) continue;  // MultilayerGraph.cpp:126
             uint32_t a = map.get(u), b = map.get(v);
@@ -296,7 +303,13 @@ fc_status load_dir(const std::string& dir, int order, bool write_vtx_map, fc_gra
     for (uint32_t l = 0; l < L; l++) {
         auto& d = dir_pairs[l];
         d.reserve(raw[l].size() * 2);
-        for (size_t i = 0; i < raw[l].size(); i += 2) {
+        const size_t nr = raw[l].size();
+        for (size_t i = 0; i < nr; i += 2) {
+            // the table outgrows the caches: fetch the slots 16 ids ahead
+            if (i + 16 < nr) {
+                map.prefetch(raw[l][i + 16]);
+                map.prefetch(raw[l][i + 17]);
+            }
             uint32_t a = map.get(raw[l][i]), b = map.get(raw[l][i + 1]);
             d.push_back(a);
             d.push_back(b);
@@ -310,11 +323,23 @@ fc_status load_dir(const std::string& dir, int order, bool write_vtx_map, fc_gra
         FILE* f = fopen((dir + "__vtx_map.txt").c_str(), "wb");
         if (!f) return FC_ERR_IO;
         std::string out;
-        out.reserve(g->id2vtx.size() * 16);
+        out.reserve(g->id2vtx.size() * 22);
         char b[48];
+        // decimal digits of x, written backwards from e; returns the start
+        auto digits = [](uint64_t x, char* e) {
+            do {
+                *--e = (char)('0' + x % 10);
+                x /= 10;
+            } while (x);
+            return e;
+        };
         for (size_t i = 0; i < g->id2vtx.size(); i++) {
-            int k = snprintf(b, sizeof(b), "%u %zu\n", (unsigned)g->id2vtx[i], i);
-            out.append(b, (size_t)k);
+            char* e = b + sizeof(b);
+            *--e = '\n';
+            e = digits(i, e);
+            *--e = ' ';
+            e = digits((uint32_t)g->id2vtx[i], e);
+            out.append(e, (size_t)(b + sizeof(b) - e));
         }
         bool ok = fwrite(out.data(), 1, out.size(), f) == out.size();
         ok = (fclose(f) == 0) && ok;
