@@ -173,9 +173,30 @@ void parse_pairs(const std::vector<char>& text, std::vector<uint32_t>& out) {
 // dropped (Graph.cpp:27-47).  Counting sort by source, then each row sorted.
 // C: the count type, 32-bit when the layer's entries fit (half the bytes of
 // the two randomly written count arrays)
+// f(lo, hi) over node ranges [lo, hi) of about equal entry counts (by the
+// row prefix `cnt`), on `threads` host threads.
+template <class C, class F>
+void for_node_ranges(uint32_t n, const std::vector<C>& cnt, unsigned threads, F f) {
+    if (threads <= 1 || n < 4096) {
+        f(0u, n);
+        return;
+    }
+    const uint64_t total = cnt[n];
+    std::vector<uint32_t> cut(threads + 1, n);
+    cut[0] = 0;
+    for (unsigned t = 1; t < threads; t++) {
+        const uint64_t want = total * t / threads;  // first row starting at or after it
+        cut[t] = (uint32_t)(std::lower_bound(cnt.begin(), cnt.begin() + n, (C)want) - cnt.begin());
+        if (cut[t] < cut[t - 1]) cut[t] = cut[t - 1];
+    }
+    std::vector<std::thread> th;
+    for (unsigned t = 0; t < threads; t++) th.emplace_back([&, t] { f(cut[t], cut[t + 1]); });
+    for (auto& x : th) x.join();
+}
+
 template <class C>
 void build_layer_t(uint32_t n, const std::vector<uint32_t>& dir_pairs, std::vector<uint64_t>& off,
-                   std::vector<uint32_t>& adj) {
+                   std::vector<uint32_t>& adj, unsigned threads) {
     uint64_t m = dir_pairs.size() / 2;
     std::vector<C> cnt((size_t)n + 1, 0);
     for (uint64_t i = 0; i < m; i++) cnt[dir_pairs[2 * i] + 1]++;
@@ -183,24 +204,35 @@ void build_layer_t(uint32_t n, const std::vector<uint32_t>& dir_pairs, std::vect
     std::vector<uint32_t> tgt(m);
     std::vector<C> pos(cnt.begin(), cnt.end() - 1);
     for (uint64_t i = 0; i < m; i++) tgt[pos[dir_pairs[2 * i]]++] = dir_pairs[2 * i + 1];
+    std::vector<C>().swap(pos);
+    // each row sorted in place with its distinct neighbours moved to its
+    // front (the reference's sort + dedupe, Graph.cpp:17-50), then the
+    // distinct ones copied out: both passes over node ranges in parallel
+    std::vector<uint32_t> uniq(n);
+    for_node_ranges(n, cnt, threads, [&](uint32_t lo, uint32_t hi) {
+        for (uint32_t v = lo; v < hi; v++) {
+            uint32_t* b = tgt.data() + cnt[v];
+            uint32_t* e = tgt.data() + cnt[v + 1];
+            std::sort(b, e);
+            uint32_t* w = b;
+            for (uint32_t* q = b; q < e; q++)
+                if (q == b || *q != q[-1]) *w++ = *q;
+            uniq[v] = (uint32_t)(w - b);
+        }
+    });
     off.assign((size_t)n + 1, 0);
-    adj.clear();
-    adj.reserve(m);
-    for (uint32_t v = 0; v < n; v++) {
-        off[v] = adj.size();
-        uint32_t* b = tgt.data() + cnt[v];
-        uint32_t* e = tgt.data() + cnt[v + 1];
-        std::sort(b, e);
-        for (uint32_t* q = b; q < e; q++)
-            if (q == b || *q != q[-1]) adj.push_back(*q);
-    }
-    off[n] = adj.size();
+    for (uint32_t v = 0; v < n; v++) off[v + 1] = off[v] + uniq[v];
+    adj.resize(off[n]);
+    for_node_ranges(n, cnt, threads, [&](uint32_t lo, uint32_t hi) {
+        for (uint32_t v = lo; v < hi; v++)
+            if (uniq[v]) memcpy(adj.data() + off[v], tgt.data() + cnt[v], uniq[v] * 4ull);
+    });
 }
 
 void build_layer(uint32_t n, const std::vector<uint32_t>& dir_pairs, std::vector<uint64_t>& off,
-                 std::vector<uint32_t>& adj) {
-    if (dir_pairs.size() / 2 < (1ull << 32)) build_layer_t<uint32_t>(n, dir_pairs, off, adj);
-    else build_layer_t<uint64_t>(n, dir_pairs, off, adj);
+                 std::vector<uint32_t>& adj, unsigned threads) {
+    if (dir_pairs.size() / 2 < (1ull << 32)) build_layer_t<uint32_t>(n, dir_pairs, off, adj, threads);
+    else build_layer_t<uint64_t>(n, dir_pairs, off, adj, threads);
 }
 
 // f(l) for every layer l, on up to one host thread per core (layers are
@@ -229,8 +261,11 @@ fc_status finish(uint32_t n, uint32_t L, std::vector<std::vector<uint32_t>>& dir
     for (uint32_t i = 0; i < L; i++) g->order[i] = i;
     std::vector<std::vector<uint64_t>> offs(L);
     std::vector<std::vector<uint32_t>> adjs(L);
+    // layers in parallel; the cores beyond L help inside each layer
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned per_layer = L && hw > L ? hw / L : 1u;
     for_each_layer(L, [&](uint32_t l) {
-        build_layer(n, dir_pairs[l], offs[l], adjs[l]);
+        build_layer(n, dir_pairs[l], offs[l], adjs[l], per_layer);
         std::vector<uint32_t>().swap(dir_pairs[l]);
     });
     std::vector<uint64_t> base(L + 1, 0);

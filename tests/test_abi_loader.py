@@ -60,6 +60,17 @@ def test_loader_from_pairs_matches_reference(name):
     assert np.array_equal(off, o_off) and np.array_equal(adj, o_adj)
 
 
+def test_csr_build_split_over_threads_matches_oracle():
+    """Few layers and many nodes: each layer's rows are sorted and deduplicated
+    on several host threads (node ranges of equal entry counts); the CSR must
+    still equal the oracle's, duplicates and self loops included."""
+    gen = synth.chung_lu_graph(30000, 2, 120000, 2.1, 0.4, 97, dirty=True)
+    g = MultilayerGraph.from_pairs(gen.layers)
+    off, adj = g.csr()
+    o_off, o_adj = O.OracleGraph(gen.layers).csr()
+    assert np.array_equal(off, o_off) and np.array_equal(adj, o_adj)
+
+
 def _write_texts(d, texts):
     with open(os.path.join(d, "mlg.conf"), "w") as f:
         f.write("".join(f"l{i}.txt\n" for i in range(len(texts))))
