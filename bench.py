@@ -10,16 +10,27 @@ its adjacency, so a full fcgrid is L * 2M edge visits (M = undirected edges
 summed over layers).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload c1|c2|c3|c4|c5] [--split lambda|replicas]
 
 `value` is device-timed with CUDA events on the launching stream (graph
 resident in HBM); `e2e` is the same step through the public API from pinned
-host memory, with the upload and the table read-back inside the timed region.
-Under torchrun every rank runs its own copy of the workload (no collective
-in the data path; weak scaling) and rank 0 prints the max-over-ranks time.
+host memory, with the upload and the table read-back inside the timed region,
+and its phases timed with CUDA events between the calls.  Under torchrun the
+single-graph workloads split the graph's lambda columns over the ranks
+(`--split lambda`, the default; no collective in the data path, the cells
+are gathered once at the end and folded) or run a replica per rank
+(`--split replicas`); the 256-graph mix splits its graphs by work.  Rank 0
+prints the max-over-ranks time.
+
+The CPU baseline follows one protocol: the reference's table methods
+(ParGrid, ParGridPlus, ParCoreIndex) and WdsList, compiled from its sources,
+each run as shipped and with OMP_THREAD_LIMIT = the host's cores; the fastest
+table method plus the fastest WdsList is the reference's time for a step.
 """
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import statistics
@@ -37,6 +48,8 @@ sys.path.insert(0, ROOT)
 METRIC = "fcgrid time & edge-visits/s, batched vs plain GPU (bit-exact), vs ParGrid CPU"
 UNIT = "edge-visits/s"
 L2_BYTES = 126 * 1024 * 1024
+TABLE_METHODS = ("ParGrid", "ParGridPlus", "ParCoreIndex")
+SETTINGS = ("as_shipped", "thread_limit")
 
 
 def parse_args():
@@ -46,20 +59,27 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c3", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--split", default="lambda", choices=["lambda", "replicas"],
+                    help="single-graph workloads under torchrun: lambda columns over ranks, "
+                         "or one replica per rank")
     ap.add_argument("--batch-count", type=int, default=256)
     ap.add_argument("--block-threads", type=int, default=0,
                     help="c4: fixed peel launch shape (0 = autotuned)")
     ap.add_argument("--hub-threshold", type=int, default=0,
                     help="c4: fixed longest row queued as one item (0 = autotuned)")
     ap.add_argument("--no-plain", action="store_true",
-                    help="c4: skip the plain form and the table comparison (profiling)")
+                    help="c4: skip the plain forms and the table comparison (profiling)")
     ap.add_argument("--rates", default="25,50,100,200",
                     help="c5: arrival rates (requests/s) of the sweep")
     ap.add_argument("--requests", type=int, default=150, help="c5: requests per rate")
     ap.add_argument("--pool", type=int, default=64, help="c5: distinct small graphs")
     ap.add_argument("--beta", type=float, default=1.0)
+    ap.add_argument("--ref-reps", type=int, default=0,
+                    help="runs of each reference method in the protocol (0: 3 for the "
+                         "reference arm, 1 for our arm's cpu_baseline)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-probe", action="store_true", help="skip the atomic-throughput probe")
     return ap.parse_args()
 
 
@@ -71,6 +91,18 @@ def describe(name):
                 f" copy={c['copy']} seed={c['seed']}; full fcgrid + densest(beta)")
     return (f"{name}: Erdos-Renyi n={c['n']} L={c['L']} p~U[{c['p_lo']},{c['p_hi']}] "
             f"seed={c['seed']}; full fcgrid + densest(beta)")
+
+
+def config_dict(args, n, L, m2, world):
+    """The workload, identical in both arms' lines."""
+    split = ("single process" if world == 1 else
+             f"lambda columns split over {world} ranks" if args.split == "lambda" else
+             f"{world} replicas")
+    return {"workload": describe(args.workload), "n": n, "L": L, "directed_entries": m2,
+            "edge_visits_per_step": L * m2, "beta": args.beta,
+            "l2": (f"inputs larger than L2 (adjacency {m2 * 4 / 2**20:.0f} MiB > 126 MiB)"
+                   if m2 * 4 > L2_BYTES else "inputs smaller than L2 (no flush)"),
+            "parallelism": split}
 
 
 def dist_setup(init=True):
@@ -160,67 +192,145 @@ def committed_traffic(workload):
     return None, None
 
 
-def cpu_baseline(layers, L, visits, beta, steps=1, warmup=0):
-    """The reference's own ParGrid + WdsList (compiled from its sources into
-    oracle/_ref) on this host's cores, on the same graph."""
-    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
-    if not os.path.exists(harness):
-        return None, "oracle/_ref/ref_harness not built"
+def bytes_per_column(n, L, m2):
+    """Algorithmic bytes of one lambda column: 4*2M adjacency slots + 4*L*(n+1)
+    offsets + 2*4*L*n degree table (written once, read once) + 4*n core output."""
+    return 4 * m2 + 4 * L * (n + 1) + 8 * L * n + 4 * n
+
+
+# ---- the reference on the host cores ------------------------------------------
+
+def _harness():
+    h = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    return h if os.path.exists(h) else None
+
+
+def _run_harness(fcg, steps, warmup, beta, cores, methods, setting, timeout=3000):
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+    env.pop("OMP_THREAD_LIMIT", None)
+    if setting == "thread_limit":
+        env["OMP_THREAD_LIMIT"] = str(cores)
+    r = subprocess.run([_harness(), fcg, "bench", str(steps), str(warmup), repr(beta), str(cores),
+                        ",".join(methods)], capture_output=True, text=True, env=env,
+                       timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr.strip()[-300:])
+    runs = [json.loads(x[5:]) for x in r.stdout.splitlines() if x.startswith("STEP ")]
+    return [x for x in runs if not x["warmup"]]
+
+
+def ref_protocol(fcg, beta, reps, cores, methods=TABLE_METHODS):
+    """Every listed table method and WdsList, `reps` runs each, as shipped
+    and with OMP_THREAD_LIMIT = cores.  Returns the per-(setting, method)
+    median seconds, the fastest table method with its setting, and the
+    fastest WdsList."""
+    med = {}
+    densest = None
+    for setting in SETTINGS:
+        runs = _run_harness(fcg, reps, 0, beta, cores, list(methods) + ["WdsList"], setting)
+        med[setting] = {m: statistics.median(x[m] for x in runs) for m in list(methods) +
+                        ["WdsList"]}
+        densest = {k: runs[-1][k] for k in ("density", "k", "lmd", "len")}
+    best = min(((med[s][m], s, m) for s in SETTINGS for m in methods))
+    wds = min(((med[s]["WdsList"], s) for s in SETTINGS))
+    return {"median_s": med, "table_s": best[0], "table_setting": best[1], "table_method": best[2],
+            "wdslist_s": wds[0], "wdslist_setting": wds[1], "reps": reps, "cores": cores,
+            "densest": densest}
+
+
+def _graph_fcg(layers, d):
     from pargridcpu_b200 import synth
+    fcg = os.path.join(d, "g.fcg")
+    synth.write_fcg(synth.Graph(layers), fcg)
+    return fcg
+
+
+def cpu_baseline(layers, visits, beta, reps):
+    """The protocol on this host's cores for our arm's line (a bounded
+    sample: `reps` runs of each method)."""
+    if not _harness():
+        return None, "oracle/_ref/ref_harness not built"
     cores = os.cpu_count() or 1
     with tempfile.TemporaryDirectory() as d:
-        fcg = os.path.join(d, "g.fcg")
-        synth.write_fcg(synth.Graph(layers), fcg)
-        env = dict(os.environ, OMP_NUM_THREADS=str(cores))
-        r = subprocess.run([harness, fcg, "bench", str(steps), str(warmup), repr(beta), str(cores)],
-                           capture_output=True, text=True, env=env, timeout=3000)
-    if r.returncode != 0:
-        return None, r.stderr.strip()[-300:]
-    runs = [json.loads(x[5:]) for x in r.stdout.splitlines() if x.startswith("STEP ")]
-    timed = [x for x in runs if not x["warmup"]] or runs
-    secs = [x["pargrid_s"] + x["wdslist_s"] for x in timed]
-    mean = sum(secs) / len(secs)
-    return {"value": visits / mean, "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": f"{len(timed)} run(s) of the reference ParGrid (full fcgrid) + WdsList "
-                      f"(beta={beta}) on the same graph, OpenMP threads={cores}; its own "
-                      f"timers (load excluded)",
-            "pargrid_s": statistics.mean(x["pargrid_s"] for x in timed),
-            "wdslist_s": statistics.mean(x["wdslist_s"] for x in timed),
-            "densest": {k: timed[-1][k] for k in ("density", "k", "lmd", "len")}}, None
+        try:
+            p = ref_protocol(_graph_fcg(layers, d), beta, reps, cores)
+        except Exception as e:  # noqa: BLE001
+            return None, str(e)
+    step_s = p["table_s"] + p["wdslist_s"]
+    return {"value": visits / step_s, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": (f"{reps} run(s) each of the reference's ParGrid, ParGridPlus, ParCoreIndex "
+                       f"and WdsList (beta={beta}) on the same graph, as shipped and with "
+                       f"OMP_THREAD_LIMIT={cores}, OpenMP threads={cores}, their own timers "
+                       f"(load excluded); step = fastest table method ({p['table_method']}, "
+                       f"{p['table_setting']}) + fastest WdsList ({p['wdslist_setting']})"),
+            "protocol": p}, None
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
     from pargridcpu_b200 import synth
+    if args.workload == "c4":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "the 256-graph mix's reference time is reported as the c4 line's "
+                          "cpu_baseline (a per-graph sample), not as a separate arm"}))
+        return
+    if not _harness():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness not built"}))
+        return
     g = synth.config_graph(args.workload)
-    import oracle as O  # noqa: F401  (the checker package, for the loader restatement)
+    import oracle as O  # the checker package: the loader restatement gives n and M
     og = O.OracleGraph(g.layers)
-    L = og.L
+    L, n = og.L, og.n
     m2 = int(og.layer_m().sum())
     visits = L * m2
-    base, err = cpu_baseline(g.layers, L, visits, args.beta, steps=args.steps, warmup=args.warmup)
-    if base is None:
-        print(json.dumps({"impl": "reference", "unavailable": err}))
-        return
-    secs = visits / base["value"]
-    line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT,
+    cores = os.cpu_count() or 1
+    reps = args.ref_reps or 3
+    with tempfile.TemporaryDirectory() as d:
+        fcg = _graph_fcg(g.layers, d)
+        p = ref_protocol(fcg, args.beta, reps, cores)
+        # the timed steps: the fastest table method (in its setting) + WdsList
+        runs = _run_harness(fcg, args.steps, args.warmup, args.beta, cores,
+                            [p["table_method"], "WdsList"], p["table_setting"])
+    secs = statistics.mean(x[p["table_method"]] + x["WdsList"] for x in runs)
+    value = visits / secs
+    sample = (f"{args.steps} timed step(s) after {args.warmup} warm-up of the reference's fastest "
+              f"table method ({p['table_method']}, {p['table_setting']}) + WdsList "
+              f"(beta={args.beta}) on the same graph, OpenMP threads={cores}, its own timers "
+              f"(load excluded); fastest chosen by the protocol ({reps} runs each of ParGrid, "
+              f"ParGridPlus, ParCoreIndex, WdsList, as shipped and with OMP_THREAD_LIMIT={cores})")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": secs * 1e3, "higher_is_better": True, "scaling": "weak",
+            "ms_per_step": secs * 1e3, "higher_is_better": True,
+            "scaling": "strong" if world > 1 and args.split == "lambda" else "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": describe(args.workload), "n": og.n, "L": L,
-                       "directed_entries": m2, "beta": args.beta},
-            "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
-            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+            "config": config_dict(args, n, L, m2, world),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
-            "detail": {"pargrid_s": base["pargrid_s"], "wdslist_s": base["wdslist_s"],
-                       "densest": base["densest"]}}
+            "detail": {"protocol": p, "step_table_s": statistics.mean(x[p["table_method"]]
+                                                                       for x in runs),
+                       "step_wdslist_s": statistics.mean(x["WdsList"] for x in runs),
+                       "densest": {k: runs[-1][k] for k in ("density", "k", "lmd", "len")}}}
     print(json.dumps(line))
+
+
+# ---- our arm: one graph --------------------------------------------------------
+
+def atomic_probe(table_bytes):
+    """Returned-value atomic subtractions per second at random addresses of
+    a buffer the size of the peel's degree tables, and of one that fits L2."""
+    from pargridcpu_b200 import probe_atomics
+    fit = probe_atomics(64 << 20, 1 << 28)
+    same = probe_atomics(max(table_bytes, 4096), 1 << 28)
+    return {"l2_resident_gatomics_per_s": fit, "table_sized_gatomics_per_s": same,
+            "table_sized_bytes": int(table_bytes)}
 
 
 def run_ours(args, world, rank, local):
     import torch
-    from pargridcpu_b200 import MultilayerGraph, launch_count, synth
+    from pargridcpu_b200 import MultilayerGraph, launch_count, shard, synth
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
@@ -231,9 +341,14 @@ def run_ours(args, world, rank, local):
     visits = L * m2
     stream = torch.cuda.Stream(device=dev)
     beta = [args.beta]
+    split = world > 1 and args.split == "lambda"
+    lo, hi = shard.column_ranges(L, world)[rank] if split else (1, L + 1)
+    my_cols = hi - lo
 
     def step():
         g.reset_results()
+        if split:
+            return g.cells_range(lo, hi, args.beta, stream=stream) if my_cols else []
         g.coreindex(stream=stream, copy=False)
         return g.densest(beta, stream=stream)[0]
 
@@ -243,9 +358,20 @@ def run_ours(args, world, rank, local):
             import torch.distributed as dist
             dist.barrier()
 
+    def max_over_ranks(x):
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([x], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            x = float(t.item())
+        return x
+
     g.upload(stream=stream)
     for _ in range(args.warmup):
         step()
+    probe = None
+    if not args.no_probe and rank == 0:
+        probe = atomic_probe(4 * n * L * min(L, max(my_cols, 1)))
     clocks = Clocks(local)
     barrier()
     clocks.start()
@@ -266,112 +392,200 @@ def run_ours(args, world, rank, local):
     barrier()
     launches = launch_count() - l0
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
     ms_per_step = ms / args.steps
-    value = world * visits * args.steps / (ms / 1e3)
+    # lambda split: the ranks together do one graph's visits per step;
+    # replicas: every rank does all of them
+    total_visits = visits if split else world * visits
+    value = total_visits * args.steps / (ms / 1e3)
     stats = g.stats()
+    if split:
+        # one exchange at the end: every rank's cells, folded in the
+        # reference's order on every rank
+        res = shard.gather_cells(res) if world > 1 else shard.merge_cells([res])
 
-    # e2e: through the public API from pinned host memory, upload + read-back inside
+    # e2e: through the public API from pinned host memory, upload + read-back
+    # inside, phases timed with CUDA events between the calls
     e2e = None
     if not args.no_e2e:
-        out_t = torch.empty((L, n), dtype=torch.int32, pin_memory=True)
+        out_t = torch.empty((max(my_cols, 1), n), dtype=torch.int32, pin_memory=True)
         out = out_t.numpy().view(np.uint32)
         h2d = L * (n + 1) * 8 + m2 * 4
-        d2h = L * n * 4 + 48
+        d2h = my_cols * n * 4 + 48
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+        phases = {"upload": [], "peel": [], "table_d2h": [], "densest": []}
 
-        def e2e_step():
+        def e2e_step(record):
             g.release_device()
+            if record:
+                evs[0].record(stream)
             g.upload(stream=stream)
-            g.coreindex(out=out, stream=stream)
-            return g.densest(beta, stream=stream)[0]
+            if record:
+                evs[1].record(stream)
+            if split:
+                if my_cols:
+                    g.coreindex_range(lo, hi, stream=stream, copy=False)
+                    if record:
+                        evs[2].record(stream)
+                    g.coreindex_range(lo, hi, out=out, stream=stream)
+                    if record:
+                        evs[3].record(stream)
+                    r = g.cells_range(lo, hi, args.beta, stream=stream)
+                else:
+                    r = []
+                    if record:
+                        evs[2].record(stream)
+                        evs[3].record(stream)
+            else:
+                g.coreindex(stream=stream, copy=False)
+                if record:
+                    evs[2].record(stream)
+                g.coreindex(out=out, stream=stream)
+                if record:
+                    evs[3].record(stream)
+                r = g.densest(beta, stream=stream)[0]
+            if record:
+                evs[4].record(stream)
+                torch.cuda.synchronize()
+                for i, k in enumerate(("upload", "peel", "table_d2h", "densest")):
+                    phases[k].append(evs[i].elapsed_time(evs[i + 1]))
+            return r
 
         for _ in range(max(1, min(args.warmup, 2))):
-            e2e_step()
+            e2e_step(False)
         barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):
-            e2e_step()
+            e2e_step(False)
         e1.record(stream)
         barrier()
-        ems = e0.elapsed_time(e1)
-        if world > 1:
-            import torch.distributed as dist
-            t = torch.tensor([ems], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
-        e2e = {"value": world * visits * args.steps / (ems / 1e3), "unit": UNIT,
+        ems = max_over_ranks(e0.elapsed_time(e1))
+        for _ in range(2):  # the phases, on separate steps (their syncs stay out of the total)
+            e2e_step(True)
+        barrier()
+        e2e = {"value": total_visits * args.steps / (ems / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "ms_per_step": ems / args.steps}
+               "ms_per_step": ems / args.steps,
+               "phases_ms": {k: statistics.mean(v) for k, v in phases.items()}}
 
     if rank != 0:
         return
     # roofline of the dominant stage (the peel: k_peel and, when it stops
     # early, the endgame kernels that finish the columns): algorithmic bytes
-    # per peel group (per lambda column: 4*2M adjacency + 4*L*(n+1) offsets +
-    # 2*4*L*n degree table + 4*n core output) over the mean CUDA-event time
-    cols = stats["columns_per_launch"] or L
-    per_col = 4 * m2 + 4 * L * (n + 1) + 8 * L * n + 4 * n
-    bytes_per_launch = cols * per_col
+    # per launch (bytes_per_column per lambda column) over the mean CUDA-event
+    # time of a launch
+    cols = min(stats["columns_per_launch"] or L, max(my_cols, 1))
+    bytes_per_launch = cols * bytes_per_column(n, L, m2)
     launch_ms = statistics.mean(p / max(1, q) for p, q in zip(peel_ms, peel_launches))
     achieved = bytes_per_launch / (launch_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
     traffic, atom_sectors = committed_traffic(args.workload)
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic,
+            "kernel": "k_peel + endgame (k_eg_index, k_eg_scan, k_eg_fill, k_eg_fill_big, "
+                      "k_endgame)", "peak_kind": peak_kind,
+            "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms,
+            # atomics are reported beside the bytes, not folded in
+            "l2_atomic_sectors_per_launch": atom_sectors,
+            "l2_atomic_gsectors_per_s": (atom_sectors / (launch_ms / 1e3) / 1e9
+                                         if atom_sectors else None)}
+    if probe:
+        roof["atomic_probe"] = probe
+        if atom_sectors:
+            rate = roof["l2_atomic_gsectors_per_s"]
+            roof["l2_atomic_frac"] = rate / probe["table_sized_gatomics_per_s"]
+            roof["l2_atomic_frac_vs_l2_resident"] = rate / probe["l2_resident_gatomics_per_s"]
+    densest = ({k: res[k] for k in ("k", "lmd", "length", "lstar", "density", "max_density_f")}
+               if res else None)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "higher_is_better": True, "scaling": "strong" if split else "weak",
+            "vs_baseline": None, "dtype": "u32",
             "data": "synthetic (seeded; shapes of the named configuration)",
-            "config": {"workload": describe(args.workload), "n": n, "L": L,
-                       "directed_entries": m2, "edge_visits_per_step": visits,
-                       "beta": args.beta,
-                       "l2": f"inputs larger than L2 (adjacency {m2 * 4 / 2**20:.0f} MiB > 126 MiB)"
-                       if m2 * 4 > L2_BYTES else "inputs smaller than L2 (no flush)",
-                       "parallelism": "replicas" if world > 1 else "single GPU"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "k_peel + endgame (k_eg_index, k_eg_scan, k_eg_fill, "
-                                   "k_eg_fill_big, k_endgame)", "peak_kind": peak_kind,
-                         "bytes_per_launch": bytes_per_launch, "launch_ms": launch_ms,
-                         # atomics are reported beside the bytes, not folded in
-                         "l2_atomic_sectors_per_launch": atom_sectors,
-                         "l2_atomic_gsectors_per_s": (atom_sectors / (launch_ms / 1e3) / 1e9
-                                                      if atom_sectors else None)},
-            "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+            "config": config_dict(args, n, L, m2, world),
+            "roofline": roof, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
             "detail": {"peel_ms_per_step": statistics.mean(peel_ms),
                        "densest_ms_per_step": statistics.mean(dens_ms),
                        "levels": stats["levels"], "subrounds": stats["subrounds"],
                        "peel_phase_ms": dict(zip(("scan", "expand", "recompute"),
                                                  stats["phase_ms"])),
-                       "densest": {k: res[k] for k in ("k", "lmd", "length", "lstar", "density",
-                                                       "max_density_f")}}}
+                       "columns_rank0": [lo, hi],
+                       "densest": densest}}
     if world == 1 and not args.no_cpu_baseline:
-        base, err = cpu_baseline(gen.layers, L, visits, args.beta)
+        base, err = cpu_baseline(gen.layers, visits, args.beta, args.ref_reps or 1)
         if base is not None:
             line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind",
                                                          "sample")}
-            line["detail"]["cpu_baseline_s"] = {"pargrid_s": base["pargrid_s"],
-                                                "wdslist_s": base["wdslist_s"]}
+            line["detail"]["cpu_protocol"] = base["protocol"]
         else:
             line["cpu_baseline"] = None
             line["detail"]["cpu_baseline_error"] = err
     print(json.dumps(line))
 
 
+# ---- our arm: the 256-graph mix ------------------------------------------------
+
+def _table_sha(t):
+    return hashlib.sha256(np.ascontiguousarray(t, dtype=np.uint32).tobytes()).hexdigest()
+
+
+def c4_reference_check(graphs, tables, results, count):
+    """Every graph's table and densest result against the reference's own
+    (tests/golden/c4_mix.json, the full seed-404 mix); None when the fixture
+    does not cover this run."""
+    p = os.path.join(ROOT, "tests", "golden", "c4_mix.json")
+    if not os.path.exists(p) or count != 256:
+        return None
+    fx = json.load(open(p))["graphs"]
+    bad = []
+    for i, (g, t, r, f) in enumerate(zip(graphs, tables, results, fx)):
+        ok = (g.n == f["n"] and g.L == f["L"] and _table_sha(t) == f["table_sha256"] and
+              (r["k"], r["lmd"], r["length"]) == (f["k"], f["lmd"], f["length"]) and
+              np.float32(r["max_density_f"]) == np.float32(f["max_density_f"]) and
+              (r["k"] == 0 or r["density"] == f["density"]))
+        if not ok:
+            bad.append(i)
+    return {"graphs": len(fx), "identical": not bad, "mismatched": bad[:16]}
+
+
+def c4_cpu_sample(gens, beta, every=16):
+    """The reference (fastest table method as the protocol found it on c3:
+    ParGrid with OMP_THREAD_LIMIT) + WdsList on every `every`-th graph of
+    the mix, one run each; edge-visits/s of the sample."""
+    if not _harness():
+        return None, "oracle/_ref/ref_harness not built"
+    import oracle as O
+    cores = os.cpu_count() or 1
+    secs, visits, n_s = 0.0, 0, 0
+    with tempfile.TemporaryDirectory() as d:
+        for i in range(0, len(gens), every):
+            og = O.OracleGraph(gens[i].layers)
+            visits += og.L * int(og.layer_m().sum())
+            fcg = _graph_fcg(gens[i].layers, d)
+            runs = _run_harness(fcg, 1, 0, beta, cores, ["ParGrid", "WdsList"], "thread_limit")
+            secs += runs[0]["ParGrid"] + runs[0]["WdsList"]
+            n_s += 1
+    return {"value": visits / secs, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": (f"{n_s} graphs of the mix (every {every}th), one run each of the "
+                       f"reference's ParGrid + WdsList (beta={beta}) with OMP_THREAD_LIMIT="
+                       f"{cores}, OpenMP threads={cores}, their own timers (load excluded); "
+                       f"{visits} edge visits in {secs:.2f} s")}, None
+
+
 def run_batch(args, world, rank, local):
     """The 256-graph mix: every (graph, lambda) column in one persistent launch
-    (batched form) against one graph and one column per launch (plain form),
-    same graphs, tables compared.  Under torchrun each rank takes the graphs
-    the work-balanced assignment gives it (no collective in the data path)."""
+    (batched form) against two plain forms on the same resident graphs -- one
+    graph per call of the library's single-graph path (fc_coreindex +
+    fc_densest, 256 calls) and one graph and one lambda column per launch --
+    with every table and densest result compared, and against the reference's
+    own results for the mix.  Under torchrun each rank takes the graphs the
+    work-balanced assignment gives it (no collective in the data path)."""
     import multiprocessing as mp
     import torch
     from concurrent.futures import ProcessPoolExecutor, ThreadPoolExecutor
-    from pargridcpu_b200 import MultilayerGraph, batch_run, shard, synth
+    from pargridcpu_b200 import MultilayerGraph, batch_run, launch_count, shard, synth
 
     torch.cuda.set_device(local)
     t0 = time.time()
@@ -384,51 +598,100 @@ def run_batch(args, world, rank, local):
         gens = list(ex.map(synth._make, mine, chunksize=1))
     with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
         graphs = list(ex.map(lambda g: MultilayerGraph.from_pairs(g.layers), gens))
-    del gens
     gen_s = time.time() - t0
     for g in graphs:
         g.upload()
-    visits = sum(int(g.layer_m().sum()) * g.L for g in graphs)
+    sizes = [(g.n, g.L, int(g.layer_m().sum())) for g in graphs]
+    visits = sum(L * m2 for n, L, m2 in sizes)
+    bytes_step = sum(L * bytes_per_column(n, L, m2) for n, L, m2 in sizes)
     stream = torch.cuda.Stream()
 
-    def timed(**kw):
+    def timed(fn):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        tables, res, rep = batch_run(graphs, beta=args.beta, want_tables=False, stream=stream, **kw)
+        out = fn()
         e1.record(stream)
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1), res, rep
+        return e0.elapsed_time(e1), out
 
     shape = dict(block_threads=args.block_threads, hub_threshold=args.hub_threshold)
-    timed(**shape)  # autotunes (unless the shape is fixed) and warms up
+
+    def batched(want_tables=False):
+        return batch_run(graphs, beta=args.beta, want_tables=want_tables, stream=stream, **shape)
+
+    timed(batched)  # autotunes (unless the shape is fixed) and warms up
     for _ in range(max(0, args.warmup - 1)):
-        timed(**shape)
+        timed(batched)
     clocks = Clocks(local)
     clocks.start()
-    batched = [timed(**shape) for _ in range(args.steps)]
+    l0 = launch_count()
+    runs = [timed(batched) for _ in range(args.steps)]
+    launches = launch_count() - l0
     clk = clocks.stop()
-    b_ms = statistics.mean(b[0] for b in batched)
-    if args.no_plain:
-        plain_ms, plain_rep, same = float("nan"), None, None
-    else:
-        plain_ms, plain_res, plain_rep = timed(plain=True)
-        same = all(a == b for a, b in zip(batched[-1][1], plain_res))
-        tb, _, _ = batch_run(graphs, beta=args.beta, **shape)
-        tp, _, _ = batch_run(graphs, beta=args.beta, plain=True)
-        same = same and all(np.array_equal(a, b) for a, b in zip(tb, tp))
+    b_ms = statistics.mean(r[0] for r in runs)
+    rep = runs[-1][1][2]
+    res_b = runs[-1][1][1]
+
+    def per_graph():
+        out = []
+        for g in graphs:
+            g.reset_results()
+            g.coreindex(stream=stream, copy=False)
+            out.append(g.densest([args.beta], stream=stream)[0])
+        return out
+
+    plain_graph_ms = plain_col_ms = None
+    same = ref_check = None
+    plain_rep = None
+    if not args.no_plain:
+        tb, res_t, _ = batched(want_tables=True)
+        per_graph()  # warm
+        plain_graph_ms, res_g = timed(per_graph)
+        tg = [g.coreindex() for g in graphs]  # the per-graph form's tables (resident)
+        plain_col_ms, (_, res_c, plain_rep) = timed(
+            lambda: batch_run(graphs, beta=args.beta, want_tables=False, plain=True, stream=stream))
+        tp = [g.coreindex() for g in graphs]  # the per-column form's tables (resident)
+        same = (all(np.array_equal(a, b) and np.array_equal(a, c) for a, b, c in zip(tb, tg, tp))
+                and res_t == res_b and res_b == res_c and
+                all((a["k"], a["lmd"], a["length"], a["lstar"], a["density"]) ==
+                    (b["k"], b["lmd"], b["length"], b["lstar"], b["density"])
+                    for a, b in zip(res_b, res_g)))
+        if world == 1:
+            ref_check = c4_reference_check(graphs, tb, res_t, args.batch_count)
+
+    # e2e: the batched form through the public API from host buffers: every
+    # graph's device copy released, uploaded again and its table read back
+    e2e = None
+    if not args.no_e2e:
+        h2d = sum(L * (n + 1) * 8 + m2 * 4 for n, L, m2 in sizes)
+        d2h = sum(L * n * 4 + 48 for n, L, m2 in sizes)
+
+        def e2e_step():
+            for g in graphs:
+                g.release_device()
+            return batched(want_tables=True)
+
+        e2e_step()
+        e_ms = statistics.mean(timed(e2e_step)[0] for _ in range(max(1, min(args.steps, 3))))
+        e2e = {"value": visits / (e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": e_ms}
     ms = b_ms
     if world > 1:
         import torch.distributed as dist
-        t = torch.tensor([b_ms, plain_ms], device="cuda")
+        t = torch.tensor([b_ms, plain_graph_ms or 0.0, plain_col_ms or 0.0], device="cuda",
+                         dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, plain_ms = float(t[0]), float(t[1])
-        v = torch.tensor([float(visits)], device="cuda", dtype=torch.float64)
+        ms, plain_graph_ms, plain_col_ms = float(t[0]), float(t[1]), float(t[2])
+        v = torch.tensor([float(visits), float(bytes_step)], device="cuda", dtype=torch.float64)
         dist.all_reduce(v)
-        visits = int(v.item())
+        visits, bytes_step = int(v[0].item()), int(v[1].item())
     if rank != 0:
         return
-    rep = batched[-1][2]
+    peak, peak_kind = peaks()
+    peel_ms = rep["peel_ms"] / max(1, rep["peel_launches"])
+    bytes_launch = bytes_step / max(1, rep["peel_launches"])
+    achieved = bytes_launch / (peel_ms / 1e3) / 1e9
     line = {"metric": METRIC, "value": visits / (ms / 1e3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
@@ -438,14 +701,31 @@ def run_batch(args, world, rank, local):
                                    "[2,32], gamma U[2,3], copy U[0,0.6], seed 404; full fcgrid "
                                    "+ densest(beta) per graph",
                        "graphs": len(graphs), "edge_visits_per_step": visits, "beta": args.beta,
+                       "l2": "inputs larger than L2 (the mix's adjacency is ~5 GB)",
                        "parallelism": ("graphs split over ranks by work (LPT)" if world > 1
-                                       else "single GPU")},
+                                       else "single process")},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "k_peel<1,T,true> (batched, all graphs' columns)",
+                         "peak_kind": peak_kind, "bytes_per_launch": bytes_launch,
+                         "launch_ms": peel_ms},
+            "e2e": e2e, "gpu_launches": launches, "clocks": clk,
             "batched": {"ms": ms, "report": rep},
-            "plain": {"ms": plain_ms, "report": plain_rep,
-                      "form": "one graph and one lambda column per launch, one after another"},
-            "speedup_batched_vs_plain": plain_ms / ms,
+            "plain_per_graph": {"ms": plain_graph_ms,
+                                "form": "one graph per call of the single-graph path "
+                                        "(fc_coreindex: all its columns in one launch with the "
+                                        "endgame, then fc_densest), graph after graph"},
+            "plain_per_column": {"ms": plain_col_ms, "report": plain_rep,
+                                 "form": "one graph and one lambda column per launch"},
+            "speedup_vs_plain_per_graph": (plain_graph_ms / ms) if plain_graph_ms else None,
+            "speedup_vs_plain_per_column": (plain_col_ms / ms) if plain_col_ms else None,
             "identical_results": None if same is None else bool(same),
-            "clocks": clk, "setup_s": gen_s}
+            "vs_reference": ref_check, "setup_s": gen_s}
+    if world == 1 and not args.no_cpu_baseline:
+        base, err = c4_cpu_sample(gens, args.beta)
+        line["cpu_baseline"] = base
+        if err:
+            line["cpu_baseline_error"] = err
     print(json.dumps(line))
 
 

@@ -182,6 +182,52 @@ fc_status fc_cell_members(fc_graph* g, uint32_t k, uint32_t lmd, uint32_t* nodes
 fc_status fc_cells(fc_graph* g, double beta, fc_cell* cells, uint32_t cap, uint32_t* count,
                    void* stream);
 
+/* ---- every cell at once --------------------------------------------------
+ * The compact form of all cells (the B200 counterpart of -m CoreMem /
+ * PathMem, main.cpp:331-362: FCSyncMem::constructCoreSync, CoreParallel/
+ * FCSyncMem.cpp:10-54, and FCPathMem::constructCore, Core/FCPathMem.cpp:9-59,
+ * which keep per cell the nodes it loses against its parent).  Cells of one
+ * column are nested, so one order per column holds every cell as a prefix:
+ *   order[(lambda-1)*n + i]  column lambda's nodes by descending core_lambda,
+ *                            ascending ids within one core value (L*n words);
+ *   col_off[lambda-1]        where column lambda's sizes start (L+1 words);
+ *   sizes[col_off[lambda-1] + k] = |C_{k,lambda}|, k = 0 .. kmax_lambda + 1
+ *                            (the last is 0).
+ * C_{k,lambda} is order[(lambda-1)*n .. (lambda-1)*n + sizes[col_off[lambda-1]
+ * + k]), and the nodes with core_lambda = k exactly are the block between the
+ * prefixes of k+1 and k.  *sizes_count receives the number of size words
+ * (col_off[L]); sizes receives min(sizes_cap, *sizes_count) of them.  Any
+ * output pointer may be NULL (call once with order = sizes = NULL to learn
+ * the size).  All outputs are host memory.  Runs fc_coreindex first when the
+ * table is not resident; the index stays resident with the table. */
+fc_status fc_cell_index(fc_graph* g, uint32_t* order, uint64_t* col_off, uint32_t* sizes,
+                        uint64_t sizes_cap, uint64_t* sizes_count, void* stream);
+
+/* Many cells at once: query q is the cell (ks[q], lmds[q]), lmds[q] in 1..L.
+ * The query lists of -m CoreIndexTimeOnline / CoreIndexTimeOffline
+ * (main.cpp:493-582): getResCore scans each query's column for the nodes
+ * with core >= k (Util/CoreIndexTime.h:8-40), getResCoreOffline takes them
+ * from a core-sorted copy by lower_bound (:43-59).  by_index = 0 answers the
+ * first way, each cell in ascending ids; by_index = 1 the second, each cell
+ * as its prefix of the fc_cell_index order (building the index first when it
+ * is not resident).  offsets (host, nq+1 words) receives the start of every
+ * query's nodes and the total; nodes (host) receives min(cap, total) ids.
+ * The reference's own loop loads only lambda = 1's core file, so its answers
+ * for other lambdas are empty; here every query is answered. */
+fc_status fc_cells_members(fc_graph* g, const uint32_t* ks, const uint32_t* lmds, uint32_t nq,
+                           int by_index, uint64_t* offsets, uint32_t* nodes, uint64_t cap,
+                           void* stream);
+
+/* The membership test of -m MLCDTime (checktime, Util/CheckMLCDTime.h:9-42,
+ * main.cpp:453-491) over per-node coreness vectors: cores (host) holds n rows
+ * of P values, node v's row at v*P.  Node v answers query (ks[q], lmds[q])
+ * when at least max(lmds[q], 1) of its P values are >= ks[q] (unsigned
+ * comparisons, as the reference's `uint k` against its values).  offsets and
+ * nodes as for fc_cells_members, ascending ids.  Needs no graph. */
+fc_status fc_mlcd_query(const uint32_t* cores, uint32_t n, uint32_t P, const uint32_t* ks,
+                        const uint32_t* lmds, uint32_t nq, uint64_t* offsets, uint32_t* nodes,
+                        uint64_t cap, void* stream);
+
 /* ---- batch ---------------------------------------------------------------
  * Many graphs at once: all (graph, lambda) columns in one persistent kernel
  * launch whose warps pull work items from device queues (captured in a CUDA
@@ -291,11 +337,20 @@ fc_status fc_server_destroy(fc_server* s);
  *   entry the slot u*L + l (neighbour u in layer l), v's layers in order --
  *   and deg0[n*L] = |N_l(v)| at v*L + l.  Output (device): table[L*n],
  *   lambda-major.  The call returns when the table is complete.
- * A graph whose one column needs more than 64 MiB of scratch (about
+ * Preconditions, as the graph's own CSR satisfies them: node_ptr[0] = 0,
+ * node_ptr non-decreasing, node_ptr[n] = entries, every slot < n*L, and the
+ * graph undirected (each entry u*L + l in v's row matched by v*L + l in u's
+ * row) with deg0[u*L + l] the number of entries u*L + l.  The first three
+ * and the slot bound are checked on the device before the peel runs (a
+ * violation returns FC_ERR_INVALID with nothing else done); the others
+ * decide only the values of the table.
+ * A graph whose one column needs more than the array's scratch (about
  * 4*n*L + 36*n + entries/16 bytes) is rejected with FC_ERR_TOO_LARGE before
  * any device work.  The first call on a device looks the array up (make it
- * before any stream capture).  All calls share the array, so calls that
- * overlap on the GPU race; each call clears the parts that must start empty. */
+ * before any stream capture).  All calls share the one array per device, so
+ * calls that overlap on the GPU -- on two streams, or from two host threads
+ * -- race, and the caller must serialize them; each call clears the parts
+ * that must start empty. */
 fc_status fc_coreindex_fixed_scratch(uint32_t n, uint32_t n_layers, uint64_t entries,
                                      const uint32_t* node_ptr, const uint32_t* adj,
                                      const uint32_t* deg0, uint32_t* table, void* stream);
@@ -316,6 +371,18 @@ typedef struct fc_stats {
 
 fc_status fc_graph_stats(const fc_graph* g, fc_stats* out);
 uint64_t fc_launch_count(void);
+/* Device and pinned-host allocations, streams and events this library has
+ * created in the process (a call that allocates nothing leaves it unchanged). */
+uint64_t fc_alloc_count(void);
+
+/* The atomic-throughput denominator of the peel's roofline (no counterpart
+ * in the reference): `ops` 4-byte atomic subtractions whose old value is
+ * returned, as the peel's degree decrements are, at pseudo-random word
+ * addresses of a device buffer of at most `bytes` bytes (a power-of-two word
+ * count; at least 4 KiB), timed with CUDA events on `stream` after one
+ * warm-up launch.  *gatomics_per_s receives the rate in 1e9 atomics/s.  The
+ * buffer is allocated and freed by the call. */
+fc_status fc_probe_atomics(uint64_t bytes, uint64_t ops, double* gatomics_per_s, void* stream);
 
 #ifdef __cplusplus
 }

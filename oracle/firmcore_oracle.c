@@ -402,3 +402,105 @@ int oracle_densest(const oracle_graph* g, const uint32_t* table, double beta,
     free(powl); free(e2); free(ld); free(order); free(col);
     return 0;
 }
+
+/* ---- query-time methods (Util/CoreIndexTime.h, Util/CheckMLCDTime.h) ---- */
+
+/* getResCore, Util/CoreIndexTime.h:8-40: for each listed k of each lambda,
+ * every (key, val) of the column with val >= k, in the file's order. */
+uint64_t oracle_cells_scan(const uint32_t* table, uint32_t n, uint32_t L, const uint32_t* ks,
+                           const uint32_t* lmds, uint32_t nq, uint64_t* offsets, uint32_t* nodes) {
+    uint64_t at = 0;
+    for (uint32_t q = 0; q < nq; q++) {
+        offsets[q] = at;
+        if (lmds[q] < 1 || lmds[q] > L) continue;
+        const uint32_t* col = table + (uint64_t)(lmds[q] - 1) * n;
+        for (uint32_t v = 0; v < n; v++)
+            if (col[v] >= ks[q]) {
+                if (nodes) nodes[at] = v;
+                at++;
+            }
+    }
+    offsets[nq] = at;
+    return at;
+}
+
+/* main.cpp:567-572 sorts each column's (value, key) pairs by value; then
+ * getResCoreOffline, Util/CoreIndexTime.h:43-59, takes lower_bound(k) and
+ * everything after it.  A counting sort (stable) stands in for std::sort. */
+uint64_t oracle_cells_sorted(const uint32_t* table, uint32_t n, uint32_t L, const uint32_t* ks,
+                             const uint32_t* lmds, uint32_t nq, uint64_t* offsets,
+                             uint32_t* nodes) {
+    uint64_t at = 0;
+    uint32_t* sorted = (uint32_t*)malloc(((size_t)n + 1) * 4);
+    for (uint32_t q = 0; q < nq; q++) {
+        offsets[q] = at;
+        if (lmds[q] < 1 || lmds[q] > L || !sorted) continue;
+        const uint32_t* col = table + (uint64_t)(lmds[q] - 1) * n;
+        uint32_t kmax = 0;
+        for (uint32_t v = 0; v < n; v++)
+            if (col[v] > kmax) kmax = col[v];
+        uint64_t* start = (uint64_t*)calloc((size_t)kmax + 2, 8);
+        if (!start) continue;
+        for (uint32_t v = 0; v < n; v++) start[col[v] + 1]++;
+        for (uint32_t c = 1; c <= kmax + 1; c++) start[c] += start[c - 1];
+        for (uint32_t v = 0; v < n; v++) sorted[start[col[v]]++] = v;
+        /* start[c] is now the end of value c's run: lower_bound(k) = end of k-1's */
+        const uint64_t lb = ks[q] == 0 ? 0 : (ks[q] - 1 <= kmax ? start[ks[q] - 1] : n);
+        for (uint64_t i = lb; i < n; i++) {
+            if (nodes) nodes[at] = sorted[i];
+            at++;
+        }
+        free(start);
+    }
+    free(sorted);
+    offsets[nq] = at;
+    return at;
+}
+
+/* checktime, Util/CheckMLCDTime.h:9-42, node-major as there: for node i and
+ * query j, t counts the values >= k and f is set once t >= lmd after a
+ * match; node i joins query j's list when f. */
+uint64_t oracle_mlcd_query(const uint32_t* cores, uint32_t n, uint32_t P, const uint32_t* ks,
+                           const uint32_t* lmds, uint32_t nq, uint64_t* offsets,
+                           uint32_t* nodes) {
+    uint64_t* cnt = (uint64_t*)calloc((size_t)nq + 1, 8);
+    uint8_t* hit = (uint8_t*)malloc((size_t)n * (nq ? nq : 1));
+    uint64_t total = 0;
+    if (!cnt || !hit) {
+        free(cnt);
+        free(hit);
+        return 0;
+    }
+    for (uint32_t i = 0; i < n; i++) {
+        for (uint32_t j = 0; j < nq; j++) {
+            const uint32_t k = ks[j], lmd = lmds[j];
+            int f = 0;
+            uint32_t t = 0;
+            for (uint32_t p = 0; p < P; p++) {
+                if (cores[(uint64_t)i * P + p] >= k) {
+                    t++;
+                    if (t >= lmd) {
+                        f = 1;
+                        break;
+                    }
+                }
+            }
+            hit[(uint64_t)i * nq + j] = (uint8_t)f;
+            cnt[j] += (uint64_t)f;
+        }
+    }
+    for (uint32_t j = 0; j < nq; j++) {
+        offsets[j] = total;
+        total += cnt[j];
+    }
+    offsets[nq] = total;
+    if (nodes)
+        for (uint32_t j = 0; j < nq; j++) {
+            uint64_t at = offsets[j];
+            for (uint32_t i = 0; i < n; i++)
+                if (hit[(uint64_t)i * nq + j]) nodes[at++] = i;
+        }
+    free(cnt);
+    free(hit);
+    return total;
+}

@@ -57,6 +57,30 @@ int oracle_densest(const oracle_graph* g, const uint32_t* table, double beta,
                    oracle_densest_result* res, oracle_cell* cells, uint32_t cells_cap,
                    uint32_t* nodes, uint32_t* layers);
 
+/* getResCore (Util/CoreIndexTime.h:8-40): query q is the cell (ks[q], lmds[q]);
+ * its answer is every node v whose core_lmd(v) >= k, in ascending ids (the
+ * order of the core file the reference scans).  offsets (nq+1) receives each
+ * answer's start and the total; nodes (may be NULL) the ids.  Returns the total. */
+uint64_t oracle_cells_scan(const uint32_t* table, uint32_t n, uint32_t L, const uint32_t* ks,
+                           const uint32_t* lmds, uint32_t nq, uint64_t* offsets, uint32_t* nodes);
+
+/* getResCoreOffline with main.cpp:567-572 (Util/CoreIndexTime.h:43-59): the
+ * column's (core, v) pairs sorted by core, then every pair from the first
+ * with core >= k (lower_bound) to the end.  The sort here is stable, so a
+ * query's nodes come by ascending core and ascending ids within a core (the
+ * reference's std::sort leaves ties in any order: compare as sets).  Same
+ * outputs as oracle_cells_scan. */
+uint64_t oracle_cells_sorted(const uint32_t* table, uint32_t n, uint32_t L, const uint32_t* ks,
+                             const uint32_t* lmds, uint32_t nq, uint64_t* offsets,
+                             uint32_t* nodes);
+
+/* checktime (Util/CheckMLCDTime.h:9-42): node i answers query (ks[q], lmds[q])
+ * when, counting its values cores[i*P + p] >= k in p order, the count
+ * reaches lmd (tested only after a match).  Answers in ascending ids. */
+uint64_t oracle_mlcd_query(const uint32_t* cores, uint32_t n, uint32_t P, const uint32_t* ks,
+                           const uint32_t* lmds, uint32_t nq, uint64_t* offsets,
+                           uint32_t* nodes);
+
 #ifdef __cplusplus
 }
 #endif

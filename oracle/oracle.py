@@ -55,6 +55,12 @@ def lib():
         L.oracle_coreindex.argtypes = [p, p]
         L.oracle_densest.argtypes = [p, p, C.c_double, C.POINTER(DensestResult), p, C.c_uint32,
                                      p, p]
+        for name in ("oracle_cells_scan", "oracle_cells_sorted"):
+            f = getattr(L, name)
+            f.argtypes = [p, C.c_uint32, C.c_uint32, p, p, C.c_uint32, p, p]
+            f.restype = C.c_uint64
+        L.oracle_mlcd_query.argtypes = [p, C.c_uint32, C.c_uint32, p, p, C.c_uint32, p, p]
+        L.oracle_mlcd_query.restype = C.c_uint64
         _lib = L
     return _lib
 
@@ -130,6 +136,56 @@ class OracleGraph:
         return out
 
 
+def _split(offsets, nodes):
+    return [nodes[offsets[i]:offsets[i + 1]].copy() for i in range(len(offsets) - 1)]
+
+
+def _queries(ks, lmds):
+    ks = np.ascontiguousarray(np.asarray(ks, dtype=np.uint32))
+    lmds = np.ascontiguousarray(np.asarray(lmds, dtype=np.uint32))
+    return ks, lmds, len(ks)
+
+
+def cells_scan(table, ks, lmds):
+    """getResCore's answers (Util/CoreIndexTime.h:8-40): per query (k, lmd)
+    the nodes with core_lmd >= k, ascending ids."""
+    table = np.ascontiguousarray(table, dtype=np.uint32)
+    L, n = table.shape
+    ks, lmds, nq = _queries(ks, lmds)
+    off = np.zeros(nq + 1, np.uint64)
+    lib().oracle_cells_scan(_ptr(table), n, L, _ptr(ks), _ptr(lmds), nq, _ptr(off), None)
+    nodes = np.zeros(int(off[-1]) + 1, np.uint32)
+    lib().oracle_cells_scan(_ptr(table), n, L, _ptr(ks), _ptr(lmds), nq, _ptr(off), _ptr(nodes))
+    return _split(off, nodes)
+
+
+def cells_sorted(table, ks, lmds):
+    """getResCoreOffline's answers (Util/CoreIndexTime.h:43-59 after the sort
+    of main.cpp:567-572): by ascending core, ids ascending within a core."""
+    table = np.ascontiguousarray(table, dtype=np.uint32)
+    L, n = table.shape
+    ks, lmds, nq = _queries(ks, lmds)
+    off = np.zeros(nq + 1, np.uint64)
+    lib().oracle_cells_sorted(_ptr(table), n, L, _ptr(ks), _ptr(lmds), nq, _ptr(off), None)
+    nodes = np.zeros(int(off[-1]) + 1, np.uint32)
+    lib().oracle_cells_sorted(_ptr(table), n, L, _ptr(ks), _ptr(lmds), nq, _ptr(off),
+                              _ptr(nodes))
+    return _split(off, nodes)
+
+
+def mlcd_query(cores, ks, lmds):
+    """checktime's answers (Util/CheckMLCDTime.h:9-42) over the (n, P)
+    coreness matrix, ascending ids."""
+    cores = np.ascontiguousarray(cores, dtype=np.uint32)
+    n, P = cores.shape
+    ks, lmds, nq = _queries(ks, lmds)
+    off = np.zeros(nq + 1, np.uint64)
+    lib().oracle_mlcd_query(_ptr(cores), n, P, _ptr(ks), _ptr(lmds), nq, _ptr(off), None)
+    nodes = np.zeros(int(off[-1]) + 1, np.uint32)
+    lib().oracle_mlcd_query(_ptr(cores), n, P, _ptr(ks), _ptr(lmds), nq, _ptr(off), _ptr(nodes))
+    return _split(off, nodes)
+
+
 # ---- the reference itself ---------------------------------------------------
 
 def harness_available():
@@ -147,7 +203,7 @@ def run_harness(src, mode, *args, timeout=3600):
 def ref_table(src, L, n, mode="table", threads=1):
     with tempfile.TemporaryDirectory() as d:
         out = os.path.join(d, "t.bin")
-        run_harness(src, mode, out, *([threads] if mode == "pgtable" else []))
+        run_harness(src, mode, out, *([threads] if threads > 1 or mode == "pgtable" else []))
         return np.fromfile(out, dtype=np.uint32).reshape(L, n)
 
 

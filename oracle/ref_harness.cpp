@@ -17,8 +17,11 @@
 //           FCTree::WeightDenestSubgraph (Core/FCTree.cpp:69-82) as main.cpp
 //           does for `-m WdsList` (main.cpp:402-424); prints the per-cell
 //           records of the tree and the winning cell's node set.
-//   bench   times ParGrid (FCSyncLeft::Execute, main.cpp:229-257) and
-//           WdsList on the same loaded graph, K timed runs after W warm-up runs.
+//   bench   times the reference's methods on the same loaded graph as
+//           main.cpp times them: ParGrid (FCSyncLeft::Execute, main.cpp:
+//           229-239), ParGridPlus (FCSyncLeft::ExecuteMix, :277-291),
+//           ParCoreIndex (CoreIndex::ExecuteParallel, :378-385) and WdsList
+//           (:402-418), W warm-up then K timed runs of the listed ones.
 //
 // Input is either a dataset directory loaded by the reference's own
 // MultilayerGraph::LoadFromFile (Graph/MultilayerGraph.cpp:65-102), or an
@@ -112,9 +115,13 @@ static void emit_table(const std::vector<std::vector<uint>>& t, const char* out)
     fclose(f);
 }
 
-static void mode_table(MultilayerGraph& mg, const char* out) {
+// With threads > 1 the lambda columns run in parallel, each on its own fresh
+// degree table, as CoreIndex::ExecuteParallel runs them (CoreIndex.cpp:
+// 252-275).
+static void mode_table(MultilayerGraph& mg, const char* out, int threads) {
     uint n = mg.GetN(), L = mg.getLayerNumber();
     std::vector<std::vector<uint>> t(L, std::vector<uint>(n));
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads > 0 ? threads : 1)
     for (uint lmd = 1; lmd <= L; lmd++) {
         uint** d = fresh_degs(mg);
         uint* c = get_index2(mg, d, lmd, nullptr);
@@ -231,28 +238,75 @@ static double now() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-static void mode_bench(MultilayerGraph& mg, int steps, int warmup, double beta, int threads) {
+// The reference's methods as main.cpp times them, one call each; returns
+// seconds.  ParGridPlus turns nested parallelism on as main.cpp:278-281 does
+// and off again after, so that it does not carry over to the other methods
+// (each of which main.cpp runs in a process of its own).
+static double time_method(MultilayerGraph& mg, const std::string& m, int threads, double beta,
+                          ll_uint* id2vtx, uint* rk, uint* rl, uint* rlen, float* md) {
     uint n = mg.GetN();
     omp_set_num_threads(threads);
-    for (int it = 0; it < warmup + steps; it++) {
-        // ParGrid exactly as main.cpp:229-239 times it
-        omp_set_num_threads(threads);
+    if (m == "ParGrid") {  // main.cpp:229-239
         double t0 = omp_get_wtime();
         FCCoreTree tree(1, 1, n);
         FCSyncLeft::Execute(mg, tree);
-        double t1 = omp_get_wtime();
-        // WdsList exactly as main.cpp:402-418 times it
-        uint rk = 0, rl = 0, rlen = 0;
-        float md = 0.0f;
-        double t2 = omp_get_wtime();
+        return omp_get_wtime() - t0;
+    }
+    if (m == "ParGridPlus") {  // main.cpp:277-291
+        omp_set_nested(1);
+        omp_set_max_active_levels(2);
+        omp_set_num_threads(threads);
+        double t0 = omp_get_wtime();
+        FCCoreTree tree(1, 1, n);
+        FCSyncLeft::ExecuteMix(mg, tree);
+        double t = omp_get_wtime() - t0;
+        omp_set_nested(0);
+        omp_set_max_active_levels(1);
+        return t;
+    }
+    if (m == "ParCoreIndex") {  // main.cpp:378-385
+        double t0 = omp_get_wtime();
+        CoreIndex::ExecuteParallel(mg, id2vtx);
+        return omp_get_wtime() - t0;
+    }
+    if (m == "WdsList") {  // main.cpp:402-418
+        double t0 = omp_get_wtime();
         FCTree wt(1, 1, n);
         FCPathLevelLeft::Execute(mg, wt, true, beta);
-        double t3 = omp_get_wtime();
-        wt.WeightDenestSubgraph(wt.getNode(), md, rk, rl, rlen);
+        double t = omp_get_wtime() - t0;
+        wt.WeightDenestSubgraph(wt.getNode(), *md, *rk, *rl, *rlen);
         free_tree(wt.getNode(), n);
-        printf("STEP {\"step\": %d, \"warmup\": %s, \"pargrid_s\": %.6f, \"wdslist_s\": %.6f, "
-               "\"density\": %.9g, \"k\": %u, \"lmd\": %u, \"len\": %u}\n",
-               it, it < warmup ? "true" : "false", t1 - t0, t3 - t2, (double)md, rk, rl, rlen);
+        return t;
+    }
+    die("unknown method");
+    return 0;
+}
+
+// `methods` is a comma-separated list of ParGrid, ParGridPlus, ParCoreIndex,
+// WdsList; every step times each of them once, in that order, and prints one
+// STEP line with their seconds.
+static void mode_bench(MultilayerGraph& mg, int steps, int warmup, double beta, int threads,
+                       const std::string& methods, ll_uint* id2vtx) {
+    std::vector<std::string> ms;
+    for (size_t a = 0; a <= methods.size();) {
+        size_t b = methods.find(',', a);
+        if (b == std::string::npos) b = methods.size();
+        if (b > a) ms.push_back(methods.substr(a, b - a));
+        a = b + 1;
+    }
+    for (int it = 0; it < warmup + steps; it++) {
+        uint rk = 0, rl = 0, rlen = 0;
+        float md = 0.0f;
+        std::string times;
+        for (const std::string& m : ms) {
+            double t = time_method(mg, m, threads, beta, id2vtx, &rk, &rl, &rlen, &md);
+            char b[96];
+            snprintf(b, sizeof(b), ", \"%s\": %.6f", m.c_str(), t);
+            times += b;
+        }
+        printf("STEP {\"step\": %d, \"warmup\": %s%s, \"density\": %.9g, \"k\": %u, "
+               "\"lmd\": %u, \"len\": %u}\n",
+               it, it < warmup ? "true" : "false", times.c_str(), (double)md, rk, rl, rlen);
         fflush(stdout);
     }
 }
@@ -260,10 +314,11 @@ static void mode_bench(MultilayerGraph& mg, int steps, int warmup, double beta, 
 int main(int argc, char** argv) {
     if (argc < 4) {
         fprintf(stderr,
-                "usage: ref_harness <dir/|file.fcg> table <out.bin>\n"
+                "usage: ref_harness <dir/|file.fcg> table <out.bin> [threads]\n"
                 "       ref_harness <dir/|file.fcg> pgtable <out.bin> [threads]\n"
                 "       ref_harness <dir/|file.fcg> wds <out.txt> <beta> [threads]\n"
-                "       ref_harness <dir/|file.fcg> bench <steps> <warmup> <beta> <threads>\n");
+                "       ref_harness <dir/|file.fcg> bench <steps> <warmup> <beta> <threads> "
+                "[methods, default ParGrid,WdsList]\n");
         return 2;
     }
     std::string in = argv[1];
@@ -278,14 +333,19 @@ int main(int argc, char** argv) {
     }
     double tl1 = now();
     fprintf(stderr, "loaded n=%u L=%u in %.2fs\n", mg.GetN(), mg.getLayerNumber(), tl1 - tl0);
-    if (mode == "table") mode_table(mg, argv[3]);
+    if (mode == "table") mode_table(mg, argv[3], argc > 4 ? atoi(argv[4]) : 1);
     else if (mode == "pgtable") mode_pgtable(mg, argv[3], argc > 4 ? atoi(argv[4]) : 1);
     else if (mode == "wds") {
         if (argc < 5) die("wds needs beta");
         mode_wds(mg, atof(argv[4]), argc > 5 ? atoi(argv[5]) : 1, argv[3]);
     } else if (mode == "bench") {
         if (argc < 7) die("bench needs steps warmup beta threads");
-        mode_bench(mg, atoi(argv[3]), atoi(argv[4]), atof(argv[5]), atoi(argv[6]));
+        if (id2vtx.empty()) {
+            id2vtx.resize(mg.GetN());
+            mg.LoadId2VtxMap(id2vtx.data());
+        }
+        mode_bench(mg, atoi(argv[3]), atoi(argv[4]), atof(argv[5]), atoi(argv[6]),
+                   argc > 7 ? argv[7] : "ParGrid,WdsList", id2vtx.data());
     } else die("unknown mode");
     return 0;
 }

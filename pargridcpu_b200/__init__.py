@@ -26,7 +26,7 @@ import numpy as np
 from . import native as _n
 
 __all__ = ["MultilayerGraph", "CoreIndex", "FCSyncLeft", "FCPathLevelLeft", "batch_run",
-           "Server", "build", "FcError", "launch_count"]
+           "Server", "build", "FcError", "launch_count", "mlcd_query"]
 
 FcError = _n.FcError
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -196,23 +196,65 @@ class MultilayerGraph:
                                           C.byref(cnt), _n.stream_handle(stream)), "cell_members")
         return nodes[:cnt.value].copy()
 
-    def coreindex_range(self, lmd_lo, lmd_hi, stream=None):
+    def cell_index(self, stream=None):
+        """Every cell as a prefix (the compact form of -m CoreMem / PathMem):
+        (order, col_off, sizes) -- order[lambda-1] is column lambda's nodes by
+        descending core, ids ascending within a core; C_{k,lambda} is
+        order[lambda-1][:sizes[col_off[lambda-1] + k]]."""
+        n, L = self.n, self.L
+        off = np.zeros(L + 1, np.uint64)
+        cnt = C.c_uint64()
+        _n.check(_n.lib().fc_cell_index(self._h, None, _n.ptr(off), None, 0, C.byref(cnt),
+                                        _n.stream_handle(stream)), "cell_index")
+        order = np.zeros((L, n), np.uint32)
+        sizes = np.zeros(max(cnt.value, 1), np.uint32)
+        _n.check(_n.lib().fc_cell_index(self._h, _n.ptr(order), _n.ptr(off), _n.ptr(sizes),
+                                        cnt.value, C.byref(cnt), _n.stream_handle(stream)),
+                 "cell_index")
+        return order, off, sizes[:cnt.value]
+
+    def cells_members(self, ks, lmds, by_index=False, stream=None):
+        """Many cells at once (-m CoreIndexTimeOnline / Offline): one array of
+        node ids per query (k, lmd); ascending ids, or with by_index=True each
+        cell's prefix of the cell index order."""
+        ks = np.ascontiguousarray(np.asarray(ks, dtype=np.uint32))
+        lmds = np.ascontiguousarray(np.asarray(lmds, dtype=np.uint32))
+        nq = len(ks)
+        off = np.zeros(nq + 1, np.uint64)
+        h = _n.stream_handle(stream)
+        _n.check(_n.lib().fc_cells_members(self._h, _n.ptr(ks), _n.ptr(lmds), nq, int(by_index),
+                                           _n.ptr(off), None, 0, h), "cells_members")
+        nodes = np.zeros(max(int(off[-1]), 1), np.uint32)
+        _n.check(_n.lib().fc_cells_members(self._h, _n.ptr(ks), _n.ptr(lmds), nq, int(by_index),
+                                           _n.ptr(off), _n.ptr(nodes), int(off[-1]), h),
+                 "cells_members")
+        return [nodes[off[i]:off[i + 1]].copy() for i in range(nq)]
+
+    def coreindex_range(self, lmd_lo, lmd_hi, out=None, stream=None, copy=True):
         """Columns lmd_lo .. lmd_hi-1 of the core table, (lmd_hi - lmd_lo, n):
-        one process's share when a graph is split by lambda range."""
-        out = np.zeros((lmd_hi - lmd_lo, self.n), np.uint32)
+        one process's share when a graph is split by lambda range.  With
+        copy=False the columns are only computed (they stay resident)."""
+        h = _n.stream_handle(stream)
+        if not copy:
+            _n.check(_n.lib().fc_coreindex_range(self._h, int(lmd_lo), int(lmd_hi), None, 0, h),
+                     "coreindex_range")
+            return None
+        if out is None:
+            out = np.zeros((lmd_hi - lmd_lo, self.n), np.uint32)
         _n.check(_n.lib().fc_coreindex_range(self._h, int(lmd_lo), int(lmd_hi), _n.ptr(out), 0,
-                                             _n.stream_handle(stream)), "coreindex_range")
+                                             h), "coreindex_range")
         return out
 
-    def cells_range(self, lmd_lo, lmd_hi, beta=1.0):
+    def cells_range(self, lmd_lo, lmd_hi, beta=1.0, stream=None):
         """The cells of lambda lmd_lo .. lmd_hi-1 as (k, lmd, length, lstar,
         density) tuples, the form shard.merge_cells folds."""
         cnt = C.c_uint32()
+        h = _n.stream_handle(stream)
         _n.check(_n.lib().fc_cells_range(self._h, int(lmd_lo), int(lmd_hi), float(beta), None, 0,
-                                         C.byref(cnt), None), "cells_range")
+                                         C.byref(cnt), h), "cells_range")
         buf = (_n.Cell * max(cnt.value, 1))()
         _n.check(_n.lib().fc_cells_range(self._h, int(lmd_lo), int(lmd_hi), float(beta),
-                                         C.cast(buf, C.c_void_p), cnt.value, C.byref(cnt), None),
+                                         C.cast(buf, C.c_void_p), cnt.value, C.byref(cnt), h),
                  "cells_range")
         return [(int(c.k), int(c.lmd), int(c.length), int(c.lstar), float(c.density))
                 for c in buf[:cnt.value]]
@@ -255,6 +297,33 @@ class FCPathLevelLeft:
     @staticmethod
     def Execute(mg: MultilayerGraph, tree=None, wds=True, beta=1.0):
         return mg.densest([beta])[0] if wds else mg.coreindex()
+
+
+def mlcd_query(cores, ks, lmds, stream=None):
+    """The membership test of -m MLCDTime (checktime) on an (n, P) matrix of
+    per-node coreness values: one ascending id array per query (k, lmd)."""
+    cores = np.ascontiguousarray(cores, dtype=np.uint32)
+    n, P = cores.shape
+    ks = np.ascontiguousarray(np.asarray(ks, dtype=np.uint32))
+    lmds = np.ascontiguousarray(np.asarray(lmds, dtype=np.uint32))
+    nq = len(ks)
+    off = np.zeros(nq + 1, np.uint64)
+    h = _n.stream_handle(stream)
+    _n.check(_n.lib().fc_mlcd_query(_n.ptr(cores), n, P, _n.ptr(ks), _n.ptr(lmds), nq,
+                                    _n.ptr(off), None, 0, h), "mlcd_query")
+    nodes = np.zeros(max(int(off[-1]), 1), np.uint32)
+    _n.check(_n.lib().fc_mlcd_query(_n.ptr(cores), n, P, _n.ptr(ks), _n.ptr(lmds), nq,
+                                    _n.ptr(off), _n.ptr(nodes), int(off[-1]), h), "mlcd_query")
+    return [nodes[off[i]:off[i + 1]].copy() for i in range(nq)]
+
+
+def probe_atomics(buffer_bytes, ops=1 << 28, stream=None):
+    """Returned-value 4-byte atomic subtractions per second (1e9/s) at random
+    addresses of a device buffer of ``buffer_bytes`` (fc_probe_atomics)."""
+    r = C.c_double()
+    _n.check(_n.lib().fc_probe_atomics(int(buffer_bytes), int(ops), C.byref(r),
+                                       _n.stream_handle(stream)), "probe_atomics")
+    return r.value
 
 
 def launch_count():

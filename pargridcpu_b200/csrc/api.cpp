@@ -11,6 +11,8 @@ namespace fc {
 
 static std::atomic<uint64_t> g_launches{0};
 void count_launch(uint32_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+static std::atomic<uint64_t> g_allocs{0};
+void count_alloc(uint32_t k) { g_allocs.fetch_add(k, std::memory_order_relaxed); }
 
 // The peel of columns [lo, hi) in launches of up to peel_columns_per_group
 // columns each, with the launches' statistics.
@@ -281,6 +283,44 @@ fc_status fc_cells(fc_graph* g, double beta, fc_cell* cells_out, uint32_t cap, u
     return cells(g, beta, cells_out, cap, count, (cudaStream_t)stream);
 }
 
+fc_status fc_cell_index(fc_graph* g, uint32_t* order, uint64_t* col_off, uint32_t* sizes,
+                        uint64_t sizes_cap, uint64_t* sizes_count, void* stream) {
+    if (!g) return FC_ERR_INVALID;
+    if (!cuda_available()) return FC_ERR_NO_DEVICE;
+    if (!g->n || !g->L) {
+        if (col_off)
+            for (uint32_t l = 0; l <= g->L; l++) col_off[l] = 0;
+        if (sizes_count) *sizes_count = 0;
+        return FC_OK;
+    }
+    return cell_index(g, order, col_off, sizes, sizes_cap, sizes_count, (cudaStream_t)stream);
+}
+
+fc_status fc_cells_members(fc_graph* g, const uint32_t* ks, const uint32_t* lmds, uint32_t nq,
+                           int by_index, uint64_t* offsets, uint32_t* nodes, uint64_t cap,
+                           void* stream) {
+    if (!g || (nq && (!ks || !lmds))) return FC_ERR_INVALID;
+    if (!cuda_available()) return FC_ERR_NO_DEVICE;
+    for (uint32_t q = 0; q < nq; q++)
+        if (lmds[q] < 1 || lmds[q] > g->L) return FC_ERR_INVALID;
+    if (!g->n) {
+        if (offsets)
+            for (uint32_t q = 0; q <= nq; q++) offsets[q] = 0;
+        return FC_OK;
+    }
+    return cells_members(g, ks, lmds, nq, by_index != 0, offsets, nodes, cap,
+                         (cudaStream_t)stream);
+}
+
+fc_status fc_mlcd_query(const uint32_t* cores, uint32_t n, uint32_t P, const uint32_t* ks,
+                        const uint32_t* lmds, uint32_t nq, uint64_t* offsets, uint32_t* nodes,
+                        uint64_t cap, void* stream) {
+    if ((n && P && !cores) || (nq && (!ks || !lmds))) return FC_ERR_INVALID;
+    if (!cuda_available()) return FC_ERR_NO_DEVICE;
+    if ((uint64_t)n * P >= (1ull << 40)) return FC_ERR_TOO_LARGE;
+    return mlcd_query(cores, n, P, ks, lmds, nq, offsets, nodes, cap, (cudaStream_t)stream);
+}
+
 fc_status fc_graph_stats(const fc_graph* g, fc_stats* out) {
     if (!g || !out) return FC_ERR_INVALID;
     *out = g->dev ? g->dev->stats : fc_stats{};
@@ -288,6 +328,13 @@ fc_status fc_graph_stats(const fc_graph* g, fc_stats* out) {
 }
 
 uint64_t fc_launch_count(void) { return g_launches.load(std::memory_order_relaxed); }
+uint64_t fc_alloc_count(void) { return g_allocs.load(std::memory_order_relaxed); }
+
+fc_status fc_probe_atomics(uint64_t bytes, uint64_t ops, double* gatomics_per_s, void* stream) {
+    if (!gatomics_per_s || !ops) return FC_ERR_INVALID;
+    if (!cuda_available()) return FC_ERR_NO_DEVICE;
+    return probe_atomics(bytes, ops, gatomics_per_s, (cudaStream_t)stream);
+}
 
 fc_status fc_batch_run(fc_graph* const* graphs, uint32_t count, double beta,
                        uint32_t* const* tables, fc_densest_result* res,

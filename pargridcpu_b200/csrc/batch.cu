@@ -66,6 +66,7 @@ static std::vector<DenseWorker>* dense_workers() {
         v.resize(DENSE_WORKERS);
         for (DenseWorker& w : v) {
             if (cudaStreamCreateWithFlags(&w.s, cudaStreamNonBlocking) != cudaSuccess) w.s = nullptr;
+            count_alloc(2);  // the stream and the staging buffer
             if (cudaHostAlloc(&w.stage.p, 1u << 20, cudaHostAllocDefault) == cudaSuccess)
                 w.stage.cap = 1u << 20;
             else

@@ -6,8 +6,24 @@
 //
 // Methods: ParGrid, ParGridPlus, CoreIndex, ParCoreIndex (the core table),
 // WdsList, WdsCoreIndex (densest subgraph), fcgrid (kupper/lmdupper report),
-// kpe with -k/-lmd (writes one cell to ../output/, FCTree::saveCoreToLocal).
-// Extra flag: -table <file> writes the L*n uint32 table (lambda-major).
+// kpe with -k/-lmd (writes one cell to ../output/, FCTree::saveCoreToLocal),
+// CoreMem / PathMem (every cell in compact form: the cell index),
+// CoreIndexTimeOnline / CoreIndexTimeOffline (a list of cells answered from
+// the table by a scan / from the cell index) and MLCDTime (the MLCD
+// membership test on a coreness file), main.cpp:331-362, 453-582.
+// Extra flags:
+//   -table <file>  writes the L*n uint32 table (lambda-major);
+//   -klmd <file>   the cell list of the query methods, "k lmd" per line
+//                  (default ../klmd/<d>_klmd.txt, the reference's klmd/
+//                  directory; the reference reads a fixed absolute path);
+//   -cores <file>  MLCDTime's coreness file, one node per line, P values each
+//                  (default ../cores/<d>_cores.txt);
+//   -qout <file>   the query methods write their answers there, one block per
+//                  query: "########## k_<k>_lmd_<lmd>_length_<len>", then the
+//                  nodes (original ids; MLCDTime: row numbers), one per line;
+//   -cells <file>  CoreMem / PathMem write the cell index there (binary,
+//                  little-endian: u32 L, u32 n, u64 col_off[L+1],
+//                  u32 sizes[col_off[L]], u32 order[L*n]; fc_cell_index).
 #include <sys/resource.h>
 
 #include <algorithm>
@@ -17,6 +33,7 @@
 #include <fstream>
 #include <iomanip>
 #include <iostream>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -48,7 +65,7 @@ int main(int argc, char* argv[]) {
     int order = 0;
     unsigned k = 0, lmd = 0, num_thread = 1;
     double beta = 1.0;
-    string table_out;
+    string table_out, klmd_path, cores_path, qout_path, cells_path;
     for (int i = 1; i < argc; i++) {
         string arg = argv[i];
         if (arg == "-d" && i + 1 < argc) dataset = argv[++i];
@@ -59,7 +76,13 @@ int main(int argc, char* argv[]) {
         if (arg == "-num_thread" && i + 1 < argc) num_thread = std::atoi(argv[++i]);
         if (arg == "-beta" && i + 1 < argc) beta = std::atof(argv[++i]);
         if (arg == "-table" && i + 1 < argc) table_out = argv[++i];
+        if (arg == "-klmd" && i + 1 < argc) klmd_path = argv[++i];
+        if (arg == "-cores" && i + 1 < argc) cores_path = argv[++i];
+        if (arg == "-qout" && i + 1 < argc) qout_path = argv[++i];
+        if (arg == "-cells" && i + 1 < argc) cells_path = argv[++i];
     }
+    if (klmd_path.empty()) klmd_path = "../klmd/" + dataset + "_klmd.txt";
+    if (cores_path.empty()) cores_path = "../cores/" + dataset + "_cores.txt";
     if (dataset == "") cout << "Use the default dataset example as the user did not specify the dataset" << endl;
     if (method == "") cout << "Use the FirmCore Tree Serial method as the user did not specify the method" << endl;
     cout << "method = " << method << " dataset = " << dataset << endl;
@@ -200,6 +223,117 @@ int main(int argc, char* argv[]) {
             }
         }
         write_table();
+    }
+    if (method == "CoreMem" || method == "PathMem") {
+        // the table and every cell in compact form (the per-cell difference
+        // lists of FCSyncMem / FCPathMem are the blocks of the cell index)
+        double t0 = now_s();
+        table.assign((size_t)n * L, 0);
+        if ((s = fc_coreindex(g, table.data(), 0, nullptr)) != FC_OK) return fail(method.c_str(), s);
+        std::vector<uint64_t> col_off(L + 1);
+        uint64_t nsizes = 0;
+        if ((s = fc_cell_index(g, nullptr, col_off.data(), nullptr, 0, &nsizes, nullptr)) != FC_OK)
+            return fail(method.c_str(), s);
+        std::vector<uint32_t> sizes(nsizes), order((size_t)n * L);
+        if ((s = fc_cell_index(g, order.data(), col_off.data(), sizes.data(), nsizes, &nsizes,
+                               nullptr)) != FC_OK)
+            return fail(method.c_str(), s);
+        secs = now_s() - t0;
+        if (method == "CoreMem") {
+            cout << "CoreParallel Sync with Memory reduction Elapsed time: " << secs << " seconds\n";
+            cout << "CoreParallel Sync with Memory reduction mem = " << peak_rss_mb() << " MB" << endl;
+        } else {
+            cout << "PathParallel with Memory reduction Elapsed time: " << secs << " seconds\n";
+            cout << "PathParallel Sync with Memory reduction mem = " << peak_rss_mb() << " MB" << endl;
+        }
+        if (!cells_path.empty()) {
+            std::ofstream f(cells_path, std::ios::binary);
+            f.write((const char*)&L, 4);
+            f.write((const char*)&n, 4);
+            f.write((const char*)col_off.data(), (std::streamsize)col_off.size() * 8);
+            f.write((const char*)sizes.data(), (std::streamsize)sizes.size() * 4);
+            f.write((const char*)order.data(), (std::streamsize)order.size() * 4);
+        }
+        write_table();
+    }
+
+    if (method == "CoreIndexTimeOnline" || method == "CoreIndexTimeOffline" || method == "MLCDTime") {
+        // the cell list, "k lmd" pairs (main.cpp:458-463, 497-502, 535-540)
+        std::vector<uint32_t> ks, lmds;
+        {
+            std::ifstream in(klmd_path);
+            if (!in) return fail(("reading " + klmd_path).c_str(), FC_ERR_IO);
+            long long kk, ll;
+            while (in >> kk >> ll) {
+                // the table methods index klmd[lmd] (size L+1): other lambdas
+                // are outside the reference's arrays and are left out here
+                if (method != "MLCDTime" && (ll < 1 || ll > (long long)L)) continue;
+                ks.push_back((uint32_t)kk);
+                lmds.push_back((uint32_t)ll);
+            }
+        }
+        const uint32_t nq = (uint32_t)ks.size();
+        std::vector<uint64_t> qoff(nq + 1, 0);
+        std::vector<uint32_t> qnodes;
+        std::vector<uint64_t> id2vtx;
+        if (method == "MLCDTime") {
+            // one node per line, its values (main.cpp:466-482); every line
+            // must hold as many values as the first
+            std::vector<uint32_t> cores;
+            uint32_t P = 0, rows = 0;
+            std::ifstream in(cores_path);
+            if (!in) return fail(("reading " + cores_path).c_str(), FC_ERR_IO);
+            string line;
+            while (std::getline(in, line)) {
+                std::istringstream ls(line);
+                long long x;
+                uint32_t c = 0;
+                while (ls >> x) {
+                    cores.push_back((uint32_t)x);
+                    c++;
+                }
+                if (rows == 0) P = c;
+                if (c != P) return fail(("ragged row in " + cores_path).c_str(), FC_ERR_PARSE);
+                rows++;
+            }
+            double t0 = now_s();
+            s = fc_mlcd_query(cores.data(), rows, P, ks.data(), lmds.data(), nq, qoff.data(), nullptr,
+                              0, nullptr);
+            if (s == FC_OK) {
+                qnodes.resize(qoff[nq]);
+                s = fc_mlcd_query(cores.data(), rows, P, ks.data(), lmds.data(), nq, qoff.data(),
+                                  qnodes.data(), qnodes.size(), nullptr);
+            }
+            secs = now_s() - t0;
+            if (s != FC_OK) return fail(method.c_str(), s);
+        } else {
+            // the table first, untimed: the reference reads it from a file
+            // (main.cpp:508-519, 546-557) before its timer starts
+            if ((s = fc_coreindex(g, nullptr, 0, nullptr)) != FC_OK) return fail(method.c_str(), s);
+            const int by_index = method == "CoreIndexTimeOffline";
+            double t0 = now_s();
+            s = fc_cells_members(g, ks.data(), lmds.data(), nq, by_index, qoff.data(), nullptr, 0,
+                                 nullptr);
+            if (s == FC_OK) {
+                qnodes.resize(qoff[nq]);
+                s = fc_cells_members(g, ks.data(), lmds.data(), nq, by_index, qoff.data(),
+                                     qnodes.data(), qnodes.size(), nullptr);
+            }
+            secs = now_s() - t0;
+            if (s != FC_OK) return fail(method.c_str(), s);
+            id2vtx.resize(n);
+            fc_graph_id2vtx(g, id2vtx.data());
+        }
+        std::cout << "Elapsed time: " << secs << " seconds\n";
+        if (!qout_path.empty()) {
+            std::ofstream f(qout_path);
+            for (uint32_t q = 0; q < nq; q++) {
+                f << "########## k_" << ks[q] << "_lmd_" << lmds[q] << "_length_" << qoff[q + 1] - qoff[q]
+                  << "\n";
+                for (uint64_t i = qoff[q]; i < qoff[q + 1]; i++)
+                    f << (id2vtx.empty() ? (uint64_t)qnodes[i] : id2vtx[qnodes[i]]) << "\n";
+            }
+        }
     }
     fc_graph_free(g);
     return 0;

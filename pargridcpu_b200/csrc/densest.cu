@@ -472,6 +472,7 @@ fc_status densest(fc_graph* g, const double* betas, uint32_t nb, fc_densest_resu
     cudaEvent_t e0, e1;
     FC_CUDA_TRY(cudaEventCreate(&e0));
     FC_CUDA_TRY(cudaEventCreate(&e1));
+    count_alloc(2);
     FC_CUDA_TRY(cudaEventRecord(e0, st));
     FC_TRY(build_hist(d, st, 0, d->L));
     DensState* s = (DensState*)d->dens;
@@ -560,6 +561,7 @@ fc_status densest_members(fc_graph* g, const fc_densest_result* r, uint32_t* nod
 }
 
 void invalidate_densest(DeviceGraph* d) {
+    invalidate_cell_index(d);
     DensState* s = (DensState*)d->dens;
     if (s) s->hist_valid = false;
 }

@@ -102,6 +102,8 @@ struct DeviceGraph {
     std::vector<uint32_t> kmax;    // per lambda, max core (host copy)
     // densest state for the resident table (histograms, cell records)
     void* dens = nullptr;
+    // the cell index of the resident table (cellindex.cu)
+    void* cidx = nullptr;
     // reusable scratch
     void* ws = nullptr;
     size_t ws_bytes = 0;
@@ -135,6 +137,9 @@ void count_launch(uint32_t k = 1);
 fc_status ensure_ws(DeviceGraph* d, size_t bytes, cudaStream_t s);
 void free_densest_state(DeviceGraph* d);
 void invalidate_densest(DeviceGraph* d);
+// cellindex.cu: the resident cell index goes with the table it was built from
+void free_cell_index(DeviceGraph* d);
+void invalidate_cell_index(DeviceGraph* d);
 
 // peel.cu
 struct PeelStats {

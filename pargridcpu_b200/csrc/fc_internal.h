@@ -81,6 +81,18 @@ fc_status cells(fc_graph* g, double beta, fc_cell* out, uint32_t cap, uint32_t* 
                 cudaStream_t s);
 fc_status cell_members(fc_graph* g, uint32_t k, uint32_t lmd, uint32_t* nodes, uint32_t cap,
                        uint32_t* count, cudaStream_t s);
+// every cell as a prefix of one order per column (fc_cell_index), many cells
+// at once (fc_cells_members), the MLCD membership test (fc_mlcd_query)
+fc_status cell_index(fc_graph* g, uint32_t* order, uint64_t* col_off, uint32_t* sizes,
+                     uint64_t sizes_cap, uint64_t* sizes_count, cudaStream_t s);
+fc_status cells_members(fc_graph* g, const uint32_t* ks, const uint32_t* lmds, uint32_t nq,
+                        bool by_index, uint64_t* offsets, uint32_t* nodes, uint64_t cap,
+                        cudaStream_t s);
+fc_status mlcd_query(const uint32_t* cores, uint32_t n, uint32_t P, const uint32_t* ks,
+                     const uint32_t* lmds, uint32_t nq, uint64_t* offsets, uint32_t* nodes,
+                     uint64_t cap, cudaStream_t s);
+// fc_probe_atomics (probe.cu)
+fc_status probe_atomics(uint64_t bytes, uint64_t ops, double* rate, cudaStream_t s);
 // lambda columns [lo, hi), 0-based (fc_coreindex_range / fc_cells_range)
 fc_status coreindex_range(fc_graph* g, uint32_t lo, uint32_t hi, uint32_t* out, bool out_on_device,
                           cudaStream_t s);
@@ -102,6 +114,9 @@ fc_status batch_plain_one(fc_graph* g, cudaStream_t s, double* peel_ms, uint32_t
                           uint32_t* levels);
 // a graph's device copy is going away: servers drop it from their records
 void residency_forget(fc_graph* g);
+// device or pinned-host allocations, streams and events this library created
+// (fc_alloc_count)
+void count_alloc(uint32_t k = 1);
 // loads every kernel of the library on the current device now (once)
 void preload_kernels();
 void peel_preload();

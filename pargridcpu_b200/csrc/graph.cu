@@ -248,6 +248,7 @@ fc_status dev_alloc(void** p, size_t bytes, cudaStream_t s) {
         }
     }
     FC_CUDA_TRY(cudaMallocAsync(p, bytes ? bytes : 16, s));
+    count_alloc();
     return FC_OK;
 }
 
@@ -336,7 +337,10 @@ struct TempBufs {
         *out = nullptr;
         if (k == 12) return cudaErrorMemoryAllocation;
         cudaError_t e = cudaMallocAsync((void**)out, bytes, s);
-        if (e == cudaSuccess) p[k++] = *out;
+        if (e == cudaSuccess) {
+            p[k++] = *out;
+            count_alloc();
+        }
         return e;
     }
 };
@@ -422,6 +426,7 @@ fc_status upload(fc_graph* g, cudaStream_t s) {
     FC_CUDA_TRY(cudaMallocAsync(&d_in, entries * 4 + 4, s));
     FC_CUDA_TRY(cudaMallocAsync(&rowlen, (uint64_t)n * 4 + 4, s));
     FC_CUDA_TRY(cudaMallocAsync(&d_max, 8, s));
+    count_alloc(4);
     FC_TRY(dev_alloc((void**)&d->node_ptr, ((uint64_t)n + 1) * 4, s));
     FC_TRY(dev_alloc((void**)&d->adj, entries * 4 + 4, s));
     FC_TRY(dev_alloc((void**)&d->deg0, (uint64_t)n * L * 4 + 4, s));
@@ -436,6 +441,7 @@ fc_status upload(fc_graph* g, cudaStream_t s) {
         FC_CUDA_TRY(cudaGetLastError());
         FC_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, rowlen, d->node_ptr, n + 1, s));
         FC_CUDA_TRY(cudaMallocAsync(&tmp, tmp_bytes + 16, s));
+        count_alloc();
         // rowlen has n entries; entry n of the scan input must be 0
         FC_CUDA_TRY(cudaMemsetAsync(rowlen + n, 0, 4, s));
         FC_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, rowlen, d->node_ptr, n + 1, s));
@@ -475,6 +481,7 @@ void release_device(fc_graph* g, bool wait_home) {
     if (wait_home && d->home) cudaStreamSynchronize(d->home);
     cudaGetLastError();
     free_densest_state(d);
+    free_cell_index(d);
     dev_free(d->node_ptr, 0);
     dev_free(d->adj, 0);
     dev_free(d->deg0, 0);
@@ -522,6 +529,7 @@ void preload_kernels() {
         cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, buf, buf + 8, 8, (cudaStream_t)0) ==
             cudaSuccess &&
         cudaMalloc(&tmp, tmp_bytes + 16) == cudaSuccess) {
+        count_alloc(2);
         cudaMemset(buf, 0, 64);
         cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, buf, buf + 8, 8, (cudaStream_t)0);
         cudaDeviceSynchronize();

@@ -19,6 +19,7 @@ bool HostBuf<T>::alloc(size_t count) {
     size_t bytes = (count ? count : 1) * sizeof(T);
     if (cuda_available() && cudaMallocHost((void**)&p, bytes) == cudaSuccess) {
         pinned = true;
+        count_alloc();
     } else {
         cudaGetLastError();
         p = (T*)malloc(bytes);

@@ -1164,6 +1164,7 @@ static fc_status run_job(PeelJob& j, uint32_t maxL, uint32_t threads, cudaStream
     if (instrument) {
         FC_CUDA_TRY(cudaEventCreate(&e0));
         FC_CUDA_TRY(cudaEventCreate(&e1));
+        count_alloc(2);
     }
     // the run: clear the queues and the control block, then the launch --
     // captured as one CUDA graph when asked (and when the driver captures a
@@ -1626,6 +1627,241 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame(
     if (threadIdx.x == 0) levels[c] = k - k0;
 }
 
+// ---- the endgame on a thread-block cluster per column --------------------------
+//
+// The same levels as k_endgame, with a column's survivors spread over the CS
+// blocks of one cluster (CS a power of two, at most 16): survivor i lives on
+// block i % CS, at index i / CS of that block's degrees, count, alive flag
+// and lists, and every block reaches the others' shared memory directly
+// (distributed shared memory).  A level is a SCAN round, in which each block
+// scans its own survivors, then DRAIN rounds: in each, every block expands
+// the rows of its own nodes queued in the round before, and a removal it
+// causes is queued on the removed node's owner for the next round.  Rounds
+// are separated by cluster barriers.  Block 0 holds, per round (three of
+// them in rotation), the cluster-wide counts of nodes queued and of nodes a
+// scan kept; every block reads them right after the round's barrier, so all
+// blocks take the same decisions.  The queue of round r+1 is the other half
+// of a two-half queue, so a block never reads a slot another block may still
+// be writing.  Every loop is bounded as in k_endgame, and no block leaves
+// while another may still reach its shared memory.
+constexpr uint32_t EGC_MAX = 16;
+
+__device__ __forceinline__ uint32_t egc_dec16(uint32_t* w, uint32_t i) {
+    const uint32_t sh = (i & 1) * 16;
+    return (atomicSub(w + (i >> 1), 1u << sh) >> sh) & 0xFFFFu;
+}
+
+// shared bytes per survivor a block owns: degrees (L halves), count (a half),
+// alive flag, two lists and two queue halves (16-bit indices)
+static uint32_t egc_node_bytes(uint32_t L) { return 2 * L + 11; }
+static uint32_t egc_block_capacity(uint32_t L) {
+    const uint64_t fixed = 8ull * EG_THREADS + 256;
+    uint64_t cap = (EG_SMEM - fixed) / egc_node_bytes(L);
+    if (cap > 65535) cap = 65535;
+    return cap >= 1024 ? (uint32_t)cap : 0u;
+}
+static uint64_t egc_smem_bytes(uint32_t mo, uint32_t L) {
+    return 4ull * (((uint64_t)mo * L + 1) / 2 + (mo + 1) / 2 + 2ull * EG_THREADS) + mo + 4 +
+           8ull * mo + 16;
+}
+
+__global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
+    uint32_t cap, const uint32_t* __restrict__ ecnt, const uint32_t* __restrict__ rowptr,
+    const uint64_t* __restrict__ base, const uint32_t* __restrict__ H,
+    const uint32_t* __restrict__ l2g, const uint32_t* __restrict__ deg, uint32_t n, uint32_t L,
+    FastDiv divL, uint32_t* __restrict__ t, uint32_t col0, uint32_t k0, uint32_t max_level,
+    uint32_t* __restrict__ levels, uint32_t* __restrict__ err) {
+    extern __shared__ __align__(16) uint32_t sm[];
+    __shared__ uint32_t s_warp[33];
+    __shared__ uint32_t s_next, s_qe, s_pushed, s_tail[2];
+    __shared__ uint32_t s_cnt[3], s_kept[3];  // block 0's are the cluster's
+    __shared__ uint32_t s_rd_cnt, s_rd_kept;  // what this block read after a barrier
+    cg::cluster_group cl = cg::this_cluster();
+    const uint32_t CS = cl.num_blocks();
+    const uint32_t r = cl.block_rank();
+    const uint32_t lg = 31 - __clz(CS);  // CS = 1 << lg
+    const uint32_t c = blockIdx.x / CS;
+    const uint32_t m = min(ecnt[c], cap);
+    if (m == 0) return;  // the whole cluster leaves, before any barrier
+    const uint32_t lmd = col0 + c + 1;
+    const uint32_t mo_max = (m + CS - 1) / CS;               // the same layout on every block
+    const uint32_t mo = r < m ? (m - r + CS - 1) / CS : 0u;  // survivors r, r + CS, ...
+    const uint32_t* rp = rowptr + (uint64_t)c * (cap + 1);
+    const uint32_t* Hc = H + base[c];
+    const uint32_t* g_of = l2g + (uint64_t)c * cap;
+    uint32_t* tc = t + (uint64_t)c * n;
+    uint32_t* dw = sm;                                       // (mo_max * L + 1) / 2 words
+    uint32_t* cw = dw + ((uint64_t)mo_max * L + 1) / 2;      // (mo_max + 1) / 2 words
+    uint32_t* pre = cw + (mo_max + 1) / 2;                   // EG_THREADS words
+    uint32_t* rs = pre + EG_THREADS;                         // EG_THREADS words
+    uint8_t* alive = (uint8_t*)(rs + EG_THREADS);            // mo_max bytes
+    uint16_t* list0 = (uint16_t*)(((uintptr_t)(alive + mo_max) + 3) & ~(uintptr_t)3);
+    uint16_t* list1 = list0 + mo_max;
+    uint16_t* qh[2] = {list1 + mo_max, list1 + 2 * mo_max};  // the two queue halves
+    for (uint32_t i = threadIdx.x; i < ((uint64_t)mo_max * L + 1) / 2; i += blockDim.x) dw[i] = 0;
+    for (uint32_t i = threadIdx.x; i < (mo_max + 1) / 2; i += blockDim.x) cw[i] = 0;
+    if (threadIdx.x < 3) {
+        s_cnt[threadIdx.x] = 0;
+        s_kept[threadIdx.x] = 0;
+    }
+    if (threadIdx.x == 0) s_tail[0] = s_tail[1] = 0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < mo * L; i += blockDim.x) {
+        const uint32_t idx = i / L, l = i - idx * L;
+        const uint32_t d = deg[(uint64_t)c * n * L + (uint64_t)g_of[(idx << lg) + r] * L + l];
+        atomicOr(dw + (i >> 1), (d & 0xFFFFu) << ((i & 1) * 16));
+    }
+    for (uint32_t i = threadIdx.x; i < mo; i += blockDim.x) {
+        alive[i] = 1;
+        list0[i] = (uint16_t)i;
+    }
+    uint32_t* const r0_cnt = cl.map_shared_rank(s_cnt, 0);
+    uint32_t* const r0_kept = cl.map_shared_rank(s_kept, 0);
+    cl.sync();  // every block initialised before any reaches another
+    uint16_t* cur = list0;
+    uint16_t* nxt = list1;
+    uint32_t na = mo, k = k0, rho = 0;
+    bool failed = false;
+    for (;;) {
+        if (k > max_level) {  // k is the same on every block
+            failed = true;
+            break;
+        }
+        // SCAN round rho: removals queue locally in half (rho + 1) & 1
+        const uint32_t qn = (rho + 1) & 1;
+        if (threadIdx.x == 0) {
+            s_next = 0;
+            s_pushed = 0;
+            s_tail[0] = s_tail[1] = 0;  // no block queues remotely during a scan round
+        }
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < na; i += blockDim.x) {
+            const uint32_t x = cur[i];
+            if (!alive[x]) continue;
+            uint32_t cnt = 0;
+            for (uint32_t l = 0; l < L; l++) cnt += eg_get16(dw, x * L + l) >= k + 1;
+            if (cnt < lmd) {
+                alive[x] = 0;
+                tc[g_of[(x << lg) + r]] = k;
+                qh[qn][atomicAdd(&s_tail[qn], 1u)] = (uint16_t)x;
+            } else {
+                atomicOr(cw + (x >> 1), cnt << ((x & 1) * 16));  // the half was 0
+                nxt[atomicAdd(&s_next, 1u)] = (uint16_t)x;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            if (s_tail[qn]) atomicAdd(r0_cnt + rho % 3, s_tail[qn]);
+            if (s_next) atomicAdd(r0_kept + rho % 3, s_next);
+            if (r == 0) {
+                s_cnt[(rho + 1) % 3] = 0;
+                s_kept[(rho + 1) % 3] = 0;
+            }
+        }
+        cl.sync();
+        if (threadIdx.x == 0) {
+            s_rd_cnt = r0_cnt[rho % 3];
+            s_rd_kept = r0_kept[rho % 3];
+        }
+        __syncthreads();
+        const uint32_t kept = s_rd_kept;
+        // with no survivor left in the column the rows of this scan's
+        // removals name no node that could still change
+        uint32_t pushes = kept ? s_rd_cnt : 0u;
+        rho++;
+        // DRAIN rounds while the last round queued anything (bounded: every
+        // node is queued at most once per level)
+        for (uint32_t round = 0; pushes && round <= m; round++) {
+            const uint32_t qc = rho & 1, qp = (rho + 1) & 1;
+            if (threadIdx.x == 0) {
+                s_qe = s_tail[qc];
+                s_pushed = 0;
+            }
+            __syncthreads();
+            const uint32_t qe = s_qe;
+            for (uint32_t b0 = 0; b0 < qe; b0 += EG_THREADS) {
+                const uint32_t nb = min(EG_THREADS, qe - b0);
+                uint32_t len = 0, start = 0;
+                if (threadIdx.x < nb) {
+                    const uint32_t lid = ((uint32_t)qh[qc][b0 + threadIdx.x] << lg) + r;
+                    start = rp[lid];
+                    len = rp[lid + 1] - start;
+                }
+                uint32_t ex;
+                const uint32_t total = eg_block_scan(len, &ex, s_warp);
+                pre[threadIdx.x] = ex;
+                rs[threadIdx.x] = start;
+                __syncthreads();
+                uint32_t lo0 = 0;
+                for (uint32_t e0 = threadIdx.x; e0 < total; e0 += 4 * blockDim.x) {
+                    uint32_t slot[4];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const uint32_t e = e0 + q * blockDim.x;
+                        slot[q] = UNSET;
+                        if (e < total) {
+                            uint32_t lo = lo0, hi = nb - 1;
+                            while (lo < hi) {
+                                const uint32_t mid = (lo + hi + 1) >> 1;
+                                if (pre[mid] <= e) lo = mid;
+                                else hi = mid - 1;
+                            }
+                            lo0 = lo;
+                            slot[q] = Hc[rs[lo] + (e - pre[lo])];
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        if (slot[q] == UNSET) continue;
+                        const uint32_t u = divL.div(slot[q]);
+                        if (u >= m) continue;
+                        const uint32_t l = slot[q] - u * L;
+                        const uint32_t ow = u & (CS - 1), ui = u >> lg;
+                        uint8_t* const a_ow = cl.map_shared_rank(alive, ow);
+                        if (!a_ow[ui]) continue;
+                        const uint32_t old = egc_dec16(cl.map_shared_rank(dw, ow), ui * L + l);
+                        if (old == k + 1 && egc_dec16(cl.map_shared_rank(cw, ow), ui) == lmd) {
+                            a_ow[ui] = 0;
+                            tc[g_of[u]] = k;
+                            uint32_t* const t_ow = cl.map_shared_rank(s_tail, ow);
+                            const uint32_t pos = atomicAdd(t_ow + qp, 1u);
+                            uint16_t* const q_ow = cl.map_shared_rank(qh[qp], ow);
+                            q_ow[pos] = (uint16_t)ui;
+                            atomicAdd(&s_pushed, 1u);
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) {
+                s_tail[qc] = 0;  // this half is consumed; it takes round rho + 1's queue
+                if (s_pushed) atomicAdd(r0_cnt + rho % 3, s_pushed);
+                if (r == 0) {
+                    s_cnt[(rho + 1) % 3] = 0;
+                    s_kept[(rho + 1) % 3] = 0;
+                }
+            }
+            cl.sync();
+            if (threadIdx.x == 0) s_rd_cnt = r0_cnt[rho % 3];
+            __syncthreads();
+            pushes = s_rd_cnt;
+            rho++;
+        }
+        // counts are rebuilt by the next scan: clear the kept ones
+        for (uint32_t i = threadIdx.x; i < (mo_max + 1) / 2; i += blockDim.x) cw[i] = 0;
+        na = s_next;
+        uint16_t* tmp = cur;
+        cur = nxt;
+        nxt = tmp;
+        k++;
+        __syncthreads();
+        if (kept == 0) break;  // the cluster-wide count: the same on every block
+    }
+    if (failed && r == 0 && threadIdx.x == 0) atomicExch(err, 2u);
+    if (r == 0 && threadIdx.x == 0) levels[c] = k - k0;
+    cl.sync();  // no block leaves while another may still reach its shared memory
+}
+
 static SegP make_seg(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* table,
                      uint32_t* deg, uint32_t xbase) {
     SegP p{};
@@ -1663,9 +1899,54 @@ static int peel_sms() {
 // count array holds the local ids, the other alive list the local-to-global
 // map, the node queues the row offsets and the chunk queues the entries, or
 // a temporary buffer when they do not fit), then one block per column.
+// Blocks per column in the endgame: FC_PEEL_EG_CLUSTER (1, 2, 4, 8 or 16;
+// default 16), lowered until the device can run such a cluster of k_endgame_cl
+// blocks with the largest shared memory they may take; 1 is the one-block
+// k_endgame.  Decided once per device.
+static uint32_t eg_cluster_size() {
+    static int cached[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 1;
+    if (cached[dev]) return (uint32_t)cached[dev];
+    uint32_t want = env_u32("FC_PEEL_EG_CLUSTER", 16);
+    uint32_t cs = 1;
+    while (cs * 2 <= want && cs * 2 <= EGC_MAX) cs *= 2;
+    if (cs > 1 &&
+        (cudaFuncSetAttribute(k_endgame_cl, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)EG_SMEM) != cudaSuccess ||
+         cudaFuncSetAttribute(k_endgame_cl, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+             cudaSuccess))
+        cs = 1;
+    for (; cs > 1; cs /= 2) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = cs;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(cs);
+        cfg.blockDim = dim3(EG_THREADS);
+        cfg.dynamicSmemBytes = EG_SMEM;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int nclusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&nclusters, k_endgame_cl, &cfg) == cudaSuccess &&
+            nclusters >= 1)
+            break;
+    }
+    cudaGetLastError();
+    cached[dev] = (int)cs;
+    return cs;
+}
+
+// survivors one column's endgame can hold with cs blocks (0: off for this L)
+static uint32_t eg_column_capacity(uint32_t L, uint32_t cs) {
+    return cs > 1 ? cs * egc_block_capacity(L) : eg_capacity(L);
+}
+
 static fc_status endgame_run(const PeelJob& j, const PeelGraph& g, const PeelCtl& out, uint32_t col0,
-                             uint32_t ncols, uint32_t cap, cudaStream_t s, PeelStats* st,
-                             bool instrument) {
+                             uint32_t ncols, uint32_t cap, uint32_t cs, cudaStream_t s,
+                             PeelStats* st, bool instrument) {
     const uint32_t K = out.level, ac = out.alive_cur & 1u;
     const uint32_t nalive = out.alive_cnt[ac];
     const uint32_t capE = cap < g.n ? cap : g.n;
@@ -1689,6 +1970,7 @@ static fc_status endgame_run(const PeelJob& j, const PeelGraph& g, const PeelCtl
     if (instrument) {
         FC_CUDA_TRY(cudaEventCreate(&ev.e0));
         FC_CUDA_TRY(cudaEventCreate(&ev.e1));
+        count_alloc(2);
         FC_CUDA_TRY(cudaEventRecord(ev.e0, s));
     }
     FastDiv divN, divL;
@@ -1729,6 +2011,36 @@ static fc_status endgame_run(const PeelJob& j, const PeelGraph& g, const PeelCtl
             map, capE, rowptr, c->eg_base, H, &c->eg_err);
         static const cudaError_t attr_rc = cudaFuncSetAttribute(
             k_endgame, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)EG_SMEM);
+        if (cs > 1) {
+            // a cluster of cs blocks per column (k_endgame_cl)
+            const uint32_t mo = (mmax + cs - 1) / cs;
+            const uint64_t smem = egc_smem_bytes(mo, g.L);
+            if (smem > EG_SMEM || mo > 65535) {
+                rc = FC_ERR_DEVICE;
+            } else {
+                cudaLaunchConfig_t cfg = {};
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeClusterDimension;
+                at[0].val.clusterDim.x = cs;
+                at[0].val.clusterDim.y = 1;
+                at[0].val.clusterDim.z = 1;
+                cfg.gridDim = dim3(ncols * cs);
+                cfg.blockDim = dim3(EG_THREADS);
+                cfg.dynamicSmemBytes = (size_t)smem;
+                cfg.stream = s;
+                cfg.attrs = at;
+                cfg.numAttrs = 1;
+                const cudaError_t le = cudaLaunchKernelEx(
+                    &cfg, k_endgame_cl, capE, (const uint32_t*)c->eg_cnt, (const uint32_t*)rowptr,
+                    (const uint64_t*)c->eg_base, (const uint32_t*)H, (const uint32_t*)l2g, deg, g.n,
+                    g.L, divL, j.seg0.t, col0, K + 1, j.max_level, c->eg_levels, &c->eg_err);
+                count_launch(5);
+                if (le != cudaSuccess) {
+                    set_last_cuda_error(le, "k_endgame_cl", __FILE__, __LINE__);
+                    rc = FC_ERR_DEVICE;
+                }
+            }
+        } else {
         const uint64_t smem =
             4ull * (((uint64_t)mmax * g.L + 1) / 2 + (mmax + 1) / 2 + 2ull * EG_THREADS) + mmax + 4 +
             6ull * mmax + 16;
@@ -1744,6 +2056,7 @@ static fc_status endgame_run(const PeelJob& j, const PeelGraph& g, const PeelCtl
                 set_last_cuda_error(le, "k_endgame", __FILE__, __LINE__);
                 rc = FC_ERR_DEVICE;
             }
+        }
         }
     }
     uint32_t tail[EG_MAX_COLS + 1];  // eg_levels then eg_err
@@ -1785,13 +2098,14 @@ fc_status peel_run(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* 
     j.seg_xbase = nullptr;
     j.nseg = 1;
     j.max_level = g.max_level;
-    const uint32_t cap = (endgame && ncols <= EG_MAX_COLS && env_u32("FC_PEEL_ENDGAME", 1))
-                             ? eg_capacity(g.L) : 0u;
+    const bool eg = endgame && ncols <= EG_MAX_COLS && env_u32("FC_PEEL_ENDGAME", 1);
+    const uint32_t cs = eg ? eg_cluster_size() : 1u;
+    const uint32_t cap = eg ? eg_column_capacity(g.L, cs) : 0u;
     j.stop_alive = cap;
     PeelCtl out;
     FC_TRY(run_job<false>(j, g.L, default_threads(), s, st, instrument, col0, ncols, nullptr, &out));
     if (!out.stopped) return FC_OK;
-    return endgame_run(j, g, out, col0, ncols, cap, s, st, instrument);
+    return endgame_run(j, g, out, col0, ncols, cap, cs, s, st, instrument);
 }
 
 uint64_t peel_batch_ws_bytes(const std::vector<PeelSegSpec>& specs) {

@@ -386,6 +386,7 @@ struct fc_server {
     void lane_loop() {
         cudaStream_t s = nullptr;
         cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        fc::count_alloc(2);  // the stream and the staging buffer
         // this lane's copies go through its own pinned buffer
         fc::Staging stage;
         if (cudaHostAlloc(&stage.p, 16u << 20, cudaHostAllocDefault) == cudaSuccess)

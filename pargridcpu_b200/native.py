@@ -28,7 +28,8 @@ EXPORTS = [
     "fc_densest", "fc_densest_members", "fc_cell_members", "fc_cells", "fc_coreindex_range",
     "fc_cells_range", "fc_batch_run", "fc_server_create",
     "fc_server_submit", "fc_server_wait", "fc_server_query", "fc_server_destroy", "fc_graph_stats",
-    "fc_launch_count", "fc_coreindex_fixed_scratch",
+    "fc_launch_count", "fc_coreindex_fixed_scratch", "fc_cell_index", "fc_cells_members",
+    "fc_mlcd_query", "fc_probe_atomics", "fc_alloc_count",
 ]
 
 
@@ -142,6 +143,11 @@ def lib():
         "fc_graph_stats": ([p, p], i32),
         "fc_launch_count": ([], u64),
         "fc_coreindex_fixed_scratch": ([u32, u32, u64, p, p, p, p, p], i32),
+        "fc_cell_index": ([p, p, p, p, u64, C.POINTER(u64), p], i32),
+        "fc_cells_members": ([p, p, p, u32, i32, p, p, u64, p], i32),
+        "fc_mlcd_query": ([p, u32, u32, p, p, u32, p, p, u64, p], i32),
+        "fc_probe_atomics": ([u64, u64, C.POINTER(C.c_double), p], i32),
+        "fc_alloc_count": ([], u64),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -15,7 +15,13 @@ Inputs are not stored: they are regenerated from the seeds in
 ``manifest.json`` by ``pargridcpu_b200.synth`` and checked against the stored
 SHA-256 of their raw pairs.  Loader edge cases are stored as raw file text.
 
-Usage: python tests/golden/make_golden.py [--with-c3]
+The batched mix (256 graphs, seed 404) and one large serving graph (n=2.6M,
+L=24) are pinned the same way as c3, by hashes: ``--with-c4`` writes
+``c4_mix.json`` (per graph: input and table SHA-256, per-lambda maxima, the
+WdsList result for beta = 1 and its node set's SHA-256), ``--with-c5``
+``c5_large.json`` (the same for the large graph).
+
+Usage: python tests/golden/make_golden.py [--with-c3] [--with-c4] [--with-c5]
 Needs the reference checkout (oracle/Makefile's REF) to build the checker.
 """
 from __future__ import annotations
@@ -190,16 +196,87 @@ def make_c3(manifest):
     print("c3", n, L, flush=True)
 
 
+def _pin_graph(args):
+    """One graph's reference outputs as hashes (a worker of make_c4/make_c5)."""
+    params, tag, threads = args
+    g = synth._make(params)
+    os.makedirs(SCRATCH, exist_ok=True)
+    fcg = os.path.join(SCRATCH, f"{tag}.fcg")
+    synth.write_fcg(g, fcg)
+    og = O.OracleGraph(g.layers)
+    n, L = og.n, og.L
+    table = O.ref_table(fcg, L, n, "table", threads=threads)
+    w = O.ref_wds(fcg, 1.0, threads=threads)
+    os.remove(fcg)
+    win = [c for c in w["cells"] if (c[0], c[1]) == (w.get("k", 0), w.get("lmd", 0))]
+    return dict(name=params["name"], n=int(n), L=int(L), pairs_sha256=pairs_sha(g.layers),
+                entries=int(og.layer_m().sum()),
+                table_sha256=hashlib.sha256(np.ascontiguousarray(table).tobytes()).hexdigest(),
+                kmax=[int(x) for x in table.max(axis=1)] if n else [0] * L,
+                k=int(w.get("k", 0)), lmd=int(w.get("lmd", 0)), length=int(w.get("length", 0)),
+                max_density_f=float(np.float32(w.get("max_density_f", 0.0))),
+                density=float(win[0][3]) if win else 0.0,
+                lstar=int(win[0][4]) if win else 0,
+                n_cells=len(w["cells"]),
+                nodes_sha256=hashlib.sha256(np.ascontiguousarray(w["nodes"], dtype="<u4")
+                                            .tobytes()).hexdigest())
+
+
+C4_MIX = dict(count=256, seed=404)
+
+
+def make_c4(workers):
+    """The full 256-graph mix (batch_params(256, seed=404)): every graph's
+    table and densest result from the reference, as hashes."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    params = synth.batch_params(**C4_MIX)
+    jobs = [(p, f"c4_{i}", 1) for i, p in enumerate(params)]
+    # the largest graphs first, so the pool ends together
+    order = sorted(range(len(jobs)), key=lambda i: -params[i]["n"] * params[i]["n_layers"]
+                   * params[i]["m_per_layer"] / max(1, params[i]["n"]))
+    out = [None] * len(jobs)
+    with ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+        futs = {i: ex.submit(_pin_graph, jobs[i]) for i in order}
+        for i in order:
+            out[i] = futs[i].result()
+            print("c4", i, out[i]["n"], out[i]["L"], flush=True)
+    with open(os.path.join(HERE, "c4_mix.json"), "w") as f:
+        json.dump(dict(generator=dict(C4_MIX, fn="synth.batch_params"), beta=1.0, graphs=out),
+                  f, indent=0)
+
+
+def make_c5(workers):
+    """The serving configuration's large graph (CONFIGS['c5_large'], the
+    first of the seeds the benchmark draws: seed + 0)."""
+    c = synth.CONFIGS["c5_large"]
+    p = dict(n=c["n"], n_layers=c["L"], m_per_layer=c["m"], gamma=c["gamma"], copy=c["copy"],
+             seed=c["seed"], name="large0")
+    r = _pin_graph((p, "c5", workers))
+    with open(os.path.join(HERE, "c5_large.json"), "w") as f:
+        json.dump(dict(params=p, beta=1.0, graph=r), f, indent=1)
+    print("c5", r["n"], r["L"], flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--with-c3", action="store_true")
+    ap.add_argument("--with-c4", action="store_true")
+    ap.add_argument("--with-c5", action="store_true")
     ap.add_argument("--only", default=None)
+    ap.add_argument("--workers", type=int, default=os.cpu_count() or 1)
     a = ap.parse_args()
     subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", "liboracle.so"],
                    check=True, stdout=subprocess.DEVNULL)
     mpath = os.path.join(HERE, "manifest.json")
     manifest = json.load(open(mpath)) if os.path.exists(mpath) else {}
     manifest["_generator"] = dict(mix=MIX_PARAMS, betas=list(BETAS))
+    if a.with_c4 or a.with_c5:
+        if a.with_c4:
+            make_c4(a.workers)
+        if a.with_c5:
+            make_c5(a.workers)
+        return
     for name in CASES:
         if a.only and name != a.only:
             continue

@@ -104,3 +104,40 @@ def test_batch_with_empty_graph_and_empty_layer():
         assert np.array_equal(tables[i], t)
         assert (results[i]["k"], results[i]["lmd"], results[i]["length"], results[i]["density"]) == \
             (o["k"], o["lmd"], o["length"], o["density"])
+
+
+def _c4_graphs():
+    """The full 256-graph mix (seed 404), regenerated from its seeds on the
+    host's cores, and its pinned reference results."""
+    import hashlib
+    import json
+    import multiprocessing as mp
+    import os
+    from concurrent.futures import ProcessPoolExecutor
+    fx = json.load(open(os.path.join(G.GOLDEN, "c4_mix.json")))
+    params = synth.batch_params(**{k: fx["generator"][k] for k in ("count", "seed")})
+    with ProcessPoolExecutor(os.cpu_count() or 1, mp_context=mp.get_context("spawn")) as ex:
+        gens = list(ex.map(synth._make, params, chunksize=1))
+    for gen, f in zip(gens, fx["graphs"]):
+        assert G.pairs_sha(gen.layers) == f["pairs_sha256"], f["name"]
+    return gens, fx["graphs"], hashlib
+
+
+def test_c4_mix_batched_equals_the_reference():
+    """All 256 graphs of the mix in one batched run: every table (SHA-256)
+    and every densest result equal the reference's own (tests/golden/
+    c4_mix.json, made by the reference's get_index2 and WdsList)."""
+    gens, fx, hashlib = _c4_graphs()
+    graphs = [MultilayerGraph.from_pairs(g.layers) for g in gens]
+    tables, results, rep = batch_run(graphs, beta=1.0)
+    for i, (g, t, r, f) in enumerate(zip(graphs, tables, results, fx)):
+        assert (g.n, g.L) == (f["n"], f["L"]), i
+        assert hashlib.sha256(np.ascontiguousarray(t).tobytes()).hexdigest() == \
+            f["table_sha256"], f"graph {i}: table"
+        assert (r["k"], r["lmd"], r["length"]) == (f["k"], f["lmd"], f["length"]), i
+        assert np.float32(r["max_density_f"]) == np.float32(f["max_density_f"]), i
+        if r["k"]:
+            assert r["density"] == f["density"] and r["lstar"] == f["lstar"], i
+            nodes, _ = g.densest_members(r)
+            assert hashlib.sha256(np.ascontiguousarray(nodes, dtype="<u4").tobytes()) \
+                .hexdigest() == f["nodes_sha256"], i

@@ -98,3 +98,60 @@ def test_harness_on_random_text_dataset():
         got = og.densest(ref, 1.0)
         assert (got["k"], got["lmd"], got["length"]) == (w["k"], w["lmd"], w["length"])
         assert os.path.exists(os.path.join(d, "__vtx_map.txt"))
+
+
+# ---- the query-time restatements (Util/CoreIndexTime.h, Util/CheckMLCDTime.h)
+
+@pytest.mark.parametrize("name", ["c1_small", "tiny_dirty", "layers33", "mix0"])
+def test_query_restatements_answer_the_reference_cells(name):
+    """Every cell the reference's own run reported, asked back through the
+    getResCore / getResCoreOffline restatements, has the reference's size."""
+    exp = G.expected(name)
+    table = exp["table"]
+    cells = exp["b1.0_cells"]
+    ks = [int(c[0]) for c in cells] + [0, int(table.max()) + 1]
+    lmds = [int(c[1]) for c in cells] + [1, table.shape[0]]
+    scan = O.cells_scan(table, ks, lmds)
+    srt = O.cells_sorted(table, ks, lmds)
+    for i, c in enumerate(cells):
+        assert len(scan[i]) == c[2]
+    assert len(scan[-2]) == table.shape[1] and len(scan[-1]) == 0
+    for a, b, k, lmd in zip(scan, srt, ks, lmds):
+        assert np.array_equal(a, np.nonzero(table[lmd - 1] >= k)[0])
+        assert np.array_equal(np.sort(b), a)
+        assert np.all(np.diff(table[lmd - 1][b].astype(np.int64)) >= 0)
+
+
+def test_mlcd_restatement():
+    rng = np.random.default_rng(5)
+    cores = rng.integers(0, 9, size=(700, 6)).astype(np.uint32)
+    cores[::37, 2] = 0xFFFFFFFF  # a negative int read as unsigned, as the reference compares
+    ks = [0, 1, 3, 5, 8, 9, 4, 2]
+    lmds = [0, 1, 2, 6, 1, 1, 7, 3]
+    got = O.mlcd_query(cores, ks, lmds)
+    for k, lmd, g in zip(ks, lmds, got):
+        want = np.nonzero((cores >= k).sum(axis=1) >= max(lmd, 1))[0]
+        assert np.array_equal(g, want)
+
+
+def test_oracle_matches_reference_on_the_c4_mix_sample():
+    """The smallest graphs of the 256-graph mix against the reference's own
+    results for them (tests/golden/c4_mix.json)."""
+    import hashlib
+    import json
+    from pargridcpu_b200 import synth
+    fx = json.load(open(os.path.join(G.GOLDEN, "c4_mix.json")))
+    params = synth.batch_params(**{k: fx["generator"][k] for k in ("count", "seed")})
+    small = sorted(range(len(params)), key=lambda i: fx["graphs"][i]["entries"])[:6]
+    for i in small:
+        f = fx["graphs"][i]
+        gen = synth._make(params[i])
+        assert G.pairs_sha(gen.layers) == f["pairs_sha256"]
+        og = O.OracleGraph(gen.layers)
+        t = og.coreindex()
+        assert hashlib.sha256(np.ascontiguousarray(t).tobytes()).hexdigest() == f["table_sha256"]
+        d = og.densest(t, 1.0, with_cells=False)
+        assert (d["k"], d["lmd"], d["length"]) == (f["k"], f["lmd"], f["length"])
+        assert np.float32(d["max_density_f"]) == np.float32(f["max_density_f"])
+        if d["k"]:
+            assert d["density"] == f["density"]

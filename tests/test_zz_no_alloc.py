@@ -19,7 +19,7 @@ from pargridcpu_b200 import MultilayerGraph, native, synth
 
 pytestmark = pytest.mark.gpu
 
-FC_OK, FC_ERR_TOO_LARGE = 0, 8
+FC_OK, FC_ERR_INVALID, FC_ERR_TOO_LARGE = 0, 7, 8
 
 
 def node_major(g):
@@ -110,3 +110,52 @@ def test_fixed_scratch_rejects_oversize():
     # one column of 50M nodes x 8 layers needs far more than 64 MiB: rejected
     # on the host, before anything reads these (too small) buffers
     assert _call(50_000_000, 8, 1000, tiny, tiny, tiny, tiny) == FC_ERR_TOO_LARGE
+
+
+def test_fixed_scratch_allocates_nothing():
+    """The property the entry point exists for: once a device is set up (its
+    first call), calls create no device or pinned allocation, stream or
+    event (the library's own count) and take no device memory."""
+    import torch
+    gen = synth.chung_lu_graph(20_000, 5, 60_000, 2.3, 0.4, 9093)
+    g = MultilayerGraph.from_pairs(gen.layers)
+    ref = g.coreindex()
+    node_ptr, slots, deg0 = node_major(g)
+    d_ptr, d_adj, d_deg0 = _dev(node_ptr), _dev(slots), _dev(deg0)
+    out = torch.empty((g.L, g.n), dtype=torch.int32, device="cuda")
+    assert _call(g.n, g.L, len(slots), d_ptr, d_adj, d_deg0, out) == FC_OK  # set-up call
+    torch.cuda.synchronize()
+    allocs = native.lib().fc_alloc_count()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(2):
+        out.fill_(7)
+        assert _call(g.n, g.L, len(slots), d_ptr, d_adj, d_deg0, out) == FC_OK
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), ref)
+    assert native.lib().fc_alloc_count() == allocs
+    assert torch.cuda.mem_get_info()[0] == free0
+
+
+def test_fixed_scratch_rejects_a_malformed_csr():
+    """A CSR the peel could not index safely is refused on the device before
+    the peel runs, and the next well-formed call is unaffected."""
+    import torch
+    gen = synth.erdos_renyi_graph(150, 12, 0.02, 0.1, 9094)
+    g = MultilayerGraph.from_pairs(gen.layers)
+    ref = g.coreindex()
+    node_ptr, slots, deg0 = node_major(g)
+    n, L, e = g.n, g.L, len(slots)
+    out = torch.empty((L, n), dtype=torch.int32, device="cuda")
+    bad_slot = slots.copy()
+    bad_slot[e // 2] = n * L            # names no degree counter
+    bad_ptr = node_ptr.copy()
+    bad_ptr[n // 2] = bad_ptr[n // 2 + 1] + 1  # a row of negative length
+    short_ptr = node_ptr.copy()
+    short_ptr[n] = e - 1                # ends before the entries do
+    for p, s_ in ((node_ptr, bad_slot), (bad_ptr, slots), (short_ptr, slots)):
+        rc = _call(n, L, e, _dev(p), _dev(s_), _dev(deg0), out)
+        torch.cuda.synchronize()
+        assert rc == FC_ERR_INVALID
+    assert _call(n, L, e, _dev(node_ptr), _dev(slots), _dev(deg0), out) == FC_OK
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), ref)
