@@ -997,10 +997,10 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j, volatile DrainBloc
     }
 }
 
-// T threads per block, 1024 threads resident per SM (512 x 2 or 1024 x 1):
-// at most 64 registers a thread.
-template <int G, int T, bool MULTI>
-__global__ void __launch_bounds__(T, 1024 / T) k_peel(PeelJob j) {
+// T threads per block, BPS blocks resident per SM: 1024 threads (512 x 2 or
+// 1024 x 1) at most 64 registers a thread; 512 x 3 at most 42.
+template <int G, int T, bool MULTI, int BPS = 1024 / T>
+__global__ void __launch_bounds__(T, BPS) k_peel(PeelJob j) {
     __shared__ DrainBlock s_drain;
     phase_init<MULTI>(j);
     if (!grid_barrier(j)) return;
@@ -1043,25 +1043,30 @@ uint32_t peel_columns_per_group(const DeviceGraph* d) {
     return (uint32_t)cols;
 }
 
-template <int G, int T, bool MULTI>
+template <int G, int T, bool MULTI, int BPS = 1024 / T>
 static fc_status launch_t(PeelJob& j, cudaStream_t s) {
     int dev = 0, sms = 0, occ = 0;
     FC_CUDA_TRY(cudaGetDevice(&dev));
     FC_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    FC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_peel<G, T, MULTI>, T, 0));
+    FC_CUDA_TRY(
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_peel<G, T, MULTI, BPS>, T, 0));
     if (occ < 1) return FC_ERR_DEVICE;
-    uint32_t want_occ = env_u32("FC_PEEL_BLOCKS_PER_SM", 1024 / T);
+    uint32_t want_occ = env_u32("FC_PEEL_BLOCKS_PER_SM", BPS);
     if (want_occ >= 1 && (int)want_occ < occ) occ = (int)want_occ;
     if (j.max_sms && (int)j.max_sms < sms) sms = (int)j.max_sms;
     dim3 grid(sms * occ), block(T);
     void* args[] = {&j};
-    FC_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_peel<G, T, MULTI>, grid, block, args, 0, s));
+    FC_CUDA_TRY(cudaLaunchCooperativeKernel((void*)k_peel<G, T, MULTI, BPS>, grid, block, args, 0,
+                                            s));
     return FC_OK;
 }
 
+// FC_PEEL_OCC=3 with 512-thread blocks: three blocks per SM (1536 threads,
+// 42 registers each) instead of two
 template <int G, bool MULTI>
 static fc_status launch_g(PeelJob& j, uint32_t threads, cudaStream_t s) {
     if (threads == 1024) return launch_t<G, 1024, MULTI>(j, s);
+    if (env_u32("FC_PEEL_OCC", 2) == 3) return launch_t<G, 512, MULTI, 3>(j, s);
     return launch_t<G, 512, MULTI>(j, s);
 }
 
