@@ -202,3 +202,28 @@ def test_c3_full_size():
         assert np.array_equal(dens, exp[f"{tag}_cell_density"])
         nodes, _ = g.densest_members(r)
         assert np.array_equal(nodes, exp[f"{tag}_nodes"])
+
+
+def test_c5_large_graph():
+    """The serving configuration's large graph (2.6M nodes, 24 layers, 48M
+    edges, the first seed the serving benchmark draws): table hash, per-lambda
+    maxima and densest result against the reference's own output
+    (tests/golden/c5_large.json); containment across lambda holds."""
+    import json
+    fx = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "c5_large.json")))
+    f = fx["graph"]
+    gen = synth._make(fx["params"])
+    assert G.pairs_sha(gen.layers) == f["pairs_sha256"]
+    g = MultilayerGraph.from_pairs(gen.layers)
+    assert (g.n, g.L) == (f["n"], f["L"])
+    table = g.coreindex()
+    assert [int(x) for x in table.max(axis=1)] == f["kmax"]
+    assert hashlib.sha256(np.ascontiguousarray(table).tobytes()).hexdigest() == f["table_sha256"]
+    assert np.all(table[1:] <= table[:-1])
+    r = g.densest([fx["beta"]])[0]
+    assert (r["k"], r["lmd"], r["length"], r["lstar"]) == (f["k"], f["lmd"], f["length"], f["lstar"])
+    assert r["density"] == f["density"]
+    assert np.float32(r["max_density_f"]) == np.float32(f["max_density_f"])
+    nodes, _ = g.densest_members(r)
+    assert hashlib.sha256(np.ascontiguousarray(nodes, dtype="<u4").tobytes()).hexdigest() == \
+        f["nodes_sha256"]
