@@ -74,6 +74,9 @@ def parse_args():
     ap.add_argument("--requests", type=int, default=150, help="c5: requests per rate")
     ap.add_argument("--pool", type=int, default=64, help="c5: distinct small graphs")
     ap.add_argument("--beta", type=float, default=1.0)
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="c1/c3: n and edges per layer scaled by this factor (studies only; "
+                         "the named configuration is scale 1)")
     ap.add_argument("--ref-reps", type=int, default=0,
                     help="runs of each reference method in the protocol (0: 3 for the "
                          "reference arm, 1 for our arm's cpu_baseline)")
@@ -83,12 +86,14 @@ def parse_args():
     return ap.parse_args()
 
 
-def describe(name):
+def describe(name, scale=1.0):
     from pargridcpu_b200 import synth
     c = synth.CONFIGS[name]
     if c["kind"] == "chung_lu":
-        return (f"{name}: Chung-Lu n={c['n']:,} L={c['L']} {c['m']:,} edges/layer gamma={c['gamma']}"
-                f" copy={c['copy']} seed={c['seed']}; full fcgrid + densest(beta)")
+        n, m = max(16, int(c["n"] * scale)), max(8, int(c["m"] * scale))
+        return (f"{name}{'' if scale == 1.0 else f' scaled {scale}'}: Chung-Lu n={n:,} L={c['L']} "
+                f"{m:,} edges/layer gamma={c['gamma']} copy={c['copy']} seed={c['seed']}; "
+                f"full fcgrid + densest(beta)")
     return (f"{name}: Erdos-Renyi n={c['n']} L={c['L']} p~U[{c['p_lo']},{c['p_hi']}] "
             f"seed={c['seed']}; full fcgrid + densest(beta)")
 
@@ -98,7 +103,7 @@ def config_dict(args, n, L, m2, world):
     split = ("single process" if world == 1 else
              f"lambda columns split over {world} ranks" if args.split == "lambda" else
              f"{world} replicas")
-    return {"workload": describe(args.workload), "n": n, "L": L, "directed_entries": m2,
+    return {"workload": describe(args.workload, args.scale), "n": n, "L": L, "directed_entries": m2,
             "edge_visits_per_step": L * m2, "beta": args.beta,
             "l2": (f"inputs larger than L2 (adjacency {m2 * 4 / 2**20:.0f} MiB > 126 MiB)"
                    if m2 * 4 > L2_BYTES else "inputs smaller than L2 (no flush)"),
@@ -278,7 +283,7 @@ def run_reference(args, world, rank):
     if not _harness():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_harness not built"}))
         return
-    g = synth.config_graph(args.workload)
+    g = synth.config_graph(args.workload, scale=args.scale)
     import oracle as O  # the checker package: the loader restatement gives n and M
     og = O.OracleGraph(g.layers)
     L, n = og.L, og.n
@@ -334,7 +339,7 @@ def run_ours(args, world, rank, local):
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    gen = synth.config_graph(args.workload)
+    gen = synth.config_graph(args.workload, scale=args.scale)
     g = MultilayerGraph.from_pairs(gen.layers)
     n, L = g.n, g.L
     m2 = int(g.layer_m().sum())
@@ -481,7 +486,8 @@ def run_ours(args, world, rank, local):
     launch_ms = statistics.mean(p / max(1, q) for p, q in zip(peel_ms, peel_launches))
     achieved = bytes_per_launch / (launch_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
-    traffic, atom_sectors = committed_traffic(args.workload)
+    traffic, atom_sectors = (committed_traffic(args.workload) if args.scale == 1.0
+                             else (None, None))
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "traffic": traffic,
             "kernel": "k_peel + endgame (k_eg_index, k_eg_scan, k_eg_fill, k_eg_fill_big, "

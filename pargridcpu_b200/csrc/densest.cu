@@ -131,14 +131,31 @@ __global__ void k_node_hist(const uint32_t* __restrict__ table, uint32_t n,
 }
 
 // Edge histogram for lambda columns [lam0, lam0 + nl).  Each warp takes a
-// contiguous slice of the entry array; lanes stride through it and track the
-// source node by advancing along node_ptr.  Bins live in shared memory when
-// they fit (`sh_ok`), else in global memory.
+// contiguous slice of the entry array, 32 consecutive entries at a time (one
+// per lane), and tracks each lane's source node by advancing along node_ptr.
+// Bins live in shared memory when they fit (`sh_ok`), else in global memory.
+// The entry (v, u, l) adds one to bin (l, min(core(v), core(u))) per column.
+// Where core(u) >= core(v) the key is v's own core, the same for every entry
+// of a run of adjacent lanes with the same (v, l): the run's first lane adds
+// their number with one atomic, so the hottest bins (low-core nodes, whose
+// neighbours mostly have higher cores) take one atomic per run instead of
+// one per entry.  The other entries add one each.
+__device__ __forceinline__ void edge_bin_add(uint32_t* sh, uint32_t* H, bool sh_ok, uint32_t soff,
+                                             uint64_t hbase, uint32_t l, uint32_t km1,
+                                             uint32_t key, uint32_t cnt) {
+    if (sh_ok) atomicAdd(sh + soff + l * km1 + key, cnt);
+    else atomicAdd(H + hbase + (uint64_t)l * km1 + key, cnt);
+}
+
+// V4: the group is four columns starting at a multiple of four with L a
+// multiple of four, so a node's four core values are one aligned 16-byte
+// load.  runs = 0 adds every entry with its own atomic (no run counting).
+template <bool V4>
 __global__ void k_edge_hist(const uint32_t* __restrict__ node_ptr, const uint32_t* __restrict__ adj,
                             uint32_t n, uint32_t L, uint64_t entries, FastDiv divL,
                             const uint32_t* __restrict__ coreT, uint32_t lam0, uint32_t nl,
                             const uint64_t* __restrict__ hbase, const uint32_t* __restrict__ kmax,
-                            uint32_t* __restrict__ H, uint32_t sh_words, int sh_ok) {
+                            uint32_t* __restrict__ H, uint32_t sh_words, int sh_ok, int runs) {
     extern __shared__ uint32_t sh[];
     __shared__ uint32_t soff[64];  // per column in the group: offset into sh
     if (threadIdx.x == 0) {
@@ -156,32 +173,75 @@ __global__ void k_edge_hist(const uint32_t* __restrict__ node_ptr, const uint32_
     const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint64_t per = (entries + nwarps - 1) / nwarps;
     const uint64_t e0 = gw * per, e1 = min(entries, e0 + per);
-    if (e0 < e1) {
+    if (e0 < e1) {  // warp-uniform
         // source node of this lane's first entry: last v with node_ptr[v] <= e
-        uint64_t e = e0 + lane;
         uint32_t lo = 0, hi = n;  // node_ptr[lo] <= e < node_ptr[hi]
-        if (e < e1) {
+        if (e0 + lane < e1) {
             while (hi - lo > 1) {
                 uint32_t mid = (lo + hi) >> 1;
-                if (node_ptr[mid] <= e) lo = mid;
+                if (node_ptr[mid] <= e0 + lane) lo = mid;
                 else hi = mid;
             }
         }
         uint32_t v = lo;
-        for (; e < e1; e += 32) {
-            while (node_ptr[v + 1] <= e) v++;
-            const uint32_t slot = adj[e];
-            const uint32_t u = divL.div(slot);
-            const uint32_t l = slot - u * L;
+        uint32_t next_row = node_ptr[v + 1];
+        uint4 A = V4 ? *(const uint4*)(coreT + (uint64_t)v * L + lam0) : make_uint4(0, 0, 0, 0);
+        const uint32_t below = (2u << lane) - 1u;  // lanes 0..lane (all 32 for lane 31)
+        for (uint64_t b0 = e0; b0 < e1; b0 += 32) {
+            const uint64_t e = b0 + lane;
+            const bool valid = e < e1;
+            uint32_t u = 0, l = 0;
+            if (valid) {
+                if (next_row <= e) {
+                    do v++;
+                    while (node_ptr[v + 1] <= e);
+                    next_row = node_ptr[v + 1];
+                    if (V4) A = *(const uint4*)(coreT + (uint64_t)v * L + lam0);
+                }
+                const uint32_t slot = adj[e];
+                u = divL.div(slot);
+                l = slot - u * L;
+            }
+            // runs of adjacent lanes with the same (v, l); v * L + l < n * L < 2^32
+            bool leader = true;
+            uint32_t run = 0;
+            if (runs) {
+                const uint32_t vl = valid ? v * L + l : 0xFFFFFFFFu;
+                const uint32_t prev = __shfl_up_sync(0xffffffffu, vl, 1);
+                const uint32_t starts = __ballot_sync(0xffffffffu, lane == 0 || prev != vl);
+                leader = (starts >> lane) & 1u;
+                const uint32_t above = starts & ~below;  // the next run's first lane, if any
+                const uint32_t run_end = above ? (uint32_t)__ffs(above) - 1u : 32u;
+                run = (run_end == 32u ? 0xFFFFFFFFu : ((1u << run_end) - 1u)) &
+                      ~((1u << lane) - 1u);  // this lane's run, when it leads it
+            }
+            uint4 B = make_uint4(0, 0, 0, 0);
+            if (V4 && valid && (A.x | A.y | A.z | A.w))
+                B = *(const uint4*)(coreT + (uint64_t)u * L + lam0);
             for (uint32_t i = 0; i < nl; i++) {
-                const uint32_t a = coreT[(uint64_t)v * L + lam0 + i];
-                if (!a) continue;
-                const uint32_t b = coreT[(uint64_t)u * L + lam0 + i];
-                const uint32_t key = min(a, b);
-                if (!key) continue;
+                uint32_t a = 0, b = 0;
+                if (V4) {
+                    a = i == 0 ? A.x : i == 1 ? A.y : i == 2 ? A.z : A.w;
+                    b = i == 0 ? B.x : i == 1 ? B.y : i == 2 ? B.z : B.w;
+                    if (!valid) a = 0;
+                } else if (valid) {
+                    a = coreT[(uint64_t)v * L + lam0 + i];
+                    if (a) b = coreT[(uint64_t)u * L + lam0 + i];
+                }
                 const uint32_t km1 = kmax[lam0 + i] + 1;
-                if (sh_ok) atomicAdd(sh + soff[i] + l * km1 + key, 1u);
-                else atomicAdd(H + hbase[lam0 + i] + (uint64_t)l * km1 + key, 1u);
+                if (runs) {
+                    const bool own = a && b >= a;  // key = a, counted by the run
+                    const uint32_t own_mask = __ballot_sync(0xffffffffu, own);
+                    if (leader && a) {
+                        const uint32_t cnt = __popc(own_mask & run);
+                        if (cnt) edge_bin_add(sh, H, sh_ok, soff[i], hbase[lam0 + i], l, km1, a, cnt);
+                    }
+                    if (a && b && b < a)
+                        edge_bin_add(sh, H, sh_ok, soff[i], hbase[lam0 + i], l, km1, b, 1u);
+                } else {
+                    const uint32_t key = min(a, b);
+                    if (key) edge_bin_add(sh, H, sh_ok, soff[i], hbase[lam0 + i], l, km1, key, 1u);
+                }
             }
         }
     }
@@ -404,8 +464,11 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st, uint32_t lo, uint32
         const uint32_t SH_WORDS = 48 * 1024;  // 192 KB
         // once per process (thread-safe static initialisation)
         static const cudaError_t attr_rc = cudaFuncSetAttribute(
-            k_edge_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, SH_WORDS * 4);
+            k_edge_hist<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SH_WORDS * 4);
+        static const cudaError_t attr_rc4 = cudaFuncSetAttribute(
+            k_edge_hist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SH_WORDS * 4);
         FC_CUDA_TRY(attr_rc);
+        FC_CUDA_TRY(attr_rc4);
         FastDiv divL;
         divL.init(L);
         // about 16K entries per block, at most one block per SM: a block
@@ -426,9 +489,16 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st, uint32_t lo, uint32
             int sh_ok = words <= SH_WORDS;
             size_t shb = sh_ok ? (size_t)words * 4 : 0;
             if (d->entries) {
-                k_edge_hist<<<blocks, 1024, shb, st>>>(d->node_ptr, d->adj, n, L, d->entries, divL,
-                                                      s->coreT, lam, nl, s->d_hbase, s->d_kmax,
-                                                      s->H, words, sh_ok);
+                // runs: FC_DENSEST_RUNS (default 1)
+                static const int runs = getenv("FC_DENSEST_RUNS") ? atoi(getenv("FC_DENSEST_RUNS")) : 1;
+                if (nl == 4 && L % 4 == 0 && lam % 4 == 0)
+                    k_edge_hist<true><<<blocks, 1024, shb, st>>>(
+                        d->node_ptr, d->adj, n, L, d->entries, divL, s->coreT, lam, nl, s->d_hbase,
+                        s->d_kmax, s->H, words, sh_ok, runs);
+                else
+                    k_edge_hist<false><<<blocks, 1024, shb, st>>>(
+                        d->node_ptr, d->adj, n, L, d->entries, divL, s->coreT, lam, nl, s->d_hbase,
+                        s->d_kmax, s->H, words, sh_ok, runs);
                 count_launch();
             }
             FC_CUDA_TRY(cudaGetLastError());
@@ -616,7 +686,8 @@ void densest_preload() {
     cudaFuncGetAttributes(&a, k_colmax);
     cudaFuncGetAttributes(&a, k_transpose);
     cudaFuncGetAttributes(&a, k_node_hist);
-    cudaFuncGetAttributes(&a, k_edge_hist);
+    cudaFuncGetAttributes(&a, k_edge_hist<false>);
+    cudaFuncGetAttributes(&a, k_edge_hist<true>);
     cudaFuncGetAttributes(&a, k_suffix);
     cudaFuncGetAttributes(&a, k_cells);
     cudaFuncGetAttributes(&a, k_fold);
