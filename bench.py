@@ -418,11 +418,13 @@ def run_ours(args, world, rank, local):
         h2d = L * (n + 1) * 8 + m2 * 4
         d2h = my_cols * n * 4 + 48
         evs = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
-        phases = {"upload": [], "peel": [], "table_d2h": [], "densest": []}
+        phases = {"upload": [], "peel": [], "table_d2h": [], "densest": [], "release_host": []}
 
         def e2e_step(record):
+            t_rel = time.perf_counter()
             g.release_device()
             if record:
+                phases["release_host"].append((time.perf_counter() - t_rel) * 1e3)
                 evs[0].record(stream)
             g.upload(stream=stream)
             if record:

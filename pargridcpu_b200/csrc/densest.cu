@@ -135,11 +135,10 @@ __global__ void k_node_hist(const uint32_t* __restrict__ table, uint32_t n,
 // per lane), and tracks each lane's source node by advancing along node_ptr.
 // Bins live in shared memory when they fit (`sh_ok`), else in global memory.
 // The entry (v, u, l) adds one to bin (l, min(core(v), core(u))) per column.
-// Where core(u) >= core(v) the key is v's own core, the same for every entry
-// of a run of adjacent lanes with the same (v, l): the run's first lane adds
-// their number with one atomic, so the hottest bins (low-core nodes, whose
-// neighbours mostly have higher cores) take one atomic per run instead of
-// one per entry.  The other entries add one each.
+// With `runs` set, the entries whose key is v's own core (core(u) >= core(v))
+// are counted per run of adjacent lanes with the same (v, l) and added by the
+// run's first lane with one atomic; measured slower than one atomic per
+// entry on c3, so off by default.
 __device__ __forceinline__ void edge_bin_add(uint32_t* sh, uint32_t* H, bool sh_ok, uint32_t soff,
                                              uint64_t hbase, uint32_t l, uint32_t km1,
                                              uint32_t key, uint32_t cnt) {
@@ -489,8 +488,9 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st, uint32_t lo, uint32
             int sh_ok = words <= SH_WORDS;
             size_t shb = sh_ok ? (size_t)words * 4 : 0;
             if (d->entries) {
-                // runs: FC_DENSEST_RUNS (default 1)
-                static const int runs = getenv("FC_DENSEST_RUNS") ? atoi(getenv("FC_DENSEST_RUNS")) : 1;
+                // run counting (FC_DENSEST_RUNS=1) measured slower on c3 (1.95 against
+                // 1.78 ms per search): off by default
+                static const int runs = getenv("FC_DENSEST_RUNS") ? atoi(getenv("FC_DENSEST_RUNS")) : 0;
                 if (nl == 4 && L % 4 == 0 && lam % 4 == 0)
                     k_edge_hist<true><<<blocks, 1024, shb, st>>>(
                         d->node_ptr, d->adj, n, L, d->entries, divL, s->coreT, lam, nl, s->d_hbase,

@@ -1901,306 +1901,6 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
     cl.sync();  // no block leaves while another may still reach its shared memory
 }
 
-// ---- the endgame on a cluster, drained without rounds ---------------------------
-//
-// The same levels again, survivors spread over the cluster as in k_endgame_cl,
-// but a level's removals are expanded as a work queue instead of in rounds:
-// every warp claims work items (EGA_CH-entry pieces of a removed node's
-// subgraph row) from its own block's queue as soon as they are written, and
-// a removal it causes is queued at once on the removed node's owner.  A
-// cascade step then costs a few shared-memory operations and one L2 load of
-// the row, not a cluster barrier.  The level is over when the cluster-wide
-// count of items processed equals the count of items reserved (both in
-// block 0, per level parity; an item is reserved before anything it queues
-// is counted processed, as in k_peel's drain).  A SCAN of every block's own
-// survivors starts each level, and cluster barriers separate SCAN, drain and
-// the next level.  Every wait is bounded: a wait that runs out records an
-// error, every warp then leaves the drain, and all blocks still meet at the
-// same barriers (they read the error after one) before the kernel returns.
-constexpr uint32_t EGA_CH = 256;
-constexpr uint32_t EGA_EMPTY = 0xFFFFFFFFu;
-constexpr uint32_t EGA_SPIN_LIMIT = 1u << 22;  // x ~64-256 ns per sleep: well under a second
-
-// shared bytes per owned survivor besides the queue: degrees (L halves),
-// count (a half), alive flag, two lists (16-bit), row start and length
-static uint32_t ega_node_bytes(uint32_t L) { return 2 * L + 15; }
-static uint64_t ega_smem_bytes(uint32_t mo, uint32_t L, uint32_t qcap) {
-    return 4ull * (((uint64_t)mo * L + 1) / 2 + (mo + 1) / 2 + 2ull * mo + qcap) + mo + 4 + 4ull * mo +
-           16;
-}
-
-// Work items of each block of each column: sum over its survivors of
-// ceil(row / EGA_CH), the most its queue holds in a level.
-__global__ void k_ega_qcap(const uint32_t* __restrict__ rowptr, uint32_t cap,
-                           const uint32_t* __restrict__ ecnt, uint32_t cs,
-                           uint32_t* __restrict__ qcap) {
-    const uint32_t c = blockIdx.x;
-    const uint32_t m = min(ecnt[c], cap);
-    const uint32_t* rp = rowptr + (uint64_t)c * (cap + 1);
-    for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
-        const uint32_t len = rp[i + 1] - rp[i];
-        if (len) atomicAdd(qcap + (uint64_t)c * cs + (i & (cs - 1)), (len + EGA_CH - 1) / EGA_CH);
-    }
-}
-
-__global__ void __launch_bounds__(EG_THREADS) k_endgame_ca(
-    uint32_t cap, const uint32_t* __restrict__ ecnt, const uint32_t* __restrict__ rowptr,
-    const uint64_t* __restrict__ base, const uint32_t* __restrict__ H,
-    const uint32_t* __restrict__ l2g, const uint32_t* __restrict__ deg, uint32_t n, uint32_t L,
-    FastDiv divL, uint32_t* __restrict__ t, uint32_t col0, uint32_t k0, uint32_t max_level,
-    uint32_t qcap, uint32_t* __restrict__ levels, uint32_t* __restrict__ err,
-    unsigned long long* __restrict__ tr) {
-    extern __shared__ __align__(16) uint32_t sm[];
-    __shared__ uint32_t s_next, s_head, s_tail, s_done, s_scan_items;
-    __shared__ uint32_t s_res[2], s_proc[2], s_kept[2], s_err;  // block 0's are the cluster's
-    __shared__ uint32_t s_rd_kept, s_rd_err;
-    cg::cluster_group cl = cg::this_cluster();
-    const uint32_t CS = cl.num_blocks();
-    const uint32_t r = cl.block_rank();
-    const uint32_t lg = 31 - __clz(CS);
-    const uint32_t c = blockIdx.x / CS;
-    const uint32_t m = min(ecnt[c], cap);
-    if (m == 0) return;  // the whole cluster leaves, before any barrier
-    const uint32_t lmd = col0 + c + 1;
-    const uint32_t mo_max = (m + CS - 1) / CS;
-    const uint32_t mo = r < m ? (m - r + CS - 1) / CS : 0u;
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t* rp = rowptr + (uint64_t)c * (cap + 1);
-    const uint32_t* Hc = H + base[c];
-    const uint32_t* g_of = l2g + (uint64_t)c * cap;
-    uint32_t* tc = t + (uint64_t)c * n;
-    uint32_t* dw = sm;                                       // (mo_max * L + 1) / 2 words
-    uint32_t* cw = dw + ((uint64_t)mo_max * L + 1) / 2;      // (mo_max + 1) / 2 words
-    uint32_t* rstart = cw + (mo_max + 1) / 2;                // mo_max words
-    uint32_t* rlen = rstart + mo_max;                        // mo_max words
-    uint32_t* queue = rlen + mo_max;                         // qcap words: idx | chunk << 16
-    uint8_t* alive = (uint8_t*)(queue + qcap);               // mo_max bytes
-    uint16_t* list0 = (uint16_t*)(((uintptr_t)(alive + mo_max) + 3) & ~(uintptr_t)3);
-    uint16_t* list1 = list0 + mo_max;
-    for (uint32_t i = threadIdx.x; i < ((uint64_t)mo_max * L + 1) / 2; i += blockDim.x) dw[i] = 0;
-    for (uint32_t i = threadIdx.x; i < (mo_max + 1) / 2; i += blockDim.x) cw[i] = 0;
-    if (threadIdx.x < 2) {
-        s_res[threadIdx.x] = 0;
-        s_proc[threadIdx.x] = 0;
-        s_kept[threadIdx.x] = 0;
-    }
-    if (threadIdx.x == 0) s_err = 0;
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < mo * L; i += blockDim.x) {
-        const uint32_t idx = i / L, l = i - idx * L;
-        const uint32_t d = deg[(uint64_t)c * n * L + (uint64_t)g_of[(idx << lg) + r] * L + l];
-        atomicOr(dw + (i >> 1), (d & 0xFFFFu) << ((i & 1) * 16));
-    }
-    for (uint32_t i = threadIdx.x; i < mo; i += blockDim.x) {
-        const uint32_t lid = (i << lg) + r;
-        rstart[i] = rp[lid];
-        rlen[i] = rp[lid + 1] - rp[lid];
-        alive[i] = 1;
-        list0[i] = (uint16_t)i;
-    }
-    uint32_t* const r0_res = cl.map_shared_rank(s_res, 0);
-    uint32_t* const r0_proc = cl.map_shared_rank(s_proc, 0);
-    uint32_t* const r0_kept = cl.map_shared_rank(s_kept, 0);
-    uint32_t* const r0_err = cl.map_shared_rank(&s_err, 0);
-    cl.sync();  // every block initialised before any reaches another
-    uint16_t* cur = list0;
-    uint16_t* nxt = list1;
-    uint32_t na = mo, k = k0;
-    for (;;) {
-        if (k > max_level) {  // uniform
-            if (r == 0 && threadIdx.x == 0) atomicExch(err, 2u);
-            break;
-        }
-        const uint32_t par = k & 1;
-        unsigned long long* const trl = threadIdx.x == 0 ? eg_tr(tr, c, k - k0) : nullptr;
-        // SCAN: this block's survivors; removals queue locally
-        if (threadIdx.x == 0) {
-            s_next = 0;
-            s_head = 0;
-            s_tail = 0;
-            s_done = 0;
-            s_scan_items = 0;
-            if (trl && r == 0) trl[0] = global_ns();
-        }
-        for (uint32_t i = threadIdx.x; i < qcap; i += blockDim.x) queue[i] = EGA_EMPTY;
-        __syncthreads();
-        for (uint32_t i = threadIdx.x; i < na; i += blockDim.x) {
-            const uint32_t x = cur[i];
-            if (!alive[x]) continue;
-            uint32_t cnt = 0;
-            for (uint32_t l = 0; l < L; l++) cnt += eg_get16(dw, x * L + l) >= k + 1;
-            if (cnt < lmd) {
-                alive[x] = 0;
-                tc[g_of[(x << lg) + r]] = k;
-                const uint32_t nch = (rlen[x] + EGA_CH - 1) / EGA_CH;
-                if (nch) {
-                    const uint32_t p = atomicAdd(&s_tail, nch);
-                    for (uint32_t q = 0; q < nch && p + q < qcap; q++) queue[p + q] = x | (q << 16);
-                    atomicAdd(&s_scan_items, nch);
-                }
-            } else {
-                atomicOr(cw + (x >> 1), cnt << ((x & 1) * 16));  // the half was 0
-                nxt[atomicAdd(&s_next, 1u)] = (uint16_t)x;
-            }
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            if (s_scan_items) atomicAdd(r0_res + par, s_scan_items);
-            if (s_next) atomicAdd(r0_kept + par, s_next);
-            if (r == 0) {  // the other parity's counters: last used a level ago
-                s_res[par ^ 1] = 0;
-                s_proc[par ^ 1] = 0;
-                s_kept[par ^ 1] = 0;
-            }
-        }
-        cl.sync();
-        if (threadIdx.x == 0) s_rd_kept = r0_kept[par];
-        __syncthreads();
-        const uint32_t kept = s_rd_kept;
-        // DRAIN: warps take items as they appear until the cluster has
-        // processed every item it reserved (nothing to do once no survivor
-        // is left in the column)
-        if (kept) {
-            uint32_t spins = 0, ns = 64;
-            unsigned long long my_entries = 0;
-            for (;;) {
-                uint32_t item = EGA_EMPTY, claim = EGA_EMPTY, stop = 0;
-                if (lane == 0 && *(volatile uint32_t*)&s_head < *(volatile uint32_t*)&s_tail)
-                    claim = atomicAdd(&s_head, 1u);
-                claim = __shfl_sync(0xffffffffu, claim, 0);
-                if (claim != EGA_EMPTY) {
-                    // wait (bounded) for the claimed slot to be written.  A
-                    // claim that raced past the reservations is abandoned
-                    // once the level is over (then no slot is left to fill).
-                    if (lane == 0) {
-                        for (uint32_t w = 0;; w++) {
-                            if (claim < qcap) {
-                                item = *(volatile uint32_t*)&queue[claim];
-                                if (item != EGA_EMPTY) break;
-                            }
-                            if ((w & 63) == 0) {
-                                if (*(volatile uint32_t*)&s_done || *(volatile uint32_t*)r0_err) {
-                                    stop = 1;
-                                    break;
-                                }
-                                const uint32_t p = *(volatile uint32_t*)(r0_proc + par);
-                                const uint32_t q = *(volatile uint32_t*)(r0_res + par);
-                                if (p == q) {
-                                    s_done = 1;
-                                    stop = 1;
-                                    break;
-                                }
-                            }
-                            if (w >= EGA_SPIN_LIMIT) {
-                                atomicOr(r0_err, 1u);
-                                s_done = 1;
-                                stop = 1;
-                                break;
-                            }
-                            __nanosleep(32);
-                        }
-                    }
-                    item = __shfl_sync(0xffffffffu, item, 0);
-                    stop = __shfl_sync(0xffffffffu, stop, 0);
-                    if (stop) break;
-                    // one piece of a removed node's row
-                    const uint32_t idx = item & 0xFFFFu, ch = item >> 16;
-                    const uint32_t rb = rstart[idx] + ch * EGA_CH;
-                    const uint32_t re = min(rstart[idx] + rlen[idx], rb + EGA_CH);
-                    uint32_t slot[EGA_CH / 32];
-#pragma unroll
-                    for (int q = 0; q < (int)(EGA_CH / 32); q++) {
-                        const uint32_t e = rb + q * 32 + lane;
-                        slot[q] = e < re ? Hc[e] : UNSET;
-                    }
-#pragma unroll
-                    for (int q = 0; q < (int)(EGA_CH / 32); q++) {
-                        if (slot[q] == UNSET) continue;
-                        const uint32_t u = divL.div(slot[q]);
-                        if (u >= m) continue;
-                        const uint32_t l = slot[q] - u * L;
-                        const uint32_t ow = u & (CS - 1), ui = u >> lg;
-                        uint8_t* const a_ow = cl.map_shared_rank(alive, ow);
-                        if (!a_ow[ui]) continue;
-                        const uint32_t old = egc_dec16(cl.map_shared_rank(dw, ow), ui * L + l);
-                        if (old == k + 1 && egc_dec16(cl.map_shared_rank(cw, ow), ui) == lmd) {
-                            a_ow[ui] = 0;
-                            tc[g_of[u]] = k;
-                            const uint32_t len = cl.map_shared_rank(rlen, ow)[ui];
-                            const uint32_t nch = (len + EGA_CH - 1) / EGA_CH;
-                            if (nch) {
-                                // reserve cluster-wide first, then the owner's slots
-                                atomicAdd(r0_res + par, nch);
-                                const uint32_t p = atomicAdd(cl.map_shared_rank(&s_tail, ow), nch);
-                                uint32_t* const q_ow = cl.map_shared_rank(queue, ow);
-                                for (uint32_t z = 0; z < nch; z++) {
-                                    if (p + z < qcap && z < 65536) q_ow[p + z] = ui | (z << 16);
-                                    else atomicOr(r0_err, 1u);
-                                }
-                            }
-                        }
-                    }
-                    if (lane == 0) my_entries += re - rb;
-                    // this item is done: after everything it queued is reserved
-                    __syncwarp();
-                    __threadfence();
-                    if (lane == 0) atomicAdd(r0_proc + par, 1u);
-                    spins = 0;
-                    ns = 64;
-                    continue;
-                }
-                // nothing to claim: the level is over when the cluster has
-                // processed all it reserved (processed read first; both grow)
-                if (lane == 0) {
-                    if (*(volatile uint32_t*)&s_done) {
-                        stop = 1;
-                    } else {
-                        const uint32_t p = *(volatile uint32_t*)(r0_proc + par);
-                        const uint32_t q = *(volatile uint32_t*)(r0_res + par);
-                        if (p == q || *(volatile uint32_t*)r0_err) {
-                            s_done = 1;
-                            stop = 1;
-                        } else if (++spins >= EGA_SPIN_LIMIT) {
-                            atomicOr(r0_err, 1u);
-                            s_done = 1;
-                            stop = 1;
-                        }
-                    }
-                }
-                if (__shfl_sync(0xffffffffu, stop, 0)) break;
-                __nanosleep(ns);
-                if (ns < 256) ns <<= 1;
-            }
-            if (tr && lane == 0 && k - k0 < EG_TRACE_LEVELS)
-                atomicAdd(tr + 4ull * ((uint64_t)c * EG_TRACE_LEVELS + (k - k0)) + 3, my_entries);
-        }
-        __syncthreads();
-        cl.sync();  // every block's drain is over: no remote decrement is in flight
-        if (threadIdx.x == 0) {
-            s_rd_err = *(volatile uint32_t*)r0_err;
-            if (trl && r == 0) {
-                trl[1] = 0;
-                trl[2] = r0_res[par];
-            }
-        }
-        // counts are rebuilt by the next scan: clear the kept ones
-        for (uint32_t i = threadIdx.x; i < (mo_max + 1) / 2; i += blockDim.x) cw[i] = 0;
-        na = s_next;
-        uint16_t* tmp = cur;
-        cur = nxt;
-        nxt = tmp;
-        k++;
-        __syncthreads();
-        if (s_rd_err) {
-            if (r == 0 && threadIdx.x == 0) atomicExch(err, 3u);
-            break;
-        }
-        if (kept == 0) break;  // uniform
-    }
-    if (r == 0 && threadIdx.x == 0) levels[c] = k - k0;
-    cl.sync();  // no block leaves while another may still reach its shared memory
-}
-
 static SegP make_seg(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* table,
                      uint32_t* deg, uint32_t xbase) {
     SegP p{};
@@ -2279,20 +1979,9 @@ static uint32_t eg_cluster_size() {
 }
 
 // survivors one column's endgame can hold with cs blocks (0: off for this L)
-// The asynchronous cluster drain (k_endgame_ca): FC_PEEL_EG_ASYNC=1.
-static bool eg_async() { return env_u32("FC_PEEL_EG_ASYNC", 0) != 0; }
-// survivors per block it plans for: two queue words per survivor on average
-static uint32_t ega_block_capacity(uint32_t L) {
-    const uint64_t fixed = 8ull * EG_THREADS + 512;
-    uint64_t cap = (EG_SMEM - fixed) / (ega_node_bytes(L) + 8);
-    if (cap > 65535) cap = 65535;
-    return cap >= 1024 ? (uint32_t)cap : 0u;
-}
-
 // FC_PEEL_EG_CAP lowers it (the endgame then starts later)
 static uint32_t eg_column_capacity(uint32_t L, uint32_t cs) {
-    const uint32_t cap = cs > 1 ? cs * (eg_async() ? ega_block_capacity(L) : egc_block_capacity(L))
-                                : eg_capacity(L);
+    const uint32_t cap = cs > 1 ? cs * egc_block_capacity(L) : eg_capacity(L);
     const uint32_t want = env_u32("FC_PEEL_EG_CAP", 0);
     return want && want < cap ? want : cap;
 }
@@ -2377,52 +2066,7 @@ static fc_status endgame_run(const PeelJob& j, const PeelGraph& g, const PeelCtl
             map, capE, rowptr, c->eg_base, H, &c->eg_err);
         static const cudaError_t attr_rc = cudaFuncSetAttribute(
             k_endgame, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)EG_SMEM);
-        bool done_async = false;
-        if (cs > 1 && eg_async() && (uint64_t)ncols * cs <= j.qs_cap) {
-            // work items per block (rowlen is spent once rowptr is built)
-            uint32_t* qc = rowlen;
-            FC_CUDA_TRY(cudaMemsetAsync(qc, 0, 4ull * ncols * cs, s));
-            k_ega_qcap<<<ncols, 256, 0, s>>>(rowptr, capE, c->eg_cnt, cs, qc);
-            count_launch();
-            FC_CUDA_TRY(cudaGetLastError());
-            std::vector<uint32_t> qh(ncols * cs);
-            FC_TRY(to_host(qh.data(), qc, 4ull * ncols * cs, s));
-            uint32_t qmax = 1;
-            for (uint32_t v : qh) qmax = v > qmax ? v : qmax;
-            const uint32_t mo = (mmax + cs - 1) / cs;
-            const uint64_t smem = ega_smem_bytes(mo, g.L, qmax);
-            static const cudaError_t ca_rc = cudaFuncSetAttribute(
-                k_endgame_ca, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)EG_SMEM);
-            static const cudaError_t ca_rc2 = cudaFuncSetAttribute(
-                k_endgame_ca, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-            if (smem <= EG_SMEM && mo <= 65535 && ca_rc == cudaSuccess && ca_rc2 == cudaSuccess) {
-                cudaLaunchConfig_t cfg = {};
-                cudaLaunchAttribute at[1];
-                at[0].id = cudaLaunchAttributeClusterDimension;
-                at[0].val.clusterDim.x = cs;
-                at[0].val.clusterDim.y = 1;
-                at[0].val.clusterDim.z = 1;
-                cfg.gridDim = dim3(ncols * cs);
-                cfg.blockDim = dim3(EG_THREADS);
-                cfg.dynamicSmemBytes = (size_t)smem;
-                cfg.stream = s;
-                cfg.attrs = at;
-                cfg.numAttrs = 1;
-                const cudaError_t le = cudaLaunchKernelEx(
-                    &cfg, k_endgame_ca, capE, (const uint32_t*)c->eg_cnt, (const uint32_t*)rowptr,
-                    (const uint64_t*)c->eg_base, (const uint32_t*)H, (const uint32_t*)l2g, deg, g.n,
-                    g.L, divL, j.seg0.t, col0, K + 1, j.max_level, qmax, c->eg_levels, &c->eg_err,
-                    etr);
-                count_launch(5);
-                if (le != cudaSuccess) {
-                    set_last_cuda_error(le, "k_endgame_ca", __FILE__, __LINE__);
-                    rc = FC_ERR_DEVICE;
-                }
-                done_async = true;
-            }
-        }
-        if (done_async) {
-        } else if (cs > 1) {
+        if (cs > 1) {
             // a cluster of cs blocks per column (k_endgame_cl)
             const uint32_t mo = (mmax + cs - 1) / cs;
             const uint64_t smem = egc_smem_bytes(mo, g.L);
