@@ -30,6 +30,7 @@ table method plus the fastest WdsList is the reference's time for a step.
 from __future__ import annotations
 
 import argparse
+import gc
 import hashlib
 import json
 import os
@@ -410,72 +411,96 @@ def run_ours(args, world, rank, local):
         res = shard.gather_cells(res) if world > 1 else shard.merge_cells([res])
 
     # e2e: through the public API from pinned host memory, upload + read-back
-    # inside, phases timed with CUDA events between the calls
+    # inside; CUDA events recorded between the calls of every timed step (no
+    # synchronisation added) split each step into its phases, and the host
+    # time of each call is taken beside them
     e2e = None
     if not args.no_e2e:
         out_t = torch.empty((max(my_cols, 1), n), dtype=torch.int32, pin_memory=True)
         out = out_t.numpy().view(np.uint32)
         h2d = L * (n + 1) * 8 + m2 * 4
         d2h = my_cols * n * 4 + 48
-        evs = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
-        phases = {"upload": [], "peel": [], "table_d2h": [], "densest": [], "release_host": []}
+        names = ("upload", "peel", "table_d2h", "densest")
 
-        def e2e_step(record):
-            t_rel = time.perf_counter()
+        def e2e_step(evs, host):
+            t = time.perf_counter()
             g.release_device()
-            if record:
-                phases["release_host"].append((time.perf_counter() - t_rel) * 1e3)
-                evs[0].record(stream)
+            host["release"].append((time.perf_counter() - t) * 1e3)
+            evs[0].record(stream)
+            t = time.perf_counter()
             g.upload(stream=stream)
-            if record:
-                evs[1].record(stream)
+            host["upload"].append((time.perf_counter() - t) * 1e3)
+            evs[1].record(stream)
+            t = time.perf_counter()
             if split:
                 if my_cols:
                     g.coreindex_range(lo, hi, stream=stream, copy=False)
-                    if record:
-                        evs[2].record(stream)
+                    evs[2].record(stream)
                     g.coreindex_range(lo, hi, out=out, stream=stream)
-                    if record:
-                        evs[3].record(stream)
+                    evs[3].record(stream)
                     r = g.cells_range(lo, hi, args.beta, stream=stream)
                 else:
                     r = []
-                    if record:
-                        evs[2].record(stream)
-                        evs[3].record(stream)
+                    evs[2].record(stream)
+                    evs[3].record(stream)
             else:
                 g.coreindex(stream=stream, copy=False)
-                if record:
-                    evs[2].record(stream)
+                evs[2].record(stream)
                 g.coreindex(out=out, stream=stream)
-                if record:
-                    evs[3].record(stream)
+                evs[3].record(stream)
                 r = g.densest(beta, stream=stream)[0]
-            if record:
-                evs[4].record(stream)
-                torch.cuda.synchronize()
-                for i, k in enumerate(("upload", "peel", "table_d2h", "densest")):
-                    phases[k].append(evs[i].elapsed_time(evs[i + 1]))
+            evs[4].record(stream)
+            host["compute"].append((time.perf_counter() - t) * 1e3)
             return r
 
+        def new_evs():
+            return [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+
+        warm_host = {"release": [], "upload": [], "compute": []}
         for _ in range(max(1, min(args.warmup, 2))):
-            e2e_step(False)
+            e2e_step(new_evs(), warm_host)
         barrier()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        step_evs = [new_evs() for _ in range(args.steps)]
+        host = {"release": [], "upload": [], "compute": []}
+        gc_ms = []  # the interpreter's garbage collections inside the timed steps
+
+        def gc_watch(phase, info, t=[0.0]):
+            if phase == "start":
+                t[0] = time.perf_counter()
+            else:
+                gc_ms.append((info.get("generation"), (time.perf_counter() - t[0]) * 1e3))
+
+        gc.callbacks.append(gc_watch)
         e0.record(stream)
-        for _ in range(args.steps):
-            e2e_step(False)
+        for i in range(args.steps):
+            e2e_step(step_evs[i], host)
         e1.record(stream)
+        gc.callbacks.remove(gc_watch)
         barrier()
         ems = max_over_ranks(e0.elapsed_time(e1))
-        for _ in range(2):  # the phases, on separate steps (their syncs stay out of the total)
-            e2e_step(True)
-        barrier()
+        # a step: from its first event to the next step's first (the last one
+        # to the end of the timed region)
+        starts = [ev[0] for ev in step_evs] + [e1]
+        step_ms = [starts[i].elapsed_time(starts[i + 1]) for i in range(args.steps)]
+        per = {k: [ev[i].elapsed_time(ev[i + 1]) for ev in step_evs]
+               for i, k in enumerate(names)}
+
+        def spread(v):
+            return {"median": statistics.median(v), "mean": statistics.mean(v), "max": max(v)}
+
         e2e = {"value": total_visits * args.steps / (ems / 1e3), "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "ms_per_step": ems / args.steps,
-               "phases_ms": {k: statistics.mean(v) for k, v in phases.items()}}
+               "step_ms": {"min": min(step_ms), **spread(step_ms)},
+               "phases_ms": {k: statistics.median(v) for k, v in per.items()},
+               "phases_spread_ms": {k: spread(v) for k, v in per.items()},
+               "host_call_ms": {k: spread(v) for k, v in host.items()},
+               "gc_in_timed_steps": {"collections": len(gc_ms),
+                                     "ms": sum(m for _, m in gc_ms),
+                                     "max_ms": max((m for _, m in gc_ms), default=0.0),
+                                     "full": sum(1 for g_, _ in gc_ms if g_ == 2)}}
 
     if rank != 0:
         return

@@ -346,8 +346,9 @@ fc_status fc_server_destroy(fc_server* s);
  * decide only the values of the table.
  * A graph whose one column needs more than the array's scratch (about
  * 4*n*L + 36*n + entries/16 bytes) is rejected with FC_ERR_TOO_LARGE before
- * any device work.  The first call on a device looks the array up (make it
- * before any stream capture).  All calls share the one array per device, so
+ * any device work.  A call cannot be captured in a CUDA graph: it reads the
+ * run's status back on the host (a copy and a stream synchronization) before
+ * it returns.  All calls share the one array per device, so
  * calls that overlap on the GPU -- on two streams, or from two host threads
  * -- race, and the caller must serialize them; each call clears the parts
  * that must start empty. */

@@ -44,10 +44,10 @@ struct CellIndex {
     bool valid = false;
 };
 
-void free_cell_index(DeviceGraph* d) {
+void free_cell_index(DeviceGraph* d, cudaStream_t s) {
     CellIndex* c = (CellIndex*)d->cidx;
     if (!c) return;
-    dev_free(c->order, 0);
+    dev_free(c->order, s);
     delete c;
     d->cidx = nullptr;
 }

@@ -64,7 +64,7 @@ static fc_status grow(T*& p, uint64_t& cap, uint64_t need, cudaStream_t st) {
     return FC_OK;
 }
 
-void free_densest_state(DeviceGraph* d) {
+void free_densest_state(DeviceGraph* d, cudaStream_t st) {
     DensState* s = (DensState*)d->dens;
     if (!s) return;
     // called with the graph's work finished (release_device waits for it, or
@@ -72,7 +72,7 @@ void free_densest_state(DeviceGraph* d) {
     for (void* p : {(void*)s->H, (void*)s->N, (void*)s->coreT, (void*)s->d_hbase,
                     (void*)s->d_nbase, (void*)s->d_kmax, (void*)s->cells, (void*)s->powl,
                     (void*)s->d_res, (void*)s->cell_lk})
-        dev_free(p, 0);
+        dev_free(p, st);
     delete s;
     d->dens = nullptr;
 }

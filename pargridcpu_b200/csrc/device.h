@@ -135,10 +135,11 @@ void count_launch(uint32_t k = 1);
 
 // scratch owned by a DeviceGraph, grown on demand
 fc_status ensure_ws(DeviceGraph* d, size_t bytes, cudaStream_t s);
-void free_densest_state(DeviceGraph* d);
+// the frees go on stream s, with the graph's work finished
+void free_densest_state(DeviceGraph* d, cudaStream_t s = 0);
 void invalidate_densest(DeviceGraph* d);
 // cellindex.cu: the resident cell index goes with the table it was built from
-void free_cell_index(DeviceGraph* d);
+void free_cell_index(DeviceGraph* d, cudaStream_t s = 0);
 void invalidate_cell_index(DeviceGraph* d);
 
 // peel.cu

@@ -3,6 +3,7 @@
 #include <cub/cub.cuh>
 
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -58,6 +59,28 @@ __global__ void k_scatter(const uint64_t* __restrict__ off, const uint32_t* __re
         uint32_t dst = node_ptr[v];
         if (node_ptr[v + 1] - dst > ORDER_MIN_ROW) continue;  // written ordered (k_order_scatter)
         for (uint32_t l = 0; l < L; l++) {
+            const uint64_t* o = off + (uint64_t)l * (n + 1);
+            uint64_t b = o[v], e = o[v + 1];
+            for (uint64_t j = b + lane; j < e; j += 32) adj_out[dst + (j - b)] = adj_in[j] * L + l;
+            dst += (uint32_t)(e - b);
+        }
+    }
+}
+
+// The same for layers [l0, l1) only: a row's layer l starts after its
+// layers below l (their degrees from deg0).  The upload scatters each group
+// of layers as soon as its part of the input has arrived.
+__global__ void k_scatter_layers(const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj_in,
+                                 const uint32_t* __restrict__ node_ptr,
+                                 const uint32_t* __restrict__ deg0, uint32_t n, uint32_t L,
+                                 uint32_t l0, uint32_t l1, uint32_t* __restrict__ adj_out) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t v = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
+        uint32_t dst = node_ptr[v];
+        if (node_ptr[v + 1] - dst > ORDER_MIN_ROW) continue;  // written ordered (k_order_scatter)
+        for (uint32_t l = 0; l < l0; l++) dst += deg0[(uint64_t)v * L + l];
+        for (uint32_t l = l0; l < l1; l++) {
             const uint64_t* o = off + (uint64_t)l * (n + 1);
             uint64_t b = o[v], e = o[v + 1];
             for (uint64_t j = b + lane; j < e; j += 32) adj_out[dst + (j - b)] = adj_in[j] * L + l;
@@ -402,6 +425,92 @@ static fc_status order_rows(DeviceGraph* d, const uint32_t* rowlen, const uint64
     return FC_OK;
 }
 
+// Library-owned streams, one of each kind per device (made once): the copy
+// stream of the upload pipeline, and the stream a released graph's memory is
+// freed on.
+enum SideStream { SIDE_COPY = 0, SIDE_RELEASE = 1 };
+
+static cudaStream_t side_stream(SideStream kind) {
+    static std::mutex mu;
+    static cudaStream_t cs[2][64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    cudaStream_t& st = cs[kind][dev];
+    if (!st) {
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            st = nullptr;
+        } else {
+            count_alloc();
+        }
+    }
+    return st;
+}
+
+static cudaStream_t upload_copy_stream() { return side_stream(SIDE_COPY); }
+
+// Groups of layers (at most MAX_GROUPS, about equal in entries) whose input
+// adjacency is copied on the copy stream, one cudaMemcpyAsync and one event
+// per group; `ev[i]` marks group i's arrival.
+struct UploadPipe {
+    static constexpr uint32_t MAX_GROUPS = 8;
+    cudaStream_t cs = nullptr;
+    cudaEvent_t start = nullptr;
+    cudaEvent_t ev[MAX_GROUPS] = {};
+    uint32_t l0[MAX_GROUPS + 1] = {};
+    uint32_t groups = 0;
+    ~UploadPipe() {
+        if (start) cudaEventDestroy(start);
+        for (uint32_t i = 0; i < groups; i++)
+            if (ev[i]) cudaEventDestroy(ev[i]);
+    }
+    // the groups, or 0 when the pipeline cannot be set up (one copy then)
+    uint32_t plan(const fc_graph* g, cudaStream_t s) {
+        const char* e = getenv("FC_UPLOAD_PIPE");  // 0: one copy, no pipeline
+        if (e && *e == '0') return 0;
+        cs = upload_copy_stream();
+        if (!cs || cs == s) return 0;
+        const uint32_t L = g->L, n = g->n;
+        const uint64_t total = g->total_entries();
+        uint32_t k = 0;
+        l0[0] = 0;
+        for (uint32_t l = 0; l < L && k < MAX_GROUPS; l++) {
+            // close a group once it holds its share of the entries
+            const uint64_t upto = g->off[(uint64_t)l * (n + 1) + n];
+            const bool last = l + 1 == L;
+            if (last || upto * MAX_GROUPS >= total * (k + 1)) l0[++k] = l + 1;
+        }
+        if (k == 0) return 0;
+        l0[k] = L;  // the last group takes any layers left
+        if (cudaEventCreateWithFlags(&start, cudaEventDisableTiming) != cudaSuccess) return 0;
+        for (uint32_t i = 0; i < k; i++)
+            if (cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess) {
+                groups = i;
+                cudaGetLastError();
+                return 0;
+            }
+        count_alloc(k + 1);
+        groups = k;
+        return k;
+    }
+    // the copies: after the buffers allocated on s exist
+    fc_status copy(const fc_graph* g, uint32_t* d_in, cudaStream_t s) {
+        const uint32_t n = g->n;
+        FC_CUDA_TRY(cudaEventRecord(start, s));
+        FC_CUDA_TRY(cudaStreamWaitEvent(cs, start, 0));
+        for (uint32_t i = 0; i < groups; i++) {
+            const uint64_t b = g->off[(uint64_t)l0[i] * (n + 1)];
+            const uint64_t e = g->off[(uint64_t)(l0[i + 1] - 1) * (n + 1) + n];
+            if (e > b)
+                FC_CUDA_TRY(cudaMemcpyAsync(d_in + b, g->adj.p + b, (e - b) * 4,
+                                            cudaMemcpyHostToDevice, cs));
+            FC_CUDA_TRY(cudaEventRecord(ev[i], cs));
+        }
+        return FC_OK;
+    }
+};
+
 fc_status upload(fc_graph* g, cudaStream_t s) {
     if (!cuda_available()) return FC_ERR_NO_DEVICE;
     if (g->dev) return FC_OK;
@@ -432,8 +541,17 @@ fc_status upload(fc_graph* g, cudaStream_t s) {
     FC_TRY(dev_alloc((void**)&d->deg0, (uint64_t)n * L * 4 + 4, s));
     FC_TRY(dev_alloc((void**)&d->table, (uint64_t)n * L * 4 + 4, s));
     d->bytes = ((uint64_t)n + 1) * 4 + entries * 4 + 2ull * n * L * 4;
+    // The adjacency goes over in groups of layers on a copy stream while this
+    // stream copies the offsets and builds the degrees and row pointers; each
+    // group is scattered into the node-major rows once it has arrived.
+    UploadPipe pipe;
+    const uint32_t ngroups = entries && n ? pipe.plan(g, s) : 0u;
     if (noff) FC_CUDA_TRY(cudaMemcpyAsync(d_off, g->off.p, noff * 8, cudaMemcpyHostToDevice, s));
-    if (entries) FC_CUDA_TRY(cudaMemcpyAsync(d_in, g->adj.p, entries * 4, cudaMemcpyHostToDevice, s));
+    if (ngroups) {
+        FC_TRY(pipe.copy(g, d_in, s));
+    } else if (entries) {
+        FC_CUDA_TRY(cudaMemcpyAsync(d_in, g->adj.p, entries * 4, cudaMemcpyHostToDevice, s));
+    }
     FC_CUDA_TRY(cudaMemsetAsync(d_max, 0, 8, s));
     int blocks = num_sms() * 8;
     if (n) {
@@ -445,11 +563,20 @@ fc_status upload(fc_graph* g, cudaStream_t s) {
         // rowlen has n entries; entry n of the scan input must be 0
         FC_CUDA_TRY(cudaMemsetAsync(rowlen + n, 0, 4, s));
         FC_CUDA_TRY(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, rowlen, d->node_ptr, n + 1, s));
-        k_scatter<<<blocks, 256, 0, s>>>(d_off, d_in, d->node_ptr, n, L, d->adj);
-        FC_CUDA_TRY(cudaGetLastError());
         k_max<<<blocks, 256, 0, s>>>(d->deg0, (uint64_t)n * L, d_max);
         k_max<<<blocks, 256, 0, s>>>(rowlen, n, d_max + 1);
-        count_launch(4);
+        count_launch(2);
+        if (ngroups) {
+            for (uint32_t i = 0; i < ngroups; i++) {
+                FC_CUDA_TRY(cudaStreamWaitEvent(s, pipe.ev[i], 0));
+                k_scatter_layers<<<blocks, 256, 0, s>>>(d_off, d_in, d->node_ptr, d->deg0, n, L,
+                                                        pipe.l0[i], pipe.l0[i + 1], d->adj);
+                count_launch();
+            }
+        } else {
+            k_scatter<<<blocks, 256, 0, s>>>(d_off, d_in, d->node_ptr, n, L, d->adj);
+            count_launch();
+        }
         FC_CUDA_TRY(cudaGetLastError());
         FC_TRY(order_rows(d, rowlen, d_off, d_in, s));
     }
@@ -474,21 +601,29 @@ void release_device(fc_graph* g, bool wait_home) {
     int cur = -1;
     cudaGetDevice(&cur);
     if (d->device >= 0 && d->device != cur) cudaSetDevice(d->device);
-    // the last call's work is done before its memory returns to the pool;
-    // the frees go on the legacy stream, which outlives any caller stream
+    // the last call's work is done before its memory returns to the pool:
     // a call that left work in flight recorded its stream; one that finished
     // with a synchronize did not (that stream may already be destroyed)
     if (wait_home && d->home) cudaStreamSynchronize(d->home);
     cudaGetLastError();
-    free_densest_state(d);
-    free_cell_index(d);
-    dev_free(d->node_ptr, 0);
-    dev_free(d->adj, 0);
-    dev_free(d->deg0, 0);
-    dev_free(d->big_id, 0);
-    dev_free(d->ptab, 0);
-    dev_free(d->table, 0);
-    dev_free(d->ws, 0);
+    // The frees go on the library's release stream (the legacy stream when
+    // it cannot be made), which outlives any caller stream, and that stream
+    // is synchronized: the pool hands memory freed on one stream to an
+    // allocation on another only once the free is known to be complete, so
+    // an upload right after a release reuses the blocks instead of growing
+    // the pool (which cost up to 30 ms in a step).
+    cudaStream_t rs = side_stream(SIDE_RELEASE);
+    free_densest_state(d, rs);
+    free_cell_index(d, rs);
+    dev_free(d->node_ptr, rs);
+    dev_free(d->adj, rs);
+    dev_free(d->deg0, rs);
+    dev_free(d->big_id, rs);
+    dev_free(d->ptab, rs);
+    dev_free(d->table, rs);
+    dev_free(d->ws, rs);
+    cudaStreamSynchronize(rs);
+    cudaGetLastError();
     if (cur >= 0 && d->device != cur) cudaSetDevice(cur);
     delete d;
     g->dev = nullptr;
@@ -514,6 +649,7 @@ void preload_kernels() {
     cudaFuncAttributes a;
     cudaFuncGetAttributes(&a, k_degrees);
     cudaFuncGetAttributes(&a, k_scatter);
+    cudaFuncGetAttributes(&a, k_scatter_layers);
     cudaFuncGetAttributes(&a, k_max);
     cudaFuncGetAttributes(&a, k_order_flags);
     cudaFuncGetAttributes(&a, k_order_index);

@@ -997,8 +997,9 @@ __device__ __forceinline__ void phase_drain(const PeelJob& j, volatile DrainBloc
     }
 }
 
-// T threads per block, BPS blocks resident per SM: 1024 threads (512 x 2 or
-// 1024 x 1) at most 64 registers a thread; 512 x 3 at most 42.
+// T threads per block, 1024 threads resident per SM (512 x 2 or 1024 x 1):
+// at most 64 registers a thread.  (Three 512-thread blocks per SM at 40
+// registers, with spills, measured slower: c4 batch 682 -> 814 ms.)
 template <int G, int T, bool MULTI, int BPS = 1024 / T>
 __global__ void __launch_bounds__(T, BPS) k_peel(PeelJob j) {
     __shared__ DrainBlock s_drain;
@@ -1061,12 +1062,9 @@ static fc_status launch_t(PeelJob& j, cudaStream_t s) {
     return FC_OK;
 }
 
-// FC_PEEL_OCC=3 with 512-thread blocks: three blocks per SM (1536 threads,
-// 42 registers each) instead of two
 template <int G, bool MULTI>
 static fc_status launch_g(PeelJob& j, uint32_t threads, cudaStream_t s) {
     if (threads == 1024) return launch_t<G, 1024, MULTI>(j, s);
-    if (env_u32("FC_PEEL_OCC", 2) == 3) return launch_t<G, 512, MULTI, 3>(j, s);
     return launch_t<G, 512, MULTI>(j, s);
 }
 
@@ -1670,6 +1668,27 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame(
 // be writing.  Every loop is bounded as in k_endgame, and no block leaves
 // while another may still reach its shared memory.
 constexpr uint32_t EGC_MAX = 16;
+// The count half of a node that is not kept in the current level: decrements
+// of a removed node's count (at most L, one per layer degree passing k + 1)
+// leave it far above any lmd, and never borrow (L is at most 100 here: the
+// block capacity needs 2L + 11 shared bytes per survivor).
+constexpr uint32_t EGC_DEAD = 0x8000u;
+constexpr uint32_t EGC_DEAD2 = 0x80008000u;
+// A kept node's count half is its count (bits 0-13) and, in bit 14, whether
+// its row is long; a removed node's never matches lmd in bits 0-13.
+constexpr uint32_t EGC_BIG = 0x4000u;
+constexpr uint32_t EGC_CNT = 0x3FFFu;
+// Long rows queued in one round, per cluster (more go to their owners)
+constexpr uint32_t EGC_BIG_MAX = 256;
+
+// appends column-local node u to block 0's list of long rows for a round
+__device__ __forceinline__ bool egc_push_big(uint32_t* big, uint32_t* bign, uint32_t slot,
+                                             uint32_t u) {
+    const uint32_t pos = atomicAdd(bign + slot, 1u);
+    if (pos >= EGC_BIG_MAX) return false;
+    big[slot * EGC_BIG_MAX + pos] = u;
+    return true;
+}
 
 __device__ __forceinline__ uint32_t egc_dec16(uint32_t* w, uint32_t i) {
     const uint32_t sh = (i & 1) * 16;
@@ -1695,12 +1714,14 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
     const uint64_t* __restrict__ base, const uint32_t* __restrict__ H,
     const uint32_t* __restrict__ l2g, const uint32_t* __restrict__ deg, uint32_t n, uint32_t L,
     FastDiv divL, uint32_t* __restrict__ t, uint32_t col0, uint32_t k0, uint32_t max_level,
-    uint32_t* __restrict__ levels, uint32_t* __restrict__ err, unsigned long long* __restrict__ tr) {
+    uint32_t* __restrict__ levels, uint32_t* __restrict__ err, unsigned long long* __restrict__ tr,
+    uint32_t split) {
     extern __shared__ __align__(16) uint32_t sm[];
     __shared__ uint32_t s_warp[33];
     __shared__ uint32_t s_next, s_qe, s_pushed, s_tail[2];
     __shared__ uint32_t s_cnt[3], s_kept[3];  // block 0's are the cluster's
-    __shared__ uint32_t s_rd_cnt, s_rd_kept;  // what this block read after a barrier
+    __shared__ uint32_t s_rd_cnt, s_rd_kept, s_rd_nb;  // what this block read after a barrier
+    __shared__ uint32_t s_big[3][EGC_BIG_MAX], s_bign[3];  // block 0's are the cluster's
     cg::cluster_group cl = cg::this_cluster();
     const uint32_t CS = cl.num_blocks();
     const uint32_t r = cl.block_rank();
@@ -1724,10 +1745,11 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
     uint16_t* list1 = list0 + mo_max;
     uint16_t* qh[2] = {list1 + mo_max, list1 + 2 * mo_max};  // the two queue halves
     for (uint32_t i = threadIdx.x; i < ((uint64_t)mo_max * L + 1) / 2; i += blockDim.x) dw[i] = 0;
-    for (uint32_t i = threadIdx.x; i < (mo_max + 1) / 2; i += blockDim.x) cw[i] = 0;
+    for (uint32_t i = threadIdx.x; i < (mo_max + 1) / 2; i += blockDim.x) cw[i] = EGC_DEAD2;
     if (threadIdx.x < 3) {
         s_cnt[threadIdx.x] = 0;
         s_kept[threadIdx.x] = 0;
+        s_bign[threadIdx.x] = 0;
     }
     if (threadIdx.x == 0) s_tail[0] = s_tail[1] = 0;
     __syncthreads();
@@ -1736,12 +1758,17 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
         const uint32_t d = deg[(uint64_t)c * n * L + (uint64_t)g_of[(idx << lg) + r] * L + l];
         atomicOr(dw + (i >> 1), (d & 0xFFFFu) << ((i & 1) * 16));
     }
+    // alive: 1, or 2 for a node whose row is longer than split (expanded by
+    // every block of the cluster, a slice each)
     for (uint32_t i = threadIdx.x; i < mo; i += blockDim.x) {
-        alive[i] = 1;
+        const uint32_t u = (i << lg) + r;
+        alive[i] = split && rp[u + 1] - rp[u] > split ? 2 : 1;
         list0[i] = (uint16_t)i;
     }
     uint32_t* const r0_cnt = cl.map_shared_rank(s_cnt, 0);
     uint32_t* const r0_kept = cl.map_shared_rank(s_kept, 0);
+    uint32_t* const r0_big = cl.map_shared_rank(&s_big[0][0], 0);
+    uint32_t* const r0_bign = cl.map_shared_rank(s_bign, 0);
     cl.sync();  // every block initialised before any reaches another
     uint16_t* cur = list0;
     uint16_t* nxt = list1;
@@ -1765,31 +1792,39 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
         __syncthreads();
         for (uint32_t i = threadIdx.x; i < na; i += blockDim.x) {
             const uint32_t x = cur[i];
-            if (!alive[x]) continue;
+            const uint32_t ax = alive[x];
+            if (!ax) continue;
             uint32_t cnt = 0;
             for (uint32_t l = 0; l < L; l++) cnt += eg_get16(dw, x * L + l) >= k + 1;
             if (cnt < lmd) {
                 alive[x] = 0;
                 tc[g_of[(x << lg) + r]] = k;
-                qh[qn][atomicAdd(&s_tail[qn], 1u)] = (uint16_t)x;
+                if (ax == 2 && egc_push_big(r0_big, r0_bign, (rho + 1) % 3, (x << lg) + r))
+                    atomicAdd(&s_pushed, 1u);
+                else
+                    qh[qn][atomicAdd(&s_tail[qn], 1u)] = (uint16_t)x;
             } else {
-                atomicOr(cw + (x >> 1), cnt << ((x & 1) * 16));  // the half was 0
+                // EGC_DEAD -> cnt, with the long-row flag
+                const uint32_t v = cnt | (ax == 2 ? EGC_BIG : 0u);
+                atomicSub(cw + (x >> 1), (EGC_DEAD - v) << ((x & 1) * 16));
                 nxt[atomicAdd(&s_next, 1u)] = (uint16_t)x;
             }
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            if (s_tail[qn]) atomicAdd(r0_cnt + rho % 3, s_tail[qn]);
+            if (s_tail[qn] + s_pushed) atomicAdd(r0_cnt + rho % 3, s_tail[qn] + s_pushed);
             if (s_next) atomicAdd(r0_kept + rho % 3, s_next);
             if (r == 0) {
                 s_cnt[(rho + 1) % 3] = 0;
                 s_kept[(rho + 1) % 3] = 0;
+                s_bign[(rho + 2) % 3] = 0;
             }
         }
         cl.sync();
         if (threadIdx.x == 0) {
             s_rd_cnt = r0_cnt[rho % 3];
             s_rd_kept = r0_kept[rho % 3];
+            s_rd_nb = min(r0_bign[(rho + 1) % 3], EGC_BIG_MAX);  // the next round's long rows
         }
         __syncthreads();
         const uint32_t kept = s_rd_kept;
@@ -1807,15 +1842,26 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
                 s_pushed = 0;
             }
             __syncthreads();
-            const uint32_t qe = s_qe;
+            // this block's queued rows, then its slice of every long row
+            const uint32_t qe = s_qe, nbig = s_rd_nb, items = qe + nbig;
+            const uint32_t* const bl = r0_big + (rho % 3) * EGC_BIG_MAX;
             tr_rounds++;
-            for (uint32_t b0 = 0; b0 < qe; b0 += EG_THREADS) {
-                const uint32_t nb = min(EG_THREADS, qe - b0);
+            for (uint32_t b0 = 0; b0 < items; b0 += EG_THREADS) {
+                const uint32_t nb = min(EG_THREADS, items - b0);
                 uint32_t len = 0, start = 0;
-                if (threadIdx.x < nb) {
-                    const uint32_t lid = ((uint32_t)qh[qc][b0 + threadIdx.x] << lg) + r;
+                const uint32_t it = b0 + threadIdx.x;
+                if (it < qe) {
+                    const uint32_t lid = ((uint32_t)qh[qc][it] << lg) + r;
                     start = rp[lid];
                     len = rp[lid + 1] - start;
+                    tc[g_of[lid]] = k;  // again for a scan removal: the same value
+                } else if (it < items) {
+                    const uint32_t u = bl[it - qe];
+                    const uint32_t s0 = rp[u], l0 = rp[u + 1] - s0;
+                    const uint32_t e0 = (uint32_t)((uint64_t)l0 * r / CS);
+                    start = s0 + e0;
+                    len = (uint32_t)((uint64_t)l0 * (r + 1) / CS) - e0;
+                    if ((u & (CS - 1)) == r) tc[g_of[u]] = k;  // its owner
                 }
                 uint32_t ex;
                 const uint32_t total = eg_block_scan(len, &ex, s_warp);
@@ -1841,25 +1887,40 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
                             slot[q] = Hc[rs[lo] + (e - pre[lo])];
                         }
                     }
+                    // the degree decrements first, independent of one another;
+                    // removed neighbours are decremented too (a half counts
+                    // the alive neighbours, so it never drops below 0), and
+                    // their count halves, EGC_DEAD less at most L crossings,
+                    // never equal lmd
+                    uint32_t ow[4], ui[4], old[4];
 #pragma unroll
                     for (int q = 0; q < 4; q++) {
+                        old[q] = 0;  // never k + 1
+                        ow[q] = ui[q] = 0;
                         if (slot[q] == UNSET) continue;
                         const uint32_t u = divL.div(slot[q]);
                         if (u >= m) continue;
                         const uint32_t l = slot[q] - u * L;
-                        const uint32_t ow = u & (CS - 1), ui = u >> lg;
-                        uint8_t* const a_ow = cl.map_shared_rank(alive, ow);
-                        if (!a_ow[ui]) continue;
-                        const uint32_t old = egc_dec16(cl.map_shared_rank(dw, ow), ui * L + l);
-                        if (old == k + 1 && egc_dec16(cl.map_shared_rank(cw, ow), ui) == lmd) {
-                            a_ow[ui] = 0;
-                            tc[g_of[u]] = k;
-                            uint32_t* const t_ow = cl.map_shared_rank(s_tail, ow);
+                        ow[q] = u & (CS - 1);
+                        ui[q] = u >> lg;
+                        old[q] = egc_dec16(cl.map_shared_rank(dw, ow[q]), ui[q] * L + l);
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        if (old[q] != k + 1) continue;
+                        const uint32_t oc = egc_dec16(cl.map_shared_rank(cw, ow[q]), ui[q]);
+                        if ((oc & EGC_CNT) != lmd) continue;
+                        // removed: expanded next round, by its owner or, for
+                        // a long row, by every block (the table entry is
+                        // written then)
+                        cl.map_shared_rank(alive, ow[q])[ui[q]] = 0;
+                        if (!((oc & EGC_BIG) &&
+                              egc_push_big(r0_big, r0_bign, (rho + 1) % 3, (ui[q] << lg) | ow[q]))) {
+                            uint32_t* const t_ow = cl.map_shared_rank(s_tail, ow[q]);
                             const uint32_t pos = atomicAdd(t_ow + qp, 1u);
-                            uint16_t* const q_ow = cl.map_shared_rank(qh[qp], ow);
-                            q_ow[pos] = (uint16_t)ui;
-                            atomicAdd(&s_pushed, 1u);
+                            cl.map_shared_rank(qh[qp], ow[q])[pos] = (uint16_t)ui[q];
                         }
+                        atomicAdd(&s_pushed, 1u);
                     }
                 }
                 __syncthreads();
@@ -1870,14 +1931,22 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
                 if (r == 0) {
                     s_cnt[(rho + 1) % 3] = 0;
                     s_kept[(rho + 1) % 3] = 0;
+                    s_bign[(rho + 2) % 3] = 0;
                 }
             }
             cl.sync();
-            if (threadIdx.x == 0) s_rd_cnt = r0_cnt[rho % 3];
+            if (threadIdx.x == 0) {
+                s_rd_cnt = r0_cnt[rho % 3];
+                s_rd_nb = min(r0_bign[(rho + 1) % 3], EGC_BIG_MAX);
+            }
             __syncthreads();
             pushes = s_rd_cnt;
             tr_items += pushes;
             rho++;
+        }
+        if (pushes) {  // the round bound ended the level with rows unexpanded
+            failed = true;  // (the cluster-wide count: every block breaks)
+            break;
         }
         if (trl) {
             if (r == 0) {
@@ -1886,8 +1955,8 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
             }
             atomicAdd(trl + 3, tr_entries);  // every block's rows
         }
-        // counts are rebuilt by the next scan: clear the kept ones
-        for (uint32_t i = threadIdx.x; i < (mo_max + 1) / 2; i += blockDim.x) cw[i] = 0;
+        // counts are rebuilt by the next scan: every half back to EGC_DEAD
+        for (uint32_t i = threadIdx.x; i < (mo_max + 1) / 2; i += blockDim.x) cw[i] = EGC_DEAD2;
         na = s_next;
         uint16_t* tmp = cur;
         cur = nxt;
@@ -1978,10 +2047,21 @@ static uint32_t eg_cluster_size() {
     return cs;
 }
 
+// Rows longer than this are expanded by every block of the cluster, a slice
+// each, instead of by their owner alone: FC_PEEL_EG_SPLIT (entries; 0 = never)
+static uint32_t eg_split() {
+    static const uint32_t v = env_u32("FC_PEEL_EG_SPLIT", 1024);
+    return v;
+}
+
 // survivors one column's endgame can hold with cs blocks (0: off for this L)
 // FC_PEEL_EG_CAP lowers it (the endgame then starts later)
 static uint32_t eg_column_capacity(uint32_t L, uint32_t cs) {
-    const uint32_t cap = cs > 1 ? cs * egc_block_capacity(L) : eg_capacity(L);
+    // Degrees are 16-bit halves, and a survivor's degree in a layer is below
+    // its column's survivor count: at most 65,536 survivors keep them exact.
+    // (Where the endgame starts moves c3's peel stage by less than 1 %.)
+    uint32_t cap = cs > 1 ? cs * egc_block_capacity(L) : eg_capacity(L);
+    if (cap > 65536u) cap = 65536u;
     const uint32_t want = env_u32("FC_PEEL_EG_CAP", 0);
     return want && want < cap ? want : cap;
 }
@@ -2089,7 +2169,7 @@ static fc_status endgame_run(const PeelJob& j, const PeelGraph& g, const PeelCtl
                     &cfg, k_endgame_cl, capE, (const uint32_t*)c->eg_cnt, (const uint32_t*)rowptr,
                     (const uint64_t*)c->eg_base, (const uint32_t*)H, (const uint32_t*)l2g, deg, g.n,
                     g.L, divL, j.seg0.t, col0, K + 1, j.max_level, c->eg_levels, &c->eg_err,
-                    etr);
+                    etr, eg_split());
                 count_launch(5);
                 if (le != cudaSuccess) {
                     set_last_cuda_error(le, "k_endgame_cl", __FILE__, __LINE__);
