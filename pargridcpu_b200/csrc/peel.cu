@@ -1681,6 +1681,45 @@ constexpr uint32_t EGC_CNT = 0x3FFFu;
 // Long rows queued in one round, per cluster (more go to their owners)
 constexpr uint32_t EGC_BIG_MAX = 256;
 
+// Block 0's counters of round rho + 1 (pushes, kept nodes) and its long-row
+// list of round rho + 2 start empty; called at the start of round rho, when
+// every block has read what they held three rounds before.
+__device__ __forceinline__ void egc_reset(uint32_t* cnt, uint32_t* kept, uint32_t* bign,
+                                          uint32_t rho) {
+    cnt[(rho + 1) % 3] = 0;
+    kept[(rho + 1) % 3] = 0;
+    bign[(rho + 2) % 3] = 0;
+}
+
+// adds the calling threads of a warp to a (remote) counter with one atomic
+__device__ __forceinline__ void egc_count(uint32_t* p) {
+    const uint32_t am = __activemask();
+    if ((threadIdx.x & 31) == (uint32_t)(__ffs(am) - 1)) atomicAdd(p, (uint32_t)__popc(am));
+}
+
+// Block-wide exclusive scan of 32 warps' values with one barrier: each warp
+// scans the warp totals itself.  Two calls need a barrier between them.
+__device__ __forceinline__ uint32_t egc_block_scan(uint32_t v, uint32_t* excl, uint32_t* s_warp) {
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t in = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, in, d);
+        if (lane >= (uint32_t)d) in += t;
+    }
+    if (lane == 31) s_warp[w] = in;
+    __syncthreads();
+    const uint32_t x = s_warp[lane];
+    uint32_t y = x;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, y, d);
+        if (lane >= (uint32_t)d) y += t;
+    }
+    *excl = __shfl_sync(0xffffffffu, y - x, w) + in - v;
+    return __shfl_sync(0xffffffffu, y, 31);
+}
+
 // appends column-local node u to block 0's list of long rows for a round
 __device__ __forceinline__ bool egc_push_big(uint32_t* big, uint32_t* bign, uint32_t slot,
                                              uint32_t u) {
@@ -1718,9 +1757,8 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
     uint32_t split) {
     extern __shared__ __align__(16) uint32_t sm[];
     __shared__ uint32_t s_warp[33];
-    __shared__ uint32_t s_next, s_qe, s_pushed, s_tail[2];
+    __shared__ uint32_t s_next, s_tail[2];
     __shared__ uint32_t s_cnt[3], s_kept[3];  // block 0's are the cluster's
-    __shared__ uint32_t s_rd_cnt, s_rd_kept, s_rd_nb;  // what this block read after a barrier
     __shared__ uint32_t s_big[3][EGC_BIG_MAX], s_bign[3];  // block 0's are the cluster's
     cg::cluster_group cl = cg::this_cluster();
     const uint32_t CS = cl.num_blocks();
@@ -1785,8 +1823,8 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
         unsigned long long tr_entries = 0, tr_rounds = 0, tr_items = 0;
         if (threadIdx.x == 0) {
             s_next = 0;
-            s_pushed = 0;
             s_tail[0] = s_tail[1] = 0;  // no block queues remotely during a scan round
+            if (r == 0) egc_reset(s_cnt, s_kept, s_bign, rho);
             if (trl && r == 0) trl[0] = global_ns();
         }
         __syncthreads();
@@ -1799,54 +1837,38 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
             if (cnt < lmd) {
                 alive[x] = 0;
                 tc[g_of[(x << lg) + r]] = k;
-                if (ax == 2 && egc_push_big(r0_big, r0_bign, (rho + 1) % 3, (x << lg) + r))
-                    atomicAdd(&s_pushed, 1u);
-                else
+                if (!(ax == 2 && egc_push_big(r0_big, r0_bign, (rho + 1) % 3, (x << lg) + r)))
                     qh[qn][atomicAdd(&s_tail[qn], 1u)] = (uint16_t)x;
+                egc_count(r0_cnt + rho % 3);
             } else {
                 // EGC_DEAD -> cnt, with the long-row flag
                 const uint32_t v = cnt | (ax == 2 ? EGC_BIG : 0u);
                 atomicSub(cw + (x >> 1), (EGC_DEAD - v) << ((x & 1) * 16));
                 nxt[atomicAdd(&s_next, 1u)] = (uint16_t)x;
+                egc_count(r0_kept + rho % 3);
             }
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            if (s_tail[qn] + s_pushed) atomicAdd(r0_cnt + rho % 3, s_tail[qn] + s_pushed);
-            if (s_next) atomicAdd(r0_kept + rho % 3, s_next);
-            if (r == 0) {
-                s_cnt[(rho + 1) % 3] = 0;
-                s_kept[(rho + 1) % 3] = 0;
-                s_bign[(rho + 2) % 3] = 0;
-            }
-        }
-        cl.sync();
-        if (threadIdx.x == 0) {
-            s_rd_cnt = r0_cnt[rho % 3];
-            s_rd_kept = r0_kept[rho % 3];
-            s_rd_nb = min(r0_bign[(rho + 1) % 3], EGC_BIG_MAX);  // the next round's long rows
-        }
-        __syncthreads();
-        const uint32_t kept = s_rd_kept;
+        cl.sync();  // every block's counts are in block 0, every queue is final
+        const uint32_t kept = r0_kept[rho % 3];
+        const uint32_t scanned = r0_cnt[rho % 3];
+        uint32_t nbig = min(r0_bign[(rho + 1) % 3], EGC_BIG_MAX);  // the next round's long rows
         // with no survivor left in the column the rows of this scan's
         // removals name no node that could still change
-        uint32_t pushes = kept ? s_rd_cnt : 0u;
-        tr_items = s_rd_cnt;
+        uint32_t pushes = kept ? scanned : 0u;
+        tr_items = scanned;
         rho++;
         // DRAIN rounds while the last round queued anything (bounded: every
         // node is queued at most once per level)
         for (uint32_t round = 0; pushes && round <= m; round++) {
             const uint32_t qc = rho & 1, qp = (rho + 1) & 1;
-            if (threadIdx.x == 0) {
-                s_qe = s_tail[qc];
-                s_pushed = 0;
-            }
-            __syncthreads();
-            // this block's queued rows, then its slice of every long row
-            const uint32_t qe = s_qe, nbig = s_rd_nb, items = qe + nbig;
+            // this block's queued rows, then its slice of every long row (the
+            // queue half and the list are final since the cluster barrier)
+            const uint32_t qe = s_tail[qc], items = qe + nbig;
             const uint32_t* const bl = r0_big + (rho % 3) * EGC_BIG_MAX;
+            if (threadIdx.x == 0 && r == 0) egc_reset(s_cnt, s_kept, s_bign, rho);
             tr_rounds++;
             for (uint32_t b0 = 0; b0 < items; b0 += EG_THREADS) {
+                if (b0) __syncthreads();  // the last batch's pre and rs are read
                 const uint32_t nb = min(EG_THREADS, items - b0);
                 uint32_t len = 0, start = 0;
                 const uint32_t it = b0 + threadIdx.x;
@@ -1864,7 +1886,10 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
                     if ((u & (CS - 1)) == r) tc[g_of[u]] = k;  // its owner
                 }
                 uint32_t ex;
-                const uint32_t total = eg_block_scan(len, &ex, s_warp);
+                const uint32_t total = egc_block_scan(len, &ex, s_warp);
+                // every thread has read the queue's length (before the
+                // scan's barrier): the half takes round rho + 1's queue
+                if (b0 == 0 && threadIdx.x == 0) s_tail[qc] = 0;
                 tr_entries += total;
                 pre[threadIdx.x] = ex;
                 rs[threadIdx.x] = start;
@@ -1920,27 +1945,13 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
                             const uint32_t pos = atomicAdd(t_ow + qp, 1u);
                             cl.map_shared_rank(qh[qp], ow[q])[pos] = (uint16_t)ui[q];
                         }
-                        atomicAdd(&s_pushed, 1u);
+                        egc_count(r0_cnt + rho % 3);
                     }
                 }
-                __syncthreads();
             }
-            if (threadIdx.x == 0) {
-                s_tail[qc] = 0;  // this half is consumed; it takes round rho + 1's queue
-                if (s_pushed) atomicAdd(r0_cnt + rho % 3, s_pushed);
-                if (r == 0) {
-                    s_cnt[(rho + 1) % 3] = 0;
-                    s_kept[(rho + 1) % 3] = 0;
-                    s_bign[(rho + 2) % 3] = 0;
-                }
-            }
-            cl.sync();
-            if (threadIdx.x == 0) {
-                s_rd_cnt = r0_cnt[rho % 3];
-                s_rd_nb = min(r0_bign[(rho + 1) % 3], EGC_BIG_MAX);
-            }
-            __syncthreads();
-            pushes = s_rd_cnt;
+            cl.sync();  // every push is counted in block 0 and queued
+            pushes = r0_cnt[rho % 3];
+            nbig = min(r0_bign[(rho + 1) % 3], EGC_BIG_MAX);
             tr_items += pushes;
             rho++;
         }
@@ -2050,7 +2061,7 @@ static uint32_t eg_cluster_size() {
 // Rows longer than this are expanded by every block of the cluster, a slice
 // each, instead of by their owner alone: FC_PEEL_EG_SPLIT (entries; 0 = never)
 static uint32_t eg_split() {
-    static const uint32_t v = env_u32("FC_PEEL_EG_SPLIT", 1024);
+    static const uint32_t v = env_u32("FC_PEEL_EG_SPLIT", 512);
     return v;
 }
 
