@@ -86,7 +86,7 @@ struct PeelCtl {
     Hot processed[2][2];  // [q][s] items fully processed
     // endgame (one block per column): survivors, subgraph entries, levels run
     uint32_t eg_cnt[64], eg_tot[64], eg_levels[64];
-    uint32_t eg_err, eg_pad[3];
+    uint32_t eg_err, eg_nbig, eg_pad[2];  // eg_nbig: long rows listed for k_eg_fill_big
     uint64_t eg_base[64];  // first entry of each column's subgraph
 };
 
@@ -1333,9 +1333,11 @@ __device__ __forceinline__ uint32_t eg_block_scan(uint32_t v, uint32_t* excl, ui
 __global__ void __launch_bounds__(EG_THREADS) k_eg_scan(const uint32_t* __restrict__ rowlen,
                                                         uint32_t* __restrict__ rowptr, uint32_t cap,
                                                         const uint32_t* __restrict__ ecnt,
-                                                        uint32_t* __restrict__ etot) {
+                                                        uint32_t* __restrict__ etot,
+                                                        uint32_t* __restrict__ nbig) {
     __shared__ uint32_t s_warp[33];
     const uint32_t c = blockIdx.x;
+    if (c == 0 && threadIdx.x == 0) *nbig = 0;  // k_eg_fill lists the long rows
     const uint32_t m = min(ecnt[c], cap);
     const uint32_t* in = rowlen + (uint64_t)c * (cap + 1);
     uint32_t* out = rowptr + (uint64_t)c * (cap + 1);
@@ -1375,7 +1377,8 @@ __device__ __forceinline__ uint32_t eg_need(const uint32_t* __restrict__ node_pt
 // One warp per survivor whose row part is at most EG_FILL_SPLIT entries: its
 // subgraph row, the alive neighbours in row order, as local slots lid * L + l.
 // Rows whose alive-neighbour count differs from the degrees the peel kept
-// flag an error.
+// flag an error.  A longer row's node is appended to `list` (capacity lcap,
+// count *nbig) for k_eg_fill_big.
 __global__ void k_eg_fill(const uint32_t* __restrict__ alive, uint32_t nalive,
                           const uint32_t* __restrict__ bits, FastDiv divN, FastDiv divL, uint32_t n,
                           uint32_t L, const uint32_t* __restrict__ node_ptr,
@@ -1383,7 +1386,8 @@ __global__ void k_eg_fill(const uint32_t* __restrict__ alive, uint32_t nalive,
                           const uint32_t* __restrict__ ptab, uint32_t k1,
                           const uint32_t* __restrict__ map, uint32_t cap,
                           const uint32_t* __restrict__ rowptr, const uint64_t* __restrict__ base,
-                          uint32_t* __restrict__ H, uint32_t* __restrict__ err) {
+                          uint32_t* __restrict__ H, uint32_t* __restrict__ err,
+                          uint32_t* __restrict__ list, uint32_t lcap, uint32_t* __restrict__ nbig) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t lt = (1u << lane) - 1u;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -1398,7 +1402,14 @@ __global__ void k_eg_fill(const uint32_t* __restrict__ alive, uint32_t nalive,
         uint32_t* dst = H + base[c] + o0;
         uint32_t rb;
         const uint32_t need = eg_need(node_ptr, big_id, ptab, v, k1, &rb);
-        if (need > EG_FILL_SPLIT) continue;  // k_eg_fill_big
+        if (need > EG_FILL_SPLIT) {  // k_eg_fill_big
+            if (lane == 0) {
+                const uint32_t pos = atomicAdd(nbig, 1u);
+                if (pos < lcap) list[pos] = x;
+                else atomicExch(err, 1u);
+            }
+            continue;
+        }
         uint32_t got = 0;
         for (uint32_t p0 = 0; p0 < need; p0 += 32) {
             const uint32_t p = p0 + lane;
@@ -1422,26 +1433,27 @@ __global__ void k_eg_fill(const uint32_t* __restrict__ alive, uint32_t nalive,
     }
 }
 
-// One block per survivor whose row part exceeds EG_FILL_SPLIT entries, in
-// tiles of 4 * EG_THREADS entries: each thread counts its four, a block scan
-// places them (thread-major within a tile; deterministic).
+// One block per survivor whose row part exceeds EG_FILL_SPLIT entries (the
+// nodes k_eg_fill listed), in tiles of 4 * EG_THREADS entries: each thread
+// counts its four, a block scan places them (thread-major within a tile;
+// deterministic, whatever the list's order).
 __global__ void __launch_bounds__(EG_THREADS) k_eg_fill_big(
-    const uint32_t* __restrict__ alive, uint32_t nalive, const uint32_t* __restrict__ bits,
-    FastDiv divN, FastDiv divL, uint32_t n, uint32_t L, const uint32_t* __restrict__ node_ptr,
+    const uint32_t* __restrict__ bits, FastDiv divN, FastDiv divL, uint32_t n, uint32_t L,
+    const uint32_t* __restrict__ node_ptr,
     const uint32_t* __restrict__ adj, const uint32_t* __restrict__ big_id,
     const uint32_t* __restrict__ ptab, uint32_t k1, const uint32_t* __restrict__ map, uint32_t cap,
     const uint32_t* __restrict__ rowptr, const uint64_t* __restrict__ base,
-    uint32_t* __restrict__ H, uint32_t* __restrict__ err) {
+    uint32_t* __restrict__ H, uint32_t* __restrict__ err, const uint32_t* __restrict__ list,
+    uint32_t lcap, const uint32_t* __restrict__ nbig) {
     __shared__ uint32_t s_warp[33];
-    for (uint32_t i = blockIdx.x; i < nalive; i += gridDim.x) {
-        const uint32_t x = alive[i];
-        if (!((bits[x >> 5] >> (x & 31)) & 1u)) continue;
+    const uint32_t nl = min(*nbig, lcap);
+    for (uint32_t i = blockIdx.x; i < nl; i += gridDim.x) {
+        const uint32_t x = list[i];
         const uint32_t c = divN.div(x), v = x - c * n;
         const uint32_t lid = map[x];
         if (lid >= cap) continue;
         uint32_t rb;
         const uint32_t need = eg_need(node_ptr, big_id, ptab, v, k1, &rb);
-        if (need <= EG_FILL_SPLIT) continue;  // k_eg_fill
         const uint32_t* rp = rowptr + (uint64_t)c * (cap + 1);
         const uint32_t o0 = rp[lid], want = rp[lid + 1] - o0;
         uint32_t* dst = H + base[c] + o0;
@@ -2133,7 +2145,8 @@ static fc_status endgame_run(const PeelJob& j, const PeelGraph& g, const PeelCtl
         if (cnts[i] > capE) return FC_ERR_DEVICE;  // more survivors than the stop rule allows
         mmax = cnts[i] > mmax ? cnts[i] : mmax;
     }
-    k_eg_scan<<<ncols, EG_THREADS, 0, s>>>(rowlen, rowptr, capE, c->eg_cnt, c->eg_tot);
+    k_eg_scan<<<ncols, EG_THREADS, 0, s>>>(rowlen, rowptr, capE, c->eg_cnt, c->eg_tot,
+                                           &c->eg_nbig);
     FC_CUDA_TRY(cudaGetLastError());
     FC_TRY(to_host(tots, c->eg_tot, 4ull * ncols, s));
     uint64_t bases[EG_MAX_COLS], total = 0;
@@ -2149,12 +2162,16 @@ static fc_status endgame_run(const PeelJob& j, const PeelGraph& g, const PeelCtl
     }
     fc_status rc = to_device(c->eg_base, bases, 8ull * ncols, s);
     if (rc == FC_OK) {
+        // the long rows' list takes the row lengths' buffer (spent after
+        // k_eg_scan; its capacity exceeds the survivors)
+        uint32_t* const big_list = rowlen;
         k_eg_fill<<<blocks, 256, 0, s>>>(alive, nalive, j.bits, divN, divL, g.n, g.L, g.node_ptr,
                                          g.adj, g.big_id, g.ptab, K + 1, map, capE, rowptr,
-                                         c->eg_base, H, &c->eg_err);
+                                         c->eg_base, H, &c->eg_err, big_list, j.qs_cap,
+                                         &c->eg_nbig);
         k_eg_fill_big<<<peel_sms() * 2, EG_THREADS, 0, s>>>(
-            alive, nalive, j.bits, divN, divL, g.n, g.L, g.node_ptr, g.adj, g.big_id, g.ptab, K + 1,
-            map, capE, rowptr, c->eg_base, H, &c->eg_err);
+            j.bits, divN, divL, g.n, g.L, g.node_ptr, g.adj, g.big_id, g.ptab, K + 1, map, capE, rowptr,
+            c->eg_base, H, &c->eg_err, big_list, j.qs_cap, &c->eg_nbig);
         static const cudaError_t attr_rc = cudaFuncSetAttribute(
             k_endgame, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)EG_SMEM);
         if (cs > 1) {
