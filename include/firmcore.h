@@ -142,6 +142,15 @@ fc_status fc_coreindex(fc_graph* g, uint32_t* out, int out_on_device, void* stre
  * resident.  One result per beta. */
 fc_status fc_densest(fc_graph* g, const double* betas, uint32_t n_betas, fc_densest_result* res,
                      void* stream);
+/* The core table into `table` (host memory, L*n words, as fc_coreindex with
+ * out_on_device = 0; may be NULL) and the densest results for `betas` (as
+ * fc_densest) in one call -- a -m ParGrid run and a -m WdsList run of the
+ * reference (main.cpp:229-239, 402-424) on one graph.  When `table` is pinned
+ * host memory its copy runs on the library's copy stream while the densest
+ * kernels run on `stream`; otherwise the copy comes first.  Returns when both
+ * are complete. */
+fc_status fc_coreindex_densest(fc_graph* g, uint32_t* table, const double* betas,
+                               uint32_t n_betas, fc_densest_result* res, void* stream);
 /* Node set (ascending internal ids, res->length entries) and layer set
  * (ascending layer indices, res->lstar entries) of a result from fc_densest
  * on the same graph.  Either pointer may be NULL. */

@@ -179,6 +179,20 @@ class MultilayerGraph:
                                      _n.stream_handle(stream)), "densest")
         return [r.as_dict() for r in res]
 
+    def coreindex_densest(self, out=None, betas=(1.0,), stream=None):
+        """The L x n core table into host memory (``out``, a new array when
+        None) and the densest results for ``betas``, in one call: with a
+        pinned ``out`` the table's copy overlaps the densest search.
+        Returns (table, results)."""
+        if out is None:
+            out = np.zeros((self.L, self.n), np.uint32)
+        betas = np.ascontiguousarray(np.atleast_1d(np.asarray(betas, np.float64)))
+        res = (_n.DensestResult * len(betas))()
+        _n.check(_n.lib().fc_coreindex_densest(self._h, _n.ptr(out), _n.ptr(betas), len(betas),
+                                               C.cast(res, C.c_void_p),
+                                               _n.stream_handle(stream)), "coreindex_densest")
+        return out, [r.as_dict() for r in res]
+
     def densest_members(self, result):
         r = _n.DensestResult(**{k: result[k] for k, _ in _n.DensestResult._fields_})
         nodes = np.zeros(max(r.length, 1), np.uint32)

@@ -61,6 +61,48 @@ fc_status coreindex(fc_graph* g, uint32_t* out, bool out_on_device, cudaStream_t
     return FC_OK;
 }
 
+// The table into `table` (host memory) and the densest search for `betas`:
+// when the buffer is pinned, its copy runs on the library's copy stream while
+// the densest kernels run on s; otherwise the copy comes first.  Results as
+// coreindex + densest.
+fc_status coreindex_densest(fc_graph* g, uint32_t* table, const double* betas, uint32_t nb,
+                            fc_densest_result* res, cudaStream_t s) {
+    FC_TRY(coreindex(g, nullptr, false, s));
+    DeviceGraph* d = g->dev;
+    const uint64_t bytes = (uint64_t)d->n * d->L * 4;
+    struct Events {  // destroyed on every return
+        cudaEvent_t peeled = nullptr, copied = nullptr;
+        ~Events() {
+            if (peeled) cudaEventDestroy(peeled);
+            if (copied) cudaEventDestroy(copied);
+        }
+    } ev;
+    bool overlap = false;
+    if (table && bytes) {
+        cudaPointerAttributes a{};
+        const bool pinned = cudaPointerGetAttributes(&a, table) == cudaSuccess &&
+                            a.type == cudaMemoryTypeHost;
+        cudaGetLastError();  // pageable memory is not an error
+        cudaStream_t cs = pinned ? library_copy_stream() : nullptr;
+        if (cs && cs != s &&
+            cudaEventCreateWithFlags(&ev.peeled, cudaEventDisableTiming) == cudaSuccess &&
+            cudaEventCreateWithFlags(&ev.copied, cudaEventDisableTiming) == cudaSuccess) {
+            count_alloc(2);
+            FC_CUDA_TRY(cudaEventRecord(ev.peeled, s));
+            FC_CUDA_TRY(cudaStreamWaitEvent(cs, ev.peeled, 0));
+            FC_CUDA_TRY(cudaMemcpyAsync(table, d->table, bytes, cudaMemcpyDeviceToHost, cs));
+            FC_CUDA_TRY(cudaEventRecord(ev.copied, cs));
+            overlap = true;
+        } else {
+            cudaGetLastError();
+            FC_TRY(to_host(table, d->table, bytes, s));
+        }
+    }
+    const fc_status rc = densest(g, betas, nb, res, s);
+    if (overlap) FC_CUDA_TRY(cudaEventSynchronize(ev.copied));  // even when densest failed
+    return rc;
+}
+
 // Columns [lo, hi) of the table (0-based); out (may be NULL) receives them,
 // (hi - lo) rows of n.  Peels only those columns unless the whole table, or
 // a range covering them, is already resident.
@@ -187,7 +229,8 @@ fc_status fc_graph_order(const fc_graph* g, uint32_t* out) {
 fc_status fc_graph_csr(const fc_graph* g, uint64_t* off, uint32_t* adj) {
     if (!g) return FC_ERR_INVALID;
     uint64_t no = (uint64_t)g->L * (g->n + 1);
-    if (off && no) memcpy(off, g->off.p, no * 8);
+    if (off)
+        for (uint64_t i = 0; i < no; i++) off[i] = g->off.p[i];
     uint64_t na = g->total_entries();
     if (adj && na) memcpy(adj, g->adj.p, na * 4);
     return FC_OK;
@@ -219,6 +262,16 @@ uint64_t fc_graph_device_bytes(const fc_graph* g) { return g ? device_bytes(g) :
 fc_status fc_coreindex(fc_graph* g, uint32_t* out, int out_on_device, void* stream) {
     if (!g) return FC_ERR_INVALID;
     return coreindex(g, out, out_on_device != 0, (cudaStream_t)stream);
+}
+
+fc_status fc_coreindex_densest(fc_graph* g, uint32_t* table, const double* betas,
+                               uint32_t n_betas, fc_densest_result* res, void* stream) {
+    if (!g || (n_betas && (!betas || !res))) return FC_ERR_INVALID;
+    if (!g->n || !g->L) {
+        FC_TRY(fc_coreindex(g, table, 0, stream));
+        return fc_densest(g, betas, n_betas, res, stream);
+    }
+    return coreindex_densest(g, table, betas, n_betas, res, (cudaStream_t)stream);
 }
 
 fc_status fc_densest(fc_graph* g, const double* betas, uint32_t n_betas, fc_densest_result* res,

@@ -135,10 +135,9 @@ __global__ void k_node_hist(const uint32_t* __restrict__ table, uint32_t n,
 // per lane), and tracks each lane's source node by advancing along node_ptr.
 // Bins live in shared memory when they fit (`sh_ok`), else in global memory.
 // The entry (v, u, l) adds one to bin (l, min(core(v), core(u))) per column.
-// With `runs` set, the entries whose key is v's own core (core(u) >= core(v))
-// are counted per run of adjacent lanes with the same (v, l) and added by the
-// run's first lane with one atomic; measured slower than one atomic per
-// entry on c3, so off by default.
+// The adjacency is symmetric (every (v, u, l) has its (u, v, l), in the same
+// bin), so only the entry with u > v is visited and adds two; a self-loop
+// (u = v, one entry) adds one.  The histogram is the same.
 __device__ __forceinline__ void edge_bin_add(uint32_t* sh, uint32_t* H, bool sh_ok, uint32_t soff,
                                              uint64_t hbase, uint32_t l, uint32_t km1,
                                              uint32_t key, uint32_t cnt) {
@@ -148,13 +147,13 @@ __device__ __forceinline__ void edge_bin_add(uint32_t* sh, uint32_t* H, bool sh_
 
 // V4: the group is four columns starting at a multiple of four with L a
 // multiple of four, so a node's four core values are one aligned 16-byte
-// load.  runs = 0 adds every entry with its own atomic (no run counting).
+// load.
 template <bool V4>
 __global__ void k_edge_hist(const uint32_t* __restrict__ node_ptr, const uint32_t* __restrict__ adj,
                             uint32_t n, uint32_t L, uint64_t entries, FastDiv divL,
                             const uint32_t* __restrict__ coreT, uint32_t lam0, uint32_t nl,
                             const uint64_t* __restrict__ hbase, const uint32_t* __restrict__ kmax,
-                            uint32_t* __restrict__ H, uint32_t sh_words, int sh_ok, int runs) {
+                            uint32_t* __restrict__ H, uint32_t sh_words, int sh_ok) {
     extern __shared__ uint32_t sh[];
     __shared__ uint32_t soff[64];  // per column in the group: offset into sh
     if (threadIdx.x == 0) {
@@ -185,12 +184,10 @@ __global__ void k_edge_hist(const uint32_t* __restrict__ node_ptr, const uint32_
         uint32_t v = lo;
         uint32_t next_row = node_ptr[v + 1];
         uint4 A = V4 ? *(const uint4*)(coreT + (uint64_t)v * L + lam0) : make_uint4(0, 0, 0, 0);
-        const uint32_t below = (2u << lane) - 1u;  // lanes 0..lane (all 32 for lane 31)
         for (uint64_t b0 = e0; b0 < e1; b0 += 32) {
             const uint64_t e = b0 + lane;
-            const bool valid = e < e1;
-            uint32_t u = 0, l = 0;
-            if (valid) {
+            uint32_t u = 0, l = 0, w = 0;  // w: what the entry adds (0, 1 or 2)
+            if (e < e1) {
                 if (next_row <= e) {
                     do v++;
                     while (node_ptr[v + 1] <= e);
@@ -200,47 +197,24 @@ __global__ void k_edge_hist(const uint32_t* __restrict__ node_ptr, const uint32_
                 const uint32_t slot = adj[e];
                 u = divL.div(slot);
                 l = slot - u * L;
-            }
-            // runs of adjacent lanes with the same (v, l); v * L + l < n * L < 2^32
-            bool leader = true;
-            uint32_t run = 0;
-            if (runs) {
-                const uint32_t vl = valid ? v * L + l : 0xFFFFFFFFu;
-                const uint32_t prev = __shfl_up_sync(0xffffffffu, vl, 1);
-                const uint32_t starts = __ballot_sync(0xffffffffu, lane == 0 || prev != vl);
-                leader = (starts >> lane) & 1u;
-                const uint32_t above = starts & ~below;  // the next run's first lane, if any
-                const uint32_t run_end = above ? (uint32_t)__ffs(above) - 1u : 32u;
-                run = (run_end == 32u ? 0xFFFFFFFFu : ((1u << run_end) - 1u)) &
-                      ~((1u << lane) - 1u);  // this lane's run, when it leads it
+                w = u > v ? 2u : u == v ? 1u : 0u;
             }
             uint4 B = make_uint4(0, 0, 0, 0);
-            if (V4 && valid && (A.x | A.y | A.z | A.w))
+            if (V4 && w && (A.x | A.y | A.z | A.w))
                 B = *(const uint4*)(coreT + (uint64_t)u * L + lam0);
             for (uint32_t i = 0; i < nl; i++) {
                 uint32_t a = 0, b = 0;
                 if (V4) {
                     a = i == 0 ? A.x : i == 1 ? A.y : i == 2 ? A.z : A.w;
                     b = i == 0 ? B.x : i == 1 ? B.y : i == 2 ? B.z : B.w;
-                    if (!valid) a = 0;
-                } else if (valid) {
+                } else if (w) {
                     a = coreT[(uint64_t)v * L + lam0 + i];
                     if (a) b = coreT[(uint64_t)u * L + lam0 + i];
                 }
-                const uint32_t km1 = kmax[lam0 + i] + 1;
-                if (runs) {
-                    const bool own = a && b >= a;  // key = a, counted by the run
-                    const uint32_t own_mask = __ballot_sync(0xffffffffu, own);
-                    if (leader && a) {
-                        const uint32_t cnt = __popc(own_mask & run);
-                        if (cnt) edge_bin_add(sh, H, sh_ok, soff[i], hbase[lam0 + i], l, km1, a, cnt);
-                    }
-                    if (a && b && b < a)
-                        edge_bin_add(sh, H, sh_ok, soff[i], hbase[lam0 + i], l, km1, b, 1u);
-                } else {
-                    const uint32_t key = min(a, b);
-                    if (key) edge_bin_add(sh, H, sh_ok, soff[i], hbase[lam0 + i], l, km1, key, 1u);
-                }
+                const uint32_t key = w ? min(a, b) : 0u;
+                if (key)
+                    edge_bin_add(sh, H, sh_ok, soff[i], hbase[lam0 + i], l, kmax[lam0 + i] + 1,
+                                 key, w);
             }
         }
     }
@@ -488,17 +462,14 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st, uint32_t lo, uint32
             int sh_ok = words <= SH_WORDS;
             size_t shb = sh_ok ? (size_t)words * 4 : 0;
             if (d->entries) {
-                // run counting (FC_DENSEST_RUNS=1) measured slower on c3 (1.95 against
-                // 1.78 ms per search): off by default
-                static const int runs = getenv("FC_DENSEST_RUNS") ? atoi(getenv("FC_DENSEST_RUNS")) : 0;
                 if (nl == 4 && L % 4 == 0 && lam % 4 == 0)
                     k_edge_hist<true><<<blocks, 1024, shb, st>>>(
                         d->node_ptr, d->adj, n, L, d->entries, divL, s->coreT, lam, nl, s->d_hbase,
-                        s->d_kmax, s->H, words, sh_ok, runs);
+                        s->d_kmax, s->H, words, sh_ok);
                 else
                     k_edge_hist<false><<<blocks, 1024, shb, st>>>(
                         d->node_ptr, d->adj, n, L, d->entries, divL, s->coreT, lam, nl, s->d_hbase,
-                        s->d_kmax, s->H, words, sh_ok, runs);
+                        s->d_kmax, s->H, words, sh_ok);
                 count_launch();
             }
             FC_CUDA_TRY(cudaGetLastError());

@@ -129,6 +129,9 @@ void set_thread_staging(Staging* st);
 // device -> host, waits for the copy; host -> device, waits only when staged
 fc_status to_host(void* h, const void* d, size_t bytes, cudaStream_t s);
 fc_status to_device(void* d, const void* h, size_t bytes, cudaStream_t s);
+// the library's copy stream of the current device (made once; null when it
+// cannot be made)
+cudaStream_t library_copy_stream();
 
 // kernels launched by this library (fc_launch_count)
 void count_launch(uint32_t k = 1);

@@ -46,11 +46,14 @@ struct fc_graph {
     uint32_t n = 0, L = 0;
     std::vector<uint32_t> order;   // -o permutation (file layer index of logical layer i)
     std::vector<uint64_t> id2vtx;  // internal id -> raw id
-    fc::HostBuf<uint64_t> off;     // L*(n+1), absolute indices into adj
+    // L*(n+1) absolute indices into adj, 32-bit: a graph holds fewer than
+    // 2^32 adjacency entries (FC_ERR_TOO_LARGE at load), and the upload
+    // copies half the bytes of 64-bit offsets
+    fc::HostBuf<uint32_t> off;
     fc::HostBuf<uint32_t> adj;     // all layers' rows, layer after layer
     uint64_t total_entries() const { return L ? off[(uint64_t)L * (n + 1) - 1] : 0; }
     uint64_t layer_m(uint32_t l) const {
-        const uint64_t* o = off.p + (uint64_t)l * (n + 1);
+        const uint32_t* o = off.p + (uint64_t)l * (n + 1);
         return o[n] - o[0];
     }
     fc::DeviceGraph* dev = nullptr;
@@ -73,6 +76,8 @@ fc_status upload(fc_graph* g, cudaStream_t s);
 void release_device(fc_graph* g, bool wait_home = true);
 uint64_t device_bytes(const fc_graph* g);
 fc_status coreindex(fc_graph* g, uint32_t* out, bool out_on_device, cudaStream_t s);
+fc_status coreindex_densest(fc_graph* g, uint32_t* table, const double* betas, uint32_t nb,
+                            fc_densest_result* res, cudaStream_t s);
 fc_status densest(fc_graph* g, const double* betas, uint32_t nb, fc_densest_result* res,
                   cudaStream_t s);
 fc_status densest_members(fc_graph* g, const fc_densest_result* r, uint32_t* nodes,

@@ -34,12 +34,12 @@ bool cuda_available() {
 }
 
 // deg0[v*L + l] and the row length of every node, from per-layer offsets.
-__global__ void k_degrees(const uint64_t* __restrict__ off, uint32_t n, uint32_t L,
+__global__ void k_degrees(const uint32_t* __restrict__ off, uint32_t n, uint32_t L,
                           uint32_t* __restrict__ deg0, uint32_t* __restrict__ rowlen) {
     for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
         uint32_t sum = 0;
         for (uint32_t l = 0; l < L; l++) {
-            const uint64_t* o = off + (uint64_t)l * (n + 1);
+            const uint32_t* o = off + (uint64_t)l * (n + 1);
             uint32_t d = (uint32_t)(o[v + 1] - o[v]);
             deg0[(uint64_t)v * L + l] = d;
             sum += d;
@@ -50,7 +50,7 @@ __global__ void k_degrees(const uint64_t* __restrict__ off, uint32_t n, uint32_t
 
 // One warp per node: copy its L layer rows into its node-major range as
 // slots; the rows longer than ORDER_MIN_ROW are left to the ordering kernels.
-__global__ void k_scatter(const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj_in,
+__global__ void k_scatter(const uint32_t* __restrict__ off, const uint32_t* __restrict__ adj_in,
                           const uint32_t* __restrict__ node_ptr, uint32_t n, uint32_t L,
                           uint32_t* __restrict__ adj_out) {
     const uint32_t lane = threadIdx.x & 31;
@@ -59,7 +59,7 @@ __global__ void k_scatter(const uint64_t* __restrict__ off, const uint32_t* __re
         uint32_t dst = node_ptr[v];
         if (node_ptr[v + 1] - dst > ORDER_MIN_ROW) continue;  // written ordered (k_order_scatter)
         for (uint32_t l = 0; l < L; l++) {
-            const uint64_t* o = off + (uint64_t)l * (n + 1);
+            const uint32_t* o = off + (uint64_t)l * (n + 1);
             uint64_t b = o[v], e = o[v + 1];
             for (uint64_t j = b + lane; j < e; j += 32) adj_out[dst + (j - b)] = adj_in[j] * L + l;
             dst += (uint32_t)(e - b);
@@ -70,7 +70,7 @@ __global__ void k_scatter(const uint64_t* __restrict__ off, const uint32_t* __re
 // The same for layers [l0, l1) only: a row's layer l starts after its
 // layers below l (their degrees from deg0).  The upload scatters each group
 // of layers as soon as its part of the input has arrived.
-__global__ void k_scatter_layers(const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj_in,
+__global__ void k_scatter_layers(const uint32_t* __restrict__ off, const uint32_t* __restrict__ adj_in,
                                  const uint32_t* __restrict__ node_ptr,
                                  const uint32_t* __restrict__ deg0, uint32_t n, uint32_t L,
                                  uint32_t l0, uint32_t l1, uint32_t* __restrict__ adj_out) {
@@ -81,7 +81,7 @@ __global__ void k_scatter_layers(const uint64_t* __restrict__ off, const uint32_
         if (node_ptr[v + 1] - dst > ORDER_MIN_ROW) continue;  // written ordered (k_order_scatter)
         for (uint32_t l = 0; l < l0; l++) dst += deg0[(uint64_t)v * L + l];
         for (uint32_t l = l0; l < l1; l++) {
-            const uint64_t* o = off + (uint64_t)l * (n + 1);
+            const uint32_t* o = off + (uint64_t)l * (n + 1);
             uint64_t b = o[v], e = o[v + 1];
             for (uint64_t j = b + lane; j < e; j += 32) adj_out[dst + (j - b)] = adj_in[j] * L + l;
             dst += (uint32_t)(e - b);
@@ -141,7 +141,7 @@ __global__ void k_order_index(const uint32_t* __restrict__ fbig, const uint32_t*
 // whole warp for 32 consecutive positions at a time, in row order; a call
 // never spans two layers.
 template <class F>
-__device__ __forceinline__ void for_tile_entries(const uint64_t* __restrict__ off,
+__device__ __forceinline__ void for_tile_entries(const uint32_t* __restrict__ off,
                                                  const uint32_t* __restrict__ adj_in,
                                                  const uint32_t* __restrict__ deg0, uint32_t n,
                                                  uint32_t L, uint32_t v, uint32_t len, uint32_t i,
@@ -154,7 +154,7 @@ __device__ __forceinline__ void for_tile_entries(const uint64_t* __restrict__ of
         const uint32_t d = deg0[(uint64_t)v * L + l];
         const uint32_t a = max(s, p0), b = min(s + d, p1);
         if (a < b) {
-            const uint64_t ob = off[(uint64_t)l * (n + 1) + v] - s;
+            const uint64_t ob = (uint64_t)off[(uint64_t)l * (n + 1) + v] - s;
             for (uint32_t p = a; p < b; p += 32) {
                 const bool valid = p + lane < b;
                 const uint32_t u = valid ? adj_in[ob + p + lane] : 0u;
@@ -166,7 +166,7 @@ __device__ __forceinline__ void for_tile_entries(const uint64_t* __restrict__ of
 }
 
 // One warp per tile: its bucket histogram.
-__global__ void k_order_hist(const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj_in,
+__global__ void k_order_hist(const uint32_t* __restrict__ off, const uint32_t* __restrict__ adj_in,
                              const uint32_t* __restrict__ deg0, const uint32_t* __restrict__ node_ptr,
                              uint32_t n, uint32_t L, const uint32_t* __restrict__ ub,
                              const uint32_t* __restrict__ tile_row, const uint32_t* __restrict__ tscan,
@@ -208,7 +208,7 @@ __global__ void k_order_ptab(const uint32_t* __restrict__ big_v, const uint32_t*
 
 // One warp per tile: its entries as slots to their ordered places in the
 // row, ranked in row order within each bucket.
-__global__ void k_order_scatter(const uint64_t* __restrict__ off, const uint32_t* __restrict__ adj_in,
+__global__ void k_order_scatter(const uint32_t* __restrict__ off, const uint32_t* __restrict__ adj_in,
                                 const uint32_t* __restrict__ deg0, const uint32_t* __restrict__ node_ptr,
                                 uint32_t n, uint32_t L, const uint32_t* __restrict__ ub,
                                 const uint32_t* __restrict__ tile_row, const uint32_t* __restrict__ tscan,
@@ -371,7 +371,7 @@ struct TempBufs {
 // Writes the rows longer than ORDER_MIN_ROW, ordered by bound bucket, from
 // the per-layer input CSR (off, adj_in), and builds big_id and ptab
 // (device.h).
-static fc_status order_rows(DeviceGraph* d, const uint32_t* rowlen, const uint64_t* off,
+static fc_status order_rows(DeviceGraph* d, const uint32_t* rowlen, const uint32_t* off,
                             const uint32_t* adj_in, cudaStream_t s) {
     const uint32_t n = d->n, L = d->L;
     const int blocks = num_sms() * 8;
@@ -449,6 +449,7 @@ static cudaStream_t side_stream(SideStream kind) {
 }
 
 static cudaStream_t upload_copy_stream() { return side_stream(SIDE_COPY); }
+cudaStream_t library_copy_stream() { return side_stream(SIDE_COPY); }
 
 // Groups of layers (at most MAX_GROUPS, about equal in entries) whose input
 // adjacency is copied on the copy stream, one cudaMemcpyAsync and one event
@@ -525,13 +526,13 @@ fc_status upload(fc_graph* g, cudaStream_t s) {
     d->home = s;
     g->dev = d;
     uint64_t noff = (uint64_t)L * (n + 1);
-    uint64_t* d_off = nullptr;
+    uint32_t* d_off = nullptr;
     uint32_t* d_in = nullptr;
     uint32_t* rowlen = nullptr;
     uint32_t* d_max = nullptr;
     void* tmp = nullptr;
     size_t tmp_bytes = 0;
-    FC_CUDA_TRY(cudaMallocAsync(&d_off, noff * 8 + 8, s));
+    FC_CUDA_TRY(cudaMallocAsync(&d_off, noff * 4 + 4, s));
     FC_CUDA_TRY(cudaMallocAsync(&d_in, entries * 4 + 4, s));
     FC_CUDA_TRY(cudaMallocAsync(&rowlen, (uint64_t)n * 4 + 4, s));
     FC_CUDA_TRY(cudaMallocAsync(&d_max, 8, s));
@@ -546,7 +547,7 @@ fc_status upload(fc_graph* g, cudaStream_t s) {
     // group is scattered into the node-major rows once it has arrived.
     UploadPipe pipe;
     const uint32_t ngroups = entries && n ? pipe.plan(g, s) : 0u;
-    if (noff) FC_CUDA_TRY(cudaMemcpyAsync(d_off, g->off.p, noff * 8, cudaMemcpyHostToDevice, s));
+    if (noff) FC_CUDA_TRY(cudaMemcpyAsync(d_off, g->off.p, noff * 4, cudaMemcpyHostToDevice, s));
     if (ngroups) {
         FC_TRY(pipe.copy(g, d_in, s));
     } else if (entries) {

@@ -271,10 +271,11 @@ fc_status finish(uint32_t n, uint32_t L, std::vector<std::vector<uint32_t>>& dir
     });
     std::vector<uint64_t> base(L + 1, 0);
     for (uint32_t l = 0; l < L; l++) base[l + 1] = base[l] + adjs[l].size();
+    if (base[L] >= (1ull << 32)) return FC_ERR_TOO_LARGE;  // 32-bit offsets
     if (!g->off.alloc((uint64_t)L * (n + 1)) || !g->adj.alloc(base[L])) return FC_ERR_OOM;
     for_each_layer(L, [&](uint32_t l) {
-        uint64_t* o = g->off.p + (uint64_t)l * (n + 1);
-        for (uint32_t v = 0; v <= n; v++) o[v] = base[l] + offs[l][v];
+        uint32_t* o = g->off.p + (uint64_t)l * (n + 1);
+        for (uint32_t v = 0; v <= n; v++) o[v] = (uint32_t)(base[l] + offs[l][v]);
         if (!adjs[l].empty()) memcpy(g->adj.p + base[l], adjs[l].data(), adjs[l].size() * 4);
         std::vector<uint32_t>().swap(adjs[l]);
     });
@@ -396,14 +397,15 @@ fc_status build_from_adjbuf(uint32_t n, uint32_t L, const uint32_t* const* bufs,
     for (uint32_t i = 0; i < L; i++) g->order[i] = i;
     uint64_t total = 0;
     for (uint32_t l = 0; l < L; l++) total += m[l];
+    if (total >= (1ull << 32)) return FC_ERR_TOO_LARGE;  // 32-bit offsets
     if (!g->off.alloc((uint64_t)L * (n + 1)) || !g->adj.alloc(total)) return FC_ERR_OOM;
     uint64_t base = 0;
     for (uint32_t l = 0; l < L; l++) {
         const uint32_t* b = bufs[l];
-        uint64_t* o = g->off.p + (uint64_t)l * (n + 1);
+        uint32_t* o = g->off.p + (uint64_t)l * (n + 1);
         uint64_t r = 0, w = base;
         for (uint32_t v = 0; v < n; v++) {
-            o[v] = w;
+            o[v] = (uint32_t)w;
             uint32_t d = b[r++];
             if (w + d > base + m[l]) return FC_ERR_PARSE;
             for (uint32_t j = 0; j < d; j++) {
@@ -413,7 +415,7 @@ fc_status build_from_adjbuf(uint32_t n, uint32_t L, const uint32_t* const* bufs,
             }
         }
         if (w != base + m[l]) return FC_ERR_PARSE;
-        o[n] = w;
+        o[n] = (uint32_t)w;
         base = w;
     }
     return FC_OK;
@@ -444,16 +446,16 @@ void apply_order(int o, fc_graph* g) {
     } else {
         return;
     }
-    HostBuf<uint64_t> off2;
+    HostBuf<uint32_t> off2;
     HostBuf<uint32_t> adj2;
     uint64_t total = g->total_entries();
     if (!off2.alloc((uint64_t)L * (n + 1)) || !adj2.alloc(total)) return;
     uint64_t base = 0;
     for (uint32_t i = 0; i < L; i++) {
-        const uint64_t* src = g->off.p + (uint64_t)ord[i] * (n + 1);
-        uint64_t* dst = off2.p + (uint64_t)i * (n + 1);
+        const uint32_t* src = g->off.p + (uint64_t)ord[i] * (n + 1);
+        uint32_t* dst = off2.p + (uint64_t)i * (n + 1);
         uint64_t len = src[n] - src[0];
-        for (uint32_t v = 0; v <= n; v++) dst[v] = base + (src[v] - src[0]);
+        for (uint32_t v = 0; v <= n; v++) dst[v] = (uint32_t)(base + (src[v] - src[0]));
         if (len) memcpy(adj2.p + base, g->adj.p + src[0], len * 4);
         base += len;
     }

@@ -76,7 +76,8 @@ struct PeelCtl {
     uint32_t level, alive_cur, q_cur, stopped;  // stopped: left the rest to the endgame
     uint32_t prev_tail[2];       // per kind: items the previous level's queues held
     uint32_t alive_cnt[2];
-    uint32_t levels, items, pad1, pad2;
+    uint32_t levels, items;
+    uint32_t alive0[2];  // of alive_cnt, the pairs of the launch's first column
     uint64_t t_last;      // globaltimer at the last barrier
     uint64_t t_start;     // globaltimer at the first barrier
     uint64_t ph_ns[4];    // time per phase kind: scan, drain
@@ -234,6 +235,7 @@ __device__ void leader_step(PeelCtl* c, const PeelJob& j) {
     const uint32_t t00 = ld_l2(&c->tail[0][QS].v), t01 = ld_l2(&c->tail[0][QC].v);
     const uint32_t t10 = ld_l2(&c->tail[1][QS].v), t11 = ld_l2(&c->tail[1][QC].v);
     const uint32_t ac0 = ld_l2(&c->alive_cnt[0]), ac1 = ld_l2(&c->alive_cnt[1]);
+    const uint32_t first_col = ld_l2(&c->alive0[ac & 1u]);
     const uint32_t ts = q ? t10 : t00, tc = q ? t11 : t01;  // this level's reservations
     if (t_last) __stcg((unsigned long long*)&c->ph_ns[kind], ph + (now - t_last));
     if (j.trace && t_last && level < j.trace_levels && phase != PH_INIT) {
@@ -264,9 +266,11 @@ __device__ void leader_step(PeelCtl* c, const PeelJob& j) {
                 __stcg(&c->items, items + ts + tc);
                 if ((ac ? ac1 : ac0) == 0) {
                     next = PH_DONE;
-                } else if ((ac ? ac1 : ac0) <= j.stop_alive) {
+                } else if (j.stop_alive && first_col <= j.stop_alive) {
                     // every removal up to this level is done: the survivors
-                    // are the nodes whose core exceeds it
+                    // are the nodes whose core exceeds it.  The launch's
+                    // first column holds the most (core_(lmd+1) <= core_lmd),
+                    // so no column has more than stop_alive
                     __stcg(&c->stopped, 1u);
                     next = PH_DONE;
                 } else {
@@ -290,6 +294,7 @@ __device__ void leader_step(PeelCtl* c, const PeelJob& j) {
         __stcg(&c->level, level + 1);
         __stcg(&c->levels, levels + 1);
         __stcg(&c->alive_cnt[ac ^ 1], 0u);
+        __stcg(&c->alive0[ac ^ 1], 0u);
         next = PH_SCAN;
         if (level + 1 > j.max_level) err = ERR_LIMIT;
     }
@@ -584,49 +589,70 @@ __device__ __forceinline__ void visit_node(const PeelJob& j, const SegP& g, uint
 // the rest keep their count and move to `out`.  Survivors and queue items of
 // a block are reserved with one atomic each per block iteration (the
 // counters are shared by the whole grid).
-template <int G, bool MULTI>
-__device__ __forceinline__ void scan_nodes(const PeelJob& j, const uint32_t* src, uint32_t cnt_nodes,
-                                           uint32_t k, uint32_t q, uint32_t* out,
-                                           uint32_t* out_cnt) {
+// NPT nodes per group of G lanes and block iteration: with one-lane nodes and
+// enough of them for every block, four (their loads all in flight together,
+// and a quarter of the block barriers and reservations per node).  The kept
+// pairs of the launch's first column are counted beside the total.
+template <int G, bool MULTI, int NPT>
+__device__ __forceinline__ void scan_nodes_n(const PeelJob& j, const uint32_t* src,
+                                             uint32_t cnt_nodes, uint32_t k, uint32_t q,
+                                             uint32_t* out, uint32_t* out_cnt, uint32_t* out_cnt0) {
     __shared__ uint32_t s_keep[32], s_short[32], s_chunk[32], s_kbase, s_sbase, s_cbase;
+    __shared__ uint32_t s_keep0[32];  // kept pairs of the first column, per warp
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warp = threadIdx.x >> 5;
     const uint32_t nwarps = blockDim.x >> 5;
-    const uint32_t per_block = blockDim.x / G;
+    const uint32_t per_pass = blockDim.x / G;
+    const uint32_t per_block = per_pass * NPT;
     for (uint32_t base = blockIdx.x * per_block; base < cnt_nodes; base += gridDim.x * per_block) {
-        const uint32_t idx = base + threadIdx.x / G;
-        bool live = idx < cnt_nodes;
-        const uint32_t x = live ? (src ? ld_l2(src + idx) : idx) : 0;
-        if (live && src && !is_alive(j, x)) live = false;  // removed in the last drain
-        const SegP g = seg_load<MULTI>(j, seg_of<MULTI>(j, x));
-        const uint32_t xl = x - g.xbase;
-        const uint32_t c = g.divN.div(xl);
-        const uint32_t v = xl - c * g.n;
-        const uint32_t cnt = group_count_ge<G>(g.deg + (uint64_t)c * g.nL + (uint64_t)v * g.L, g.L,
-                                               k + 1, live);
-        const bool lead = live && (lane & (G - 1)) == 0;
-        const bool remove = lead && cnt < g.col0 + c + 1;
-        const bool keep = lead && !remove;
-        const uint32_t nch = remove ? chunks_of(g, v, j.small_row, k) : 0u;
-        const uint32_t ns = (remove && nch == 0) ? 1u : 0u;
-        if (remove) {
-            clear_alive(j, x);
-            g.t[xl] = k;
-        } else if (keep) {
-            j.cnt[x] = cnt;
-            if (!src) g.t[xl] = UNSET;
+        uint32_t xs[NPT], nchs[NPT], tk = 0, tsh = 0, tch = 0, tk0 = 0;
+        bool keeps[NPT], shorts[NPT];
+#pragma unroll
+        for (int i = 0; i < NPT; i++) {
+            const uint32_t idx = base + i * per_pass + threadIdx.x / G;
+            bool live = idx < cnt_nodes;
+            const uint32_t x = live ? (src ? ld_l2(src + idx) : idx) : 0;
+            if (live && src && !is_alive(j, x)) live = false;  // removed in the last drain
+            const SegP g = seg_load<MULTI>(j, seg_of<MULTI>(j, x));
+            const uint32_t xl = x - g.xbase;
+            const uint32_t c = g.divN.div(xl);
+            const uint32_t v = xl - c * g.n;
+            const uint32_t cnt = group_count_ge<G>(g.deg + (uint64_t)c * g.nL + (uint64_t)v * g.L,
+                                                   g.L, k + 1, live);
+            const bool lead = live && (lane & (G - 1)) == 0;
+            const bool remove = lead && cnt < g.col0 + c + 1;
+            const bool keep = lead && !remove;
+            const uint32_t nch = remove ? chunks_of(g, v, j.small_row, k) : 0u;
+            const bool ns = remove && nch == 0;
+            if (remove) {
+                clear_alive(j, x);
+                g.t[xl] = k;
+            } else if (keep) {
+                j.cnt[x] = cnt;
+                if (!src) g.t[xl] = UNSET;
+            }
+            xs[i] = x;
+            nchs[i] = nch;
+            keeps[i] = keep;
+            shorts[i] = ns;
+            tk += keep;
+            tk0 += keep && c == 0 && (!MULTI || g.xbase == 0);
+            tsh += ns;
+            tch += nch;
         }
-        const uint32_t kin = warp_incl_scan(keep ? 1u : 0u);
-        const uint32_t sin = warp_incl_scan(ns);
-        const uint32_t cin = warp_incl_scan(nch);
+        const uint32_t kin = warp_incl_scan(tk);
+        const uint32_t sin = warp_incl_scan(tsh);
+        const uint32_t cin = warp_incl_scan(tch);
+        const uint32_t k0w = __reduce_add_sync(0xffffffffu, tk0);
         if (lane == 31) {
             s_keep[warp] = kin;
             s_short[warp] = sin;
             s_chunk[warp] = cin;
+            s_keep0[warp] = k0w;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            uint32_t kt = 0, st = 0, ct = 0;
+            uint32_t kt = 0, st = 0, ct = 0, k0t = 0;
             for (uint32_t w = 0; w < nwarps; w++) {
                 uint32_t a = s_keep[w], b = s_short[w], d = s_chunk[w];
                 s_keep[w] = kt;
@@ -635,17 +661,39 @@ __device__ __forceinline__ void scan_nodes(const PeelJob& j, const uint32_t* src
                 kt += a;
                 st += b;
                 ct += d;
+                k0t += s_keep0[w];
             }
+            if (k0t) atomicAdd(out_cnt0, k0t);
             s_kbase = kt ? atomicAdd(out_cnt, kt) : 0u;
             s_sbase = st ? atomicAdd(&j.ctl->tail[q][QS].v, st) : 0u;
             s_cbase = ct ? atomicAdd(&j.ctl->tail[q][QC].v, ct) : 0u;
         }
         __syncthreads();
-        if (keep) out[s_kbase + s_keep[warp] + kin - 1] = x;
-        if (ns) write_short(j, q, s_sbase + s_short[warp] + sin - 1, x);
-        if (nch) write_chunks(j, q, s_cbase + s_chunk[warp] + cin - nch, x, 0, nch, k);
+        uint32_t kp = s_kbase + s_keep[warp] + kin - tk;
+        uint32_t sp = s_sbase + s_short[warp] + sin - tsh;
+        uint32_t cp = s_cbase + s_chunk[warp] + cin - tch;
+#pragma unroll
+        for (int i = 0; i < NPT; i++) {
+            if (keeps[i]) out[kp++] = xs[i];
+            if (shorts[i]) write_short(j, q, sp++, xs[i]);
+            if (nchs[i]) {
+                write_chunks(j, q, cp, xs[i], 0, nchs[i], k);
+                cp += nchs[i];
+            }
+        }
         __syncthreads();
     }
+}
+
+template <int G, bool MULTI>
+__device__ __forceinline__ void scan_nodes(const PeelJob& j, const uint32_t* src, uint32_t cnt_nodes,
+                                           uint32_t k, uint32_t q, uint32_t* out,
+                                           uint32_t* out_cnt, uint32_t* out_cnt0) {
+    // grid-uniform choice (every block sees the same count)
+    if (G == 1 && (uint64_t)cnt_nodes >= 4ull * gridDim.x * blockDim.x)
+        scan_nodes_n<G, MULTI, 4>(j, src, cnt_nodes, k, q, out, out_cnt, out_cnt0);
+    else
+        scan_nodes_n<G, MULTI, 1>(j, src, cnt_nodes, k, q, out, out_cnt, out_cnt0);
 }
 
 // Every column of every segment starts from the full degrees.
@@ -675,11 +723,12 @@ __device__ __forceinline__ void phase_scan(const PeelJob& j, bool first) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < pc; i += gridDim.x * blockDim.x)
         j.qc[q ^ 1][i] = EMPTY;
     if (first) {
-        scan_nodes<G, MULTI>(j, nullptr, j.nx, k, q, j.alive[1], &j.ctl->alive_cnt[1]);
+        scan_nodes<G, MULTI>(j, nullptr, j.nx, k, q, j.alive[1], &j.ctl->alive_cnt[1],
+                             &j.ctl->alive0[1]);
     } else {
         const uint32_t a = ld_l2(&c->alive_cur);
         scan_nodes<G, MULTI>(j, j.alive[a], ld_l2(&c->alive_cnt[a]), k, q, j.alive[a ^ 1],
-                             &j.ctl->alive_cnt[a ^ 1]);
+                             &j.ctl->alive_cnt[a ^ 1], &j.ctl->alive0[a ^ 1]);
     }
 }
 

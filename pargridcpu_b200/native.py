@@ -29,7 +29,7 @@ EXPORTS = [
     "fc_cells_range", "fc_batch_run", "fc_server_create",
     "fc_server_submit", "fc_server_wait", "fc_server_query", "fc_server_destroy", "fc_graph_stats",
     "fc_launch_count", "fc_coreindex_fixed_scratch", "fc_cell_index", "fc_cells_members",
-    "fc_mlcd_query", "fc_probe_atomics", "fc_alloc_count",
+    "fc_mlcd_query", "fc_probe_atomics", "fc_alloc_count", "fc_coreindex_densest",
 ]
 
 
@@ -129,6 +129,7 @@ def lib():
         "fc_graph_device_bytes": ([p], u64),
         "fc_coreindex": ([p, p, i32, p], i32),
         "fc_densest": ([p, p, u32, p, p], i32),
+        "fc_coreindex_densest": ([p, p, p, u32, p, p], i32),
         "fc_densest_members": ([p, p, p, p, p], i32),
         "fc_cell_members": ([p, u32, u32, p, u32, C.POINTER(u32), p], i32),
         "fc_cells": ([p, C.c_double, p, u32, C.POINTER(u32), p], i32),

@@ -227,3 +227,33 @@ def test_c5_large_graph():
     nodes, _ = g.densest_members(r)
     assert hashlib.sha256(np.ascontiguousarray(nodes, dtype="<u4").tobytes()).hexdigest() == \
         f["nodes_sha256"]
+
+
+@pytest.mark.parametrize("name", ["c1", "layers33", "mix0", "hubs"])
+@pytest.mark.parametrize("pinned", [True, False])
+def test_coreindex_densest_in_one_call(name, pinned):
+    """fc_coreindex_densest: the table and every beta's result equal the
+    separate calls' (and the reference's), whether the table's copy overlaps
+    the densest search (pinned buffer) or precedes it (pageable buffer)."""
+    import torch
+
+    exp = G.expected(name)
+    g = MultilayerGraph.from_pairs(G.inputs(name))
+    if pinned:
+        out = torch.zeros((g.L, g.n), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    else:
+        out = np.zeros((g.L, g.n), np.uint32)
+    table, res = g.coreindex_densest(out, G.BETAS)
+    assert table is out
+    assert np.array_equal(table, exp["table"])
+    g2 = MultilayerGraph.from_pairs(G.inputs(name))
+    sep = g2.densest(G.BETAS)
+    assert np.array_equal(g2.coreindex(), exp["table"])
+    for beta, r, s in zip(G.BETAS, res, sep):
+        assert r == s, beta
+        k, lmd, length = (int(x) for x in exp[f"b{beta}_result"])
+        assert (r["k"], r["lmd"], r["length"]) == (k, lmd, length), (beta, r)
+    # a second call on the resident table peels nothing and gives the same
+    out2 = np.zeros_like(out)
+    table2, res2 = g.coreindex_densest(out2, G.BETAS)
+    assert np.array_equal(table2, table) and res2 == res
