@@ -63,7 +63,9 @@ fc_status coreindex(fc_graph* g, uint32_t* out, bool out_on_device, cudaStream_t
 
 // The table into `table` (host memory) and the densest search for `betas`:
 // when the buffer is pinned, its copy runs on the library's copy stream while
-// the densest kernels run on s; otherwise the copy comes first.  Results as
+// the densest kernels run on s -- issued once the densest search has read its
+// per-column maxima back, so that its few small reads do not queue behind
+// the table on the copy engines; otherwise the copy comes first.  Results as
 // coreindex + densest.
 fc_status coreindex_densest(fc_graph* g, uint32_t* table, const double* betas, uint32_t nb,
                             fc_densest_result* res, cudaStream_t s) {
@@ -77,29 +79,41 @@ fc_status coreindex_densest(fc_graph* g, uint32_t* table, const double* betas, u
             if (copied) cudaEventDestroy(copied);
         }
     } ev;
-    bool overlap = false;
+    bool overlap = false, issued = false;
+    cudaStream_t cs = nullptr;
     if (table && bytes) {
         cudaPointerAttributes a{};
         const bool pinned = cudaPointerGetAttributes(&a, table) == cudaSuccess &&
                             a.type == cudaMemoryTypeHost;
         cudaGetLastError();  // pageable memory is not an error
-        cudaStream_t cs = pinned ? library_copy_stream() : nullptr;
+        cs = pinned ? library_copy_stream() : nullptr;
         if (cs && cs != s &&
             cudaEventCreateWithFlags(&ev.peeled, cudaEventDisableTiming) == cudaSuccess &&
             cudaEventCreateWithFlags(&ev.copied, cudaEventDisableTiming) == cudaSuccess) {
             count_alloc(2);
-            FC_CUDA_TRY(cudaEventRecord(ev.peeled, s));
-            FC_CUDA_TRY(cudaStreamWaitEvent(cs, ev.peeled, 0));
-            FC_CUDA_TRY(cudaMemcpyAsync(table, d->table, bytes, cudaMemcpyDeviceToHost, cs));
-            FC_CUDA_TRY(cudaEventRecord(ev.copied, cs));
             overlap = true;
         } else {
             cudaGetLastError();
             FC_TRY(to_host(table, d->table, bytes, s));
         }
     }
-    const fc_status rc = densest(g, betas, nb, res, s);
-    if (overlap) FC_CUDA_TRY(cudaEventSynchronize(ev.copied));  // even when densest failed
+    const std::function<fc_status()> issue = [&]() -> fc_status {
+        if (issued) return FC_OK;
+        issued = true;
+        FC_CUDA_TRY(cudaEventRecord(ev.peeled, s));
+        FC_CUDA_TRY(cudaStreamWaitEvent(cs, ev.peeled, 0));
+        FC_CUDA_TRY(cudaMemcpyAsync(table, d->table, bytes, cudaMemcpyDeviceToHost, cs));
+        FC_CUDA_TRY(cudaEventRecord(ev.copied, cs));
+        return FC_OK;
+    };
+    fc_status rc = densest(g, betas, nb, res, s, overlap ? &issue : nullptr);
+    if (overlap) {
+        // the histogram was already resident (the hook did not run), or the
+        // densest search failed before it
+        const fc_status rc2 = issue();
+        if (rc == FC_OK) rc = rc2;
+        if (rc2 == FC_OK) FC_CUDA_TRY(cudaEventSynchronize(ev.copied));
+    }
     return rc;
 }
 

@@ -363,7 +363,8 @@ static int sm_count() {
 // Histograms for the resident table (beta-independent), over the lambda
 // columns [lo, hi): the other columns count as empty (kmax 0, no cells), and
 // no kernel reads them, since they may not have been computed.
-static fc_status build_hist(DeviceGraph* d, cudaStream_t st, uint32_t lo, uint32_t hi) {
+static fc_status build_hist(DeviceGraph* d, cudaStream_t st, uint32_t lo, uint32_t hi,
+                            const std::function<fc_status()>* after_maxima = nullptr) {
     DensState* s = (DensState*)d->dens;
     if (s && s->hist_valid && s->lo == lo && s->hi == hi) return FC_OK;
     if (!s) {
@@ -382,6 +383,7 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st, uint32_t lo, uint32
     FC_CUDA_TRY(cudaGetLastError());
     s->kmax.assign(L, 0);
     FC_TRY(to_host(s->kmax.data(), s->d_kmax, L * 4, st));
+    if (after_maxima) FC_TRY((*after_maxima)());
     d->kmax = s->kmax;
     for (uint32_t l = 0; l < L; l++)
         if (s->kmax[l] > d->max_deg) return FC_ERR_DEVICE;  // not a valid core table
@@ -507,15 +509,22 @@ static fc_status score_cells(DeviceGraph* d, double beta, cudaStream_t st) {
 }
 
 fc_status densest(fc_graph* g, const double* betas, uint32_t nb, fc_densest_result* res,
-                  cudaStream_t st) {
+                  cudaStream_t st, const std::function<fc_status()>* after_maxima) {
     FC_TRY(coreindex(g, nullptr, false, st));
     DeviceGraph* d = g->dev;
-    cudaEvent_t e0, e1;
-    FC_CUDA_TRY(cudaEventCreate(&e0));
-    FC_CUDA_TRY(cudaEventCreate(&e1));
+    struct Events {  // destroyed on every return
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        ~Events() {
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+        }
+    } ev;
+    FC_CUDA_TRY(cudaEventCreate(&ev.e0));
+    FC_CUDA_TRY(cudaEventCreate(&ev.e1));
     count_alloc(2);
+    cudaEvent_t e0 = ev.e0, e1 = ev.e1;
     FC_CUDA_TRY(cudaEventRecord(e0, st));
-    FC_TRY(build_hist(d, st, 0, d->L));
+    FC_TRY(build_hist(d, st, 0, d->L, after_maxima));
     DensState* s = (DensState*)d->dens;
     if (!s->d_res) FC_TRY(dev_alloc((void**)&s->d_res, sizeof(fc_densest_result), st));
     for (uint32_t b = 0; b < nb; b++) {
@@ -529,8 +538,6 @@ fc_status densest(fc_graph* g, const double* betas, uint32_t nb, fc_densest_resu
     FC_CUDA_TRY(cudaStreamSynchronize(st));
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     d->stats.densest_ms = ms;
     return FC_OK;
 }

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -78,8 +79,10 @@ uint64_t device_bytes(const fc_graph* g);
 fc_status coreindex(fc_graph* g, uint32_t* out, bool out_on_device, cudaStream_t s);
 fc_status coreindex_densest(fc_graph* g, uint32_t* table, const double* betas, uint32_t nb,
                             fc_densest_result* res, cudaStream_t s);
+// after_maxima (optional) runs once the per-column maxima are on the host,
+// before the histogram kernels: the table is complete and the stream idle
 fc_status densest(fc_graph* g, const double* betas, uint32_t nb, fc_densest_result* res,
-                  cudaStream_t s);
+                  cudaStream_t s, const std::function<fc_status()>* after_maxima = nullptr);
 fc_status densest_members(fc_graph* g, const fc_densest_result* r, uint32_t* nodes,
                           uint32_t* layers, cudaStream_t s);
 fc_status cells(fc_graph* g, double beta, fc_cell* out, uint32_t cap, uint32_t* count,
