@@ -145,22 +145,32 @@ __device__ __forceinline__ void edge_bin_add(uint32_t* sh, uint32_t* H, bool sh_
     else atomicAdd(H + hbase + (uint64_t)l * km1 + key, cnt);
 }
 
-// V4: the group is four columns starting at a multiple of four with L a
-// multiple of four, so a node's four core values are one aligned 16-byte
-// load.
-template <bool V4>
+// How a node's core values for the group's columns are read: one column at a
+// time (EH_SCALAR); the group is four columns starting at a multiple of four
+// with L a multiple of four, so a node's four values are one aligned 16-byte
+// load, kept across its row (EH_V4); or the group starts at a multiple of four
+// with L a multiple of four, any number of columns: four at a time, up to
+// sixteen loads issued before their values are used (EH_QUAD).
+enum : int { EH_SCALAR = 0, EH_V4 = 1, EH_QUAD = 2 };
+
+template <int MODE>
 __global__ void k_edge_hist(const uint32_t* __restrict__ node_ptr, const uint32_t* __restrict__ adj,
                             uint32_t n, uint32_t L, uint64_t entries, FastDiv divL,
                             const uint32_t* __restrict__ coreT, uint32_t lam0, uint32_t nl,
                             const uint64_t* __restrict__ hbase, const uint32_t* __restrict__ kmax,
                             uint32_t* __restrict__ H, uint32_t sh_words, int sh_ok) {
+    constexpr bool V4 = MODE == EH_V4;
     extern __shared__ uint32_t sh[];
     __shared__ uint32_t soff[64];  // per column in the group: offset into sh
+    __shared__ uint32_t skm1[64];  // kmax + 1
+    __shared__ uint64_t shb[64];   // the column's base in H
     if (threadIdx.x == 0) {
         uint32_t o = 0;
         for (uint32_t i = 0; i < nl; i++) {
             soff[i] = o;
-            o += L * (kmax[lam0 + i] + 1);
+            skm1[i] = kmax[lam0 + i] + 1;
+            shb[i] = hbase[lam0 + i];
+            o += L * skm1[i];
         }
     }
     if (sh_ok)
@@ -199,30 +209,65 @@ __global__ void k_edge_hist(const uint32_t* __restrict__ node_ptr, const uint32_
                 l = slot - u * L;
                 w = u > v ? 2u : u == v ? 1u : 0u;
             }
-            uint4 B = make_uint4(0, 0, 0, 0);
-            if (V4 && w && (A.x | A.y | A.z | A.w))
-                B = *(const uint4*)(coreT + (uint64_t)u * L + lam0);
-            for (uint32_t i = 0; i < nl; i++) {
-                uint32_t a = 0, b = 0;
-                if (V4) {
-                    a = i == 0 ? A.x : i == 1 ? A.y : i == 2 ? A.z : A.w;
-                    b = i == 0 ? B.x : i == 1 ? B.y : i == 2 ? B.z : B.w;
-                } else if (w) {
-                    a = coreT[(uint64_t)v * L + lam0 + i];
-                    if (a) b = coreT[(uint64_t)u * L + lam0 + i];
+            if (MODE == EH_QUAD) {
+                if (w) {
+                    const uint32_t* av = coreT + (uint64_t)v * L + lam0;
+                    const uint32_t* bu = coreT + (uint64_t)u * L + lam0;
+                    const uint32_t nq = nl >> 2;
+                    for (uint32_t q0 = 0; q0 < nq; q0 += 4) {
+                        uint4 qa[4], qb[4];
+#pragma unroll
+                        for (int j = 0; j < 4; j++) {
+                            qa[j] = qb[j] = make_uint4(0, 0, 0, 0);
+                            if (q0 + j < nq) {
+                                qa[j] = *(const uint4*)(av + 4 * (q0 + j));
+                                qb[j] = *(const uint4*)(bu + 4 * (q0 + j));
+                            }
+                        }
+#pragma unroll
+                        for (int j = 0; j < 4; j++) {
+                            const uint32_t i = 4 * (q0 + j);
+                            const uint32_t ka[4] = {qa[j].x, qa[j].y, qa[j].z, qa[j].w};
+                            const uint32_t kb[4] = {qb[j].x, qb[j].y, qb[j].z, qb[j].w};
+#pragma unroll
+                            for (int c = 0; c < 4; c++) {
+                                const uint32_t key = min(ka[c], kb[c]);  // 0 past nq
+                                if (key)
+                                    edge_bin_add(sh, H, sh_ok, soff[i + c], shb[i + c], l,
+                                                 skm1[i + c], key, w);
+                            }
+                        }
+                    }
+                    for (uint32_t i = nq * 4; i < nl; i++) {
+                        const uint32_t a = av[i];
+                        const uint32_t key = a ? min(a, bu[i]) : 0u;
+                        if (key) edge_bin_add(sh, H, sh_ok, soff[i], shb[i], l, skm1[i], key, w);
+                    }
                 }
-                const uint32_t key = w ? min(a, b) : 0u;
-                if (key)
-                    edge_bin_add(sh, H, sh_ok, soff[i], hbase[lam0 + i], l, kmax[lam0 + i] + 1,
-                                 key, w);
+            } else {
+                uint4 B = make_uint4(0, 0, 0, 0);
+                if (V4 && w && (A.x | A.y | A.z | A.w))
+                    B = *(const uint4*)(coreT + (uint64_t)u * L + lam0);
+                for (uint32_t i = 0; i < nl; i++) {
+                    uint32_t a = 0, b = 0;
+                    if (V4) {
+                        a = i == 0 ? A.x : i == 1 ? A.y : i == 2 ? A.z : A.w;
+                        b = i == 0 ? B.x : i == 1 ? B.y : i == 2 ? B.z : B.w;
+                    } else if (w) {
+                        a = coreT[(uint64_t)v * L + lam0 + i];
+                        if (a) b = coreT[(uint64_t)u * L + lam0 + i];
+                    }
+                    const uint32_t key = w ? min(a, b) : 0u;
+                    if (key) edge_bin_add(sh, H, sh_ok, soff[i], shb[i], l, skm1[i], key, w);
+                }
             }
         }
     }
     __syncthreads();
     if (sh_ok) {
         for (uint32_t i = 0; i < nl; i++) {
-            const uint32_t words = L * (kmax[lam0 + i] + 1);
-            uint32_t* g = H + hbase[lam0 + i];
+            const uint32_t words = L * skm1[i];
+            uint32_t* g = H + shb[i];
             for (uint32_t w = threadIdx.x; w < words; w += blockDim.x)
                 if (sh[soff[i] + w]) atomicAdd(g + w, sh[soff[i] + w]);
         }
@@ -327,28 +372,53 @@ __global__ void k_cells(uint32_t L, uint32_t P /* pow2 >= L */, const uint64_t* 
 }
 
 // The reference's preorder fold with a float running maximum.
+// One block: the cells' densities are staged in shared memory, FOLD_CHUNK at a
+// time by all threads, and thread 0 folds them in order (the float running
+// maximum is order-dependent, so the fold itself stays sequential).
+constexpr uint32_t FOLD_CHUNK = 2048;
 __global__ void k_fold(const fc_cell* __restrict__ cells, uint64_t ncells, double beta,
                        fc_densest_result* out) {
-    if (threadIdx.x || blockIdx.x) return;
-    float maxd = 0.0f;
-    fc_densest_result r;
-    r.beta = beta;
-    r.density = 0.0;
-    r.k = r.lmd = r.length = r.lstar = 0;
-    for (uint64_t i = 0; i < ncells; i++) {
-        const fc_cell c = cells[i];
-        if (c.density >= (double)maxd) {
-            maxd = (float)c.density;
+    __shared__ double sd[FOLD_CHUNK];
+    __shared__ float s_maxd;
+    __shared__ uint64_t s_win;  // winning cell, or ~0 for none
+    if (threadIdx.x == 0) {
+        s_maxd = 0.0f;
+        s_win = ~0ull;
+    }
+    for (uint64_t c0 = 0; c0 < ncells; c0 += FOLD_CHUNK) {
+        const uint32_t m = ncells - c0 < FOLD_CHUNK ? (uint32_t)(ncells - c0) : FOLD_CHUNK;
+        __syncthreads();  // the last chunk is folded
+        for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) sd[i] = cells[c0 + i].density;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float maxd = s_maxd;
+            uint64_t win = s_win;
+            for (uint32_t i = 0; i < m; i++)
+                if (sd[i] >= (double)maxd) {
+                    maxd = (float)sd[i];
+                    win = c0 + i;
+                }
+            s_maxd = maxd;
+            s_win = win;
+        }
+    }
+    if (threadIdx.x == 0) {
+        fc_densest_result r;
+        r.beta = beta;
+        r.density = 0.0;
+        r.k = r.lmd = r.length = r.lstar = 0;
+        if (s_win != ~0ull) {
+            const fc_cell c = cells[s_win];
             r.density = c.density;
             r.k = c.k;
             r.lmd = c.lmd;
             r.length = c.length;
             r.lstar = c.lstar;
         }
+        r.max_density_f = s_maxd;
+        r.n_cells = (uint32_t)ncells;
+        *out = r;
     }
-    r.max_density_f = maxd;
-    r.n_cells = (uint32_t)ncells;
-    *out = r;
 }
 
 // ---- host --------------------------------------------------------------------
@@ -439,11 +509,14 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st, uint32_t lo, uint32
         const uint32_t SH_WORDS = 48 * 1024;  // 192 KB
         // once per process (thread-safe static initialisation)
         static const cudaError_t attr_rc = cudaFuncSetAttribute(
-            k_edge_hist<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, SH_WORDS * 4);
+            k_edge_hist<EH_SCALAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, SH_WORDS * 4);
         static const cudaError_t attr_rc4 = cudaFuncSetAttribute(
-            k_edge_hist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, SH_WORDS * 4);
+            k_edge_hist<EH_V4>, cudaFuncAttributeMaxDynamicSharedMemorySize, SH_WORDS * 4);
+        static const cudaError_t attr_rcq = cudaFuncSetAttribute(
+            k_edge_hist<EH_QUAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, SH_WORDS * 4);
         FC_CUDA_TRY(attr_rc);
         FC_CUDA_TRY(attr_rc4);
+        FC_CUDA_TRY(attr_rcq);
         FastDiv divL;
         divL.init(L);
         // about 16K entries per block, at most one block per SM: a block
@@ -461,15 +534,27 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st, uint32_t lo, uint32
                 words += w;
                 nl++;
             }
+            // with L a multiple of four, groups of a multiple of four columns
+            // keep the next group 16-byte aligned for quad loads
+            if (L % 4 == 0 && lam % 4 == 0 && nl > 4 && lam + nl < hi && nl % 4) {
+                nl &= ~3u;
+                words = 0;
+                for (uint32_t i = 0; i < nl; i++) words += L * (s->kmax[lam + i] + 1);
+            }
             int sh_ok = words <= SH_WORDS;
             size_t shb = sh_ok ? (size_t)words * 4 : 0;
             if (d->entries) {
-                if (nl == 4 && L % 4 == 0 && lam % 4 == 0)
-                    k_edge_hist<true><<<blocks, 1024, shb, st>>>(
+                const bool aligned = L % 4 == 0 && lam % 4 == 0;
+                if (aligned && nl == 4)
+                    k_edge_hist<EH_V4><<<blocks, 1024, shb, st>>>(
+                        d->node_ptr, d->adj, n, L, d->entries, divL, s->coreT, lam, nl, s->d_hbase,
+                        s->d_kmax, s->H, words, sh_ok);
+                else if (aligned && nl > 4)
+                    k_edge_hist<EH_QUAD><<<blocks, 1024, shb, st>>>(
                         d->node_ptr, d->adj, n, L, d->entries, divL, s->coreT, lam, nl, s->d_hbase,
                         s->d_kmax, s->H, words, sh_ok);
                 else
-                    k_edge_hist<false><<<blocks, 1024, shb, st>>>(
+                    k_edge_hist<EH_SCALAR><<<blocks, 1024, shb, st>>>(
                         d->node_ptr, d->adj, n, L, d->entries, divL, s->coreT, lam, nl, s->d_hbase,
                         s->d_kmax, s->H, words, sh_ok);
                 count_launch();
@@ -529,7 +614,7 @@ fc_status densest(fc_graph* g, const double* betas, uint32_t nb, fc_densest_resu
     if (!s->d_res) FC_TRY(dev_alloc((void**)&s->d_res, sizeof(fc_densest_result), st));
     for (uint32_t b = 0; b < nb; b++) {
         FC_TRY(score_cells(d, betas[b], st));
-        k_fold<<<1, 32, 0, st>>>(s->cells, s->ncells, betas[b], s->d_res);
+        k_fold<<<1, 256, 0, st>>>(s->cells, s->ncells, betas[b], s->d_res);
         count_launch();
         FC_CUDA_TRY(cudaGetLastError());
         FC_TRY(to_host(res + b, s->d_res, sizeof(fc_densest_result), st));
@@ -664,8 +749,9 @@ void densest_preload() {
     cudaFuncGetAttributes(&a, k_colmax);
     cudaFuncGetAttributes(&a, k_transpose);
     cudaFuncGetAttributes(&a, k_node_hist);
-    cudaFuncGetAttributes(&a, k_edge_hist<false>);
-    cudaFuncGetAttributes(&a, k_edge_hist<true>);
+    cudaFuncGetAttributes(&a, k_edge_hist<EH_SCALAR>);
+    cudaFuncGetAttributes(&a, k_edge_hist<EH_V4>);
+    cudaFuncGetAttributes(&a, k_edge_hist<EH_QUAD>);
     cudaFuncGetAttributes(&a, k_suffix);
     cudaFuncGetAttributes(&a, k_cells);
     cudaFuncGetAttributes(&a, k_fold);

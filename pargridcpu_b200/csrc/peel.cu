@@ -1565,17 +1565,21 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame(
     const uint64_t* __restrict__ base, const uint32_t* __restrict__ H,
     const uint32_t* __restrict__ l2g, const uint32_t* __restrict__ deg, uint32_t n, uint32_t L,
     FastDiv divL, uint32_t* __restrict__ t, uint32_t col0, uint32_t k0, uint32_t max_level,
-    uint32_t* __restrict__ levels, uint32_t* __restrict__ err, unsigned long long* __restrict__ tr) {
+    uint32_t* __restrict__ levels, uint32_t* __restrict__ err, unsigned long long* __restrict__ tr,
+    uint32_t whole) {
     extern __shared__ __align__(16) uint32_t sm[];
     __shared__ uint32_t s_warp[33];
     __shared__ uint32_t s_nalive, s_next, s_tail;
     const uint32_t c = blockIdx.x;
-    const uint32_t m = min(ecnt[c], cap);
+    // whole: every column peels the whole graph from its first level -- the
+    // graph's own rows, slots and initial degrees, local ids = node ids
+    // (n = cap nodes); otherwise the column's compacted survivor subgraph
+    const uint32_t m = whole ? cap : min(ecnt[c], cap);
     if (m == 0) return;
     const uint32_t lmd = col0 + c + 1;
-    const uint32_t* rp = rowptr + (uint64_t)c * (cap + 1);
-    const uint32_t* Hc = H + base[c];
-    const uint32_t* g_of = l2g + (uint64_t)c * cap;
+    const uint32_t* rp = whole ? rowptr : rowptr + (uint64_t)c * (cap + 1);
+    const uint32_t* Hc = whole ? H : H + base[c];
+    const uint32_t* g_of = whole ? nullptr : l2g + (uint64_t)c * cap;
     uint32_t* tc = t + (uint64_t)c * n;
     // shared layout: degrees | counts | batch prefixes | batch row starts |
     // alive | lists | queue
@@ -1592,7 +1596,8 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame(
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < m * L; i += blockDim.x) {
         const uint32_t lid = i / L, l = i - lid * L;
-        const uint32_t d = deg[(uint64_t)c * n * L + (uint64_t)g_of[lid] * L + l];
+        const uint32_t d = whole ? deg[(uint64_t)lid * L + l]
+                                 : deg[(uint64_t)c * n * L + (uint64_t)g_of[lid] * L + l];
         atomicOr(dw + (i >> 1), (d & 0xFFFFu) << ((i & 1) * 16));
     }
     for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
@@ -1628,7 +1633,7 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame(
             for (uint32_t l = 0; l < L; l++) cnt += eg_get16(dw, x * L + l) >= k + 1;
             if (cnt < lmd) {
                 alive[x] = 0;
-                tc[g_of[x]] = k;
+                tc[whole ? x : g_of[x]] = k;
                 queue[atomicAdd(&s_tail, 1u)] = (uint16_t)x;
             } else {
                 atomicOr(cw + (x >> 1), cnt << ((x & 1) * 16));  // the half was 0
@@ -1685,7 +1690,7 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame(
                         const uint32_t old = eg_dec16(dw, slot[r]);
                         if (old == k + 1 && eg_dec16(cw, u) == lmd) {
                             alive[u] = 0;
-                            tc[g_of[u]] = k;
+                            tc[whole ? u : g_of[u]] = k;
                             queue[atomicAdd(&s_tail, 1u)] = (uint16_t)u;
                         }
                     }
@@ -2262,7 +2267,7 @@ static fc_status endgame_run(const PeelJob& j, const PeelGraph& g, const PeelCtl
         } else {
             k_endgame<<<ncols, EG_THREADS, (size_t)smem, s>>>(
                 capE, c->eg_cnt, rowptr, c->eg_base, H, l2g, deg, g.n, g.L, divL, j.seg0.t, col0,
-                K + 1, j.max_level, c->eg_levels, &c->eg_err, etr);
+                K + 1, j.max_level, c->eg_levels, &c->eg_err, etr, 0u);
             count_launch(5);
             const cudaError_t le = cudaGetLastError();
             if (le != cudaSuccess) {
@@ -2308,6 +2313,70 @@ static fc_status endgame_run(const PeelJob& j, const PeelGraph& g, const PeelCtl
     return FC_OK;
 }
 
+// A graph whose nodes fit one block's shared memory: every column peels the
+// whole graph as the one-block endgame from level 0, on the graph's own rows
+// (no grid-wide levels, no compaction), one block per column.
+static uint32_t eg_whole_capacity(uint32_t L) {
+    const uint64_t fixed = 8ull * EG_THREADS + 256;
+    const uint64_t cap = (EG_SMEM - fixed) / eg_node_bytes(L);
+    return cap > 65535 ? 65535u : (uint32_t)cap;
+}
+
+static fc_status whole_run(const PeelJob& j, const PeelGraph& g, uint32_t col0, uint32_t ncols,
+                           cudaStream_t s, PeelStats* st, bool instrument) {
+    const uint32_t n = g.n, L = g.L;
+    const uint64_t smem = 4ull * (((uint64_t)n * L + 1) / 2 + (n + 1) / 2 + 2ull * EG_THREADS) +
+                          n + 4 + 6ull * n + 16;
+    static const cudaError_t attr_rc = cudaFuncSetAttribute(
+        k_endgame, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)EG_SMEM);
+    if (attr_rc != cudaSuccess || smem > EG_SMEM) return FC_ERR_DEVICE;
+    struct Events {  // destroyed on every return
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        ~Events() {
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+        }
+    } ev;
+    if (instrument) {
+        FC_CUDA_TRY(cudaEventCreate(&ev.e0));
+        FC_CUDA_TRY(cudaEventCreate(&ev.e1));
+        count_alloc(2);
+        FC_CUDA_TRY(cudaEventRecord(ev.e0, s));
+    }
+    // the levels of each column in the count array (nx >= ncols words)
+    FC_CUDA_TRY(cudaMemsetAsync(&j.ctl->eg_err, 0, 4, s));
+    FC_CUDA_TRY(cudaMemsetAsync(j.cnt, 0, 4ull * ncols, s));
+    FastDiv divL;
+    divL.init(L);
+    k_endgame<<<ncols, EG_THREADS, (size_t)smem, s>>>(
+        n, nullptr, g.node_ptr, nullptr, g.adj, nullptr, g.deg0, n, L, divL, j.seg0.t, col0, 0u,
+        j.max_level, j.cnt, &j.ctl->eg_err, nullptr, 1u);
+    count_launch();
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) {
+        set_last_cuda_error(le, "k_endgame", __FILE__, __LINE__);
+        return FC_ERR_DEVICE;
+    }
+    std::vector<uint32_t> lv(ncols);
+    uint32_t err = 0;
+    FC_TRY(to_host(lv.data(), j.cnt, 4ull * ncols, s));
+    FC_TRY(to_host(&err, &j.ctl->eg_err, 4, s));
+    if (instrument) {
+        float ms = 0;
+        cudaEventRecord(ev.e1, s);
+        cudaEventSynchronize(ev.e1);
+        cudaEventElapsedTime(&ms, ev.e0, ev.e1);
+        if (st) st->ms += ms;
+    }
+    if (err) return err == 2 ? FC_ERR_ITER_LIMIT : FC_ERR_DEVICE;
+    if (st) {
+        uint32_t m = 0;
+        for (uint32_t x : lv) m = x > m ? x : m;
+        st->levels += m;
+    }
+    return FC_OK;
+}
+
 fc_status peel_run(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* table, void* ws,
                    size_t ws_bytes, cudaStream_t s, PeelStats* st, bool instrument, bool endgame) {
     const uint64_t nx = (uint64_t)ncols * g.n;
@@ -2327,6 +2396,9 @@ fc_status peel_run(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* 
     j.seg_xbase = nullptr;
     j.nseg = 1;
     j.max_level = g.max_level;
+    if (endgame && g.n && g.n <= eg_whole_capacity(g.L) && env_u32("FC_PEEL_ENDGAME", 1) &&
+        env_u32("FC_PEEL_WHOLE", 1))
+        return whole_run(j, g, col0, ncols, s, st, instrument);
     const bool eg = endgame && ncols <= EG_MAX_COLS && env_u32("FC_PEEL_ENDGAME", 1);
     const uint32_t cs = eg ? eg_cluster_size() : 1u;
     const uint32_t cap = eg ? eg_column_capacity(g.L, cs) : 0u;
