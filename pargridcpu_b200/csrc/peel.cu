@@ -1820,7 +1820,7 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
     const uint32_t* __restrict__ l2g, const uint32_t* __restrict__ deg, uint32_t n, uint32_t L,
     FastDiv divL, uint32_t* __restrict__ t, uint32_t col0, uint32_t k0, uint32_t max_level,
     uint32_t* __restrict__ levels, uint32_t* __restrict__ err, unsigned long long* __restrict__ tr,
-    uint32_t split) {
+    uint32_t split, uint32_t whole) {
     extern __shared__ __align__(16) uint32_t sm[];
     __shared__ uint32_t s_warp[33];
     __shared__ uint32_t s_next, s_tail[2];
@@ -1831,14 +1831,16 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
     const uint32_t r = cl.block_rank();
     const uint32_t lg = 31 - __clz(CS);  // CS = 1 << lg
     const uint32_t c = blockIdx.x / CS;
-    const uint32_t m = min(ecnt[c], cap);
+    // whole: every column peels the whole graph from its first level (the
+    // graph's own rows, slots and initial degrees; local ids = node ids)
+    const uint32_t m = whole ? cap : min(ecnt[c], cap);
     if (m == 0) return;  // the whole cluster leaves, before any barrier
     const uint32_t lmd = col0 + c + 1;
     const uint32_t mo_max = (m + CS - 1) / CS;               // the same layout on every block
     const uint32_t mo = r < m ? (m - r + CS - 1) / CS : 0u;  // survivors r, r + CS, ...
-    const uint32_t* rp = rowptr + (uint64_t)c * (cap + 1);
-    const uint32_t* Hc = H + base[c];
-    const uint32_t* g_of = l2g + (uint64_t)c * cap;
+    const uint32_t* rp = whole ? rowptr : rowptr + (uint64_t)c * (cap + 1);
+    const uint32_t* Hc = whole ? H : H + base[c];
+    const uint32_t* g_of = whole ? nullptr : l2g + (uint64_t)c * cap;
     uint32_t* tc = t + (uint64_t)c * n;
     uint32_t* dw = sm;                                       // (mo_max * L + 1) / 2 words
     uint32_t* cw = dw + ((uint64_t)mo_max * L + 1) / 2;      // (mo_max + 1) / 2 words
@@ -1859,7 +1861,9 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < mo * L; i += blockDim.x) {
         const uint32_t idx = i / L, l = i - idx * L;
-        const uint32_t d = deg[(uint64_t)c * n * L + (uint64_t)g_of[(idx << lg) + r] * L + l];
+        const uint32_t u = (idx << lg) + r;
+        const uint32_t d = whole ? deg[(uint64_t)u * L + l]
+                                 : deg[(uint64_t)c * n * L + (uint64_t)g_of[u] * L + l];
         atomicOr(dw + (i >> 1), (d & 0xFFFFu) << ((i & 1) * 16));
     }
     // alive: 1, or 2 for a node whose row is longer than split (expanded by
@@ -1902,7 +1906,7 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
             for (uint32_t l = 0; l < L; l++) cnt += eg_get16(dw, x * L + l) >= k + 1;
             if (cnt < lmd) {
                 alive[x] = 0;
-                tc[g_of[(x << lg) + r]] = k;
+                tc[whole ? (x << lg) + r : g_of[(x << lg) + r]] = k;
                 if (!(ax == 2 && egc_push_big(r0_big, r0_bign, (rho + 1) % 3, (x << lg) + r)))
                     qh[qn][atomicAdd(&s_tail[qn], 1u)] = (uint16_t)x;
                 egc_count(r0_cnt + rho % 3);
@@ -1942,14 +1946,14 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
                     const uint32_t lid = ((uint32_t)qh[qc][it] << lg) + r;
                     start = rp[lid];
                     len = rp[lid + 1] - start;
-                    tc[g_of[lid]] = k;  // again for a scan removal: the same value
+                    tc[whole ? lid : g_of[lid]] = k;  // again for a scan removal: the same value
                 } else if (it < items) {
                     const uint32_t u = bl[it - qe];
                     const uint32_t s0 = rp[u], l0 = rp[u + 1] - s0;
                     const uint32_t e0 = (uint32_t)((uint64_t)l0 * r / CS);
                     start = s0 + e0;
                     len = (uint32_t)((uint64_t)l0 * (r + 1) / CS) - e0;
-                    if ((u & (CS - 1)) == r) tc[g_of[u]] = k;  // its owner
+                    if ((u & (CS - 1)) == r) tc[whole ? u : g_of[u]] = k;  // its owner
                 }
                 uint32_t ex;
                 const uint32_t total = egc_block_scan(len, &ex, s_warp);
@@ -2251,7 +2255,7 @@ static fc_status endgame_run(const PeelJob& j, const PeelGraph& g, const PeelCtl
                     &cfg, k_endgame_cl, capE, (const uint32_t*)c->eg_cnt, (const uint32_t*)rowptr,
                     (const uint64_t*)c->eg_base, (const uint32_t*)H, (const uint32_t*)l2g, deg, g.n,
                     g.L, divL, j.seg0.t, col0, K + 1, j.max_level, c->eg_levels, &c->eg_err,
-                    etr, eg_split());
+                    etr, eg_split(), 0u);
                 count_launch(5);
                 if (le != cudaSuccess) {
                     set_last_cuda_error(le, "k_endgame_cl", __FILE__, __LINE__);
@@ -2313,9 +2317,10 @@ static fc_status endgame_run(const PeelJob& j, const PeelGraph& g, const PeelCtl
     return FC_OK;
 }
 
-// A graph whose nodes fit one block's shared memory: every column peels the
-// whole graph as the one-block endgame from level 0, on the graph's own rows
-// (no grid-wide levels, no compaction), one block per column.
+// A graph whose nodes fit one block's shared memory (or one cluster's, up to
+// 65,536 nodes): every column peels the whole graph as the endgame from level
+// 0, on the graph's own rows (no grid-wide levels, no compaction), one block
+// (cluster) per column.
 static uint32_t eg_whole_capacity(uint32_t L) {
     const uint64_t fixed = 8ull * EG_THREADS + 256;
     const uint64_t cap = (EG_SMEM - fixed) / eg_node_bytes(L);
@@ -2323,13 +2328,16 @@ static uint32_t eg_whole_capacity(uint32_t L) {
 }
 
 static fc_status whole_run(const PeelJob& j, const PeelGraph& g, uint32_t col0, uint32_t ncols,
-                           cudaStream_t s, PeelStats* st, bool instrument) {
+                           uint32_t cs, cudaStream_t s, PeelStats* st, bool instrument) {
     const uint32_t n = g.n, L = g.L;
-    const uint64_t smem = 4ull * (((uint64_t)n * L + 1) / 2 + (n + 1) / 2 + 2ull * EG_THREADS) +
-                          n + 4 + 6ull * n + 16;
+    const uint32_t mo = (n + cs - 1) / cs;
+    const uint64_t smem =
+        cs > 1 ? egc_smem_bytes(mo, L)
+               : 4ull * (((uint64_t)n * L + 1) / 2 + (n + 1) / 2 + 2ull * EG_THREADS) + n + 4 +
+                     6ull * n + 16;
     static const cudaError_t attr_rc = cudaFuncSetAttribute(
         k_endgame, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)EG_SMEM);
-    if (attr_rc != cudaSuccess || smem > EG_SMEM) return FC_ERR_DEVICE;
+    if (attr_rc != cudaSuccess || smem > EG_SMEM || mo > 65535) return FC_ERR_DEVICE;
     struct Events {  // destroyed on every return
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         ~Events() {
@@ -2348,11 +2356,31 @@ static fc_status whole_run(const PeelJob& j, const PeelGraph& g, uint32_t col0, 
     FC_CUDA_TRY(cudaMemsetAsync(j.cnt, 0, 4ull * ncols, s));
     FastDiv divL;
     divL.init(L);
-    k_endgame<<<ncols, EG_THREADS, (size_t)smem, s>>>(
-        n, nullptr, g.node_ptr, nullptr, g.adj, nullptr, g.deg0, n, L, divL, j.seg0.t, col0, 0u,
-        j.max_level, j.cnt, &j.ctl->eg_err, nullptr, 1u);
+    cudaError_t le = cudaSuccess;
+    if (cs > 1) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = cs;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(ncols * cs);
+        cfg.blockDim = dim3(EG_THREADS);
+        cfg.dynamicSmemBytes = (size_t)smem;
+        cfg.stream = s;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        le = cudaLaunchKernelEx(&cfg, k_endgame_cl, n, (const uint32_t*)nullptr, g.node_ptr,
+                                (const uint64_t*)nullptr, g.adj, (const uint32_t*)nullptr,
+                                g.deg0, n, L, divL, j.seg0.t, col0, 0u, j.max_level, j.cnt,
+                                &j.ctl->eg_err, (unsigned long long*)nullptr, eg_split(), 1u);
+    } else {
+        k_endgame<<<ncols, EG_THREADS, (size_t)smem, s>>>(
+            n, nullptr, g.node_ptr, nullptr, g.adj, nullptr, g.deg0, n, L, divL, j.seg0.t, col0,
+            0u, j.max_level, j.cnt, &j.ctl->eg_err, nullptr, 1u);
+        le = cudaGetLastError();
+    }
     count_launch();
-    const cudaError_t le = cudaGetLastError();
     if (le != cudaSuccess) {
         set_last_cuda_error(le, "k_endgame", __FILE__, __LINE__);
         return FC_ERR_DEVICE;
@@ -2396,9 +2424,12 @@ fc_status peel_run(const PeelGraph& g, uint32_t col0, uint32_t ncols, uint32_t* 
     j.seg_xbase = nullptr;
     j.nseg = 1;
     j.max_level = g.max_level;
-    if (endgame && g.n && g.n <= eg_whole_capacity(g.L) && env_u32("FC_PEEL_ENDGAME", 1) &&
-        env_u32("FC_PEEL_WHOLE", 1))
-        return whole_run(j, g, col0, ncols, s, st, instrument);
+    if (endgame && g.n && env_u32("FC_PEEL_ENDGAME", 1) && env_u32("FC_PEEL_WHOLE", 1)) {
+        if (g.n <= eg_whole_capacity(g.L)) return whole_run(j, g, col0, ncols, 1, s, st, instrument);
+        const uint32_t wcs = eg_cluster_size();
+        if (wcs > 1 && g.n <= eg_column_capacity(g.L, wcs))
+            return whole_run(j, g, col0, ncols, wcs, s, st, instrument);
+    }
     const bool eg = endgame && ncols <= EG_MAX_COLS && env_u32("FC_PEEL_ENDGAME", 1);
     const uint32_t cs = eg ? eg_cluster_size() : 1u;
     const uint32_t cap = eg ? eg_column_capacity(g.L, cs) : 0u;

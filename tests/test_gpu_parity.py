@@ -100,13 +100,18 @@ def test_random_vs_oracle(name, make):
 
 @pytest.mark.parametrize("name", ["cl_L3_hubs", "cl_deep", "cl_L12"])
 def test_endgame_on_and_off_agree(name, monkeypatch):
-    """The peel's endgame (the last levels of each column in one block on the
-    survivors' subgraph) gives the table the grid-wide peel gives alone."""
+    """The three ways a single graph is peeled give the oracle's table: the
+    default (the whole graph per column on a block or a cluster when it fits
+    one), the grid-wide peel followed by the endgame on the survivors'
+    subgraph, and the grid-wide peel alone."""
     gen = dict(RANDOM)[name]()
     ref = O.OracleGraph(gen.layers).coreindex()
+    default = MultilayerGraph.from_pairs(gen.layers).coreindex()
+    monkeypatch.setenv("FC_PEEL_WHOLE", "0")
     with_eg = MultilayerGraph.from_pairs(gen.layers).coreindex()
     monkeypatch.setenv("FC_PEEL_ENDGAME", "0")
     without = MultilayerGraph.from_pairs(gen.layers).coreindex()
+    assert np.array_equal(default, ref)
     assert np.array_equal(with_eg, ref) and np.array_equal(without, ref)
 
 
@@ -167,15 +172,21 @@ def test_cell_members(name):
 
 
 def test_deadline_ends_the_run_with_an_error_and_the_device_stays_usable(monkeypatch):
-    """Every wait and loop of the peel kernel is bounded by the run's
-    deadline: a run past it ends with an error status (no fault, no trap),
-    and the next call on the same context gets the reference's table."""
+    """Every wait and loop of the grid-wide peel kernel is bounded by the
+    run's deadline: a run past it ends with an error status (no fault, no
+    trap), and the next call on the same context gets the reference's table.
+    (c1 would otherwise be peeled on thread-block clusters, whole graph per
+    column, without the grid-wide kernel.)"""
     g = MultilayerGraph.from_pairs(G.inputs("c1"))
+    monkeypatch.setenv("FC_PEEL_WHOLE", "0")
     monkeypatch.setenv("FC_PEEL_DEADLINE_MS", "0")
     with pytest.raises(native.FcError) as e:
         g.coreindex()
     assert e.value.code == 6  # FC_ERR_ITER_LIMIT
     monkeypatch.delenv("FC_PEEL_DEADLINE_MS")
+    assert np.array_equal(g.coreindex(), G.expected("c1")["table"])
+    monkeypatch.delenv("FC_PEEL_WHOLE")
+    g.reset_results()
     assert np.array_equal(g.coreindex(), G.expected("c1")["table"])
 
 
