@@ -138,10 +138,16 @@ __global__ void k_node_hist(const uint32_t* __restrict__ table, uint32_t n,
 // The adjacency is symmetric (every (v, u, l) has its (u, v, l), in the same
 // bin), so only the entry with u > v is visited and adds two; a self-loop
 // (u = v, one entry) adds one.  The histogram is the same.
-__device__ __forceinline__ void edge_bin_add(uint32_t* sh, uint32_t* H, bool sh_ok, uint32_t soff,
+// sh_mode: 0 the bins in global memory, 1 in shared memory as 32-bit words,
+// 2 in shared memory as 16-bit halves (a block's counts then stay below
+// 65,536: the host chooses it only when 2 x its entries per block do).
+__device__ __forceinline__ void edge_bin_add(uint32_t* sh, uint32_t* H, int sh_mode, uint32_t soff,
                                              uint64_t hbase, uint32_t l, uint32_t km1,
                                              uint32_t key, uint32_t cnt) {
-    if (sh_ok) atomicAdd(sh + soff + l * km1 + key, cnt);
+    if (sh_mode == 2) {
+        const uint32_t b = soff + l * km1 + key;
+        atomicAdd(sh + (b >> 1), cnt << ((b & 1) * 16));
+    } else if (sh_mode == 1) atomicAdd(sh + soff + l * km1 + key, cnt);
     else atomicAdd(H + hbase + (uint64_t)l * km1 + key, cnt);
 }
 
@@ -159,6 +165,8 @@ __global__ void k_edge_hist(const uint32_t* __restrict__ node_ptr, const uint32_
                             const uint32_t* __restrict__ coreT, uint32_t lam0, uint32_t nl,
                             const uint64_t* __restrict__ hbase, const uint32_t* __restrict__ kmax,
                             uint32_t* __restrict__ H, uint32_t sh_words, int sh_ok) {
+    // sh_ok: the shared-memory mode of edge_bin_add (0, 1 or 2); sh_words:
+    // the 32-bit words the block clears
     constexpr bool V4 = MODE == EH_V4;
     extern __shared__ uint32_t sh[];
     __shared__ uint32_t soff[64];  // per column in the group: offset into sh
@@ -264,12 +272,22 @@ __global__ void k_edge_hist(const uint32_t* __restrict__ node_ptr, const uint32_
         }
     }
     __syncthreads();
-    if (sh_ok) {
+    if (sh_ok == 1) {
         for (uint32_t i = 0; i < nl; i++) {
             const uint32_t words = L * skm1[i];
             uint32_t* g = H + shb[i];
             for (uint32_t w = threadIdx.x; w < words; w += blockDim.x)
                 if (sh[soff[i] + w]) atomicAdd(g + w, sh[soff[i] + w]);
+        }
+    } else if (sh_ok == 2) {
+        for (uint32_t i = 0; i < nl; i++) {
+            const uint32_t bins = L * skm1[i];
+            uint32_t* g = H + shb[i];
+            for (uint32_t w = threadIdx.x; w < bins; w += blockDim.x) {
+                const uint32_t b = soff[i] + w;
+                const uint32_t v = (sh[b >> 1] >> ((b & 1) * 16)) & 0xFFFFu;
+                if (v) atomicAdd(g + w, v);
+            }
         }
     }
 }
@@ -525,12 +543,17 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st, uint32_t lo, uint32
         // get the SMs this one leaves)
         const uint64_t want = (d->entries + 16383) / 16384;
         const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>(sm_count(), want));
+        // 16-bit bins when no block can count 65,536 in one bin (each entry
+        // adds at most 2; a block's warps take at most 32 entries more than
+        // an even share): twice the columns per pass over the entries
+        const bool half = 2 * ((d->entries + blocks - 1) / blocks + 32) < 65536;
+        const uint32_t budget = half ? 2 * SH_WORDS : SH_WORDS;  // bins
         uint32_t lam = lo;
         while (lam < hi) {
-            uint32_t words = 0, nl = 0;
+            uint32_t words = 0, nl = 0;  // words: bins of the group
             while (lam + nl < hi && nl < 64) {
                 uint32_t w = L * (s->kmax[lam + nl] + 1);
-                if (nl > 0 && words + w > SH_WORDS) break;
+                if (nl > 0 && words + w > budget) break;
                 words += w;
                 nl++;
             }
@@ -541,7 +564,8 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st, uint32_t lo, uint32
                 words = 0;
                 for (uint32_t i = 0; i < nl; i++) words += L * (s->kmax[lam + i] + 1);
             }
-            int sh_ok = words <= SH_WORDS;
+            const int sh_ok = words > budget ? 0 : half ? 2 : 1;
+            if (sh_ok == 2) words = (words + 1) / 2;  // the 32-bit words cleared
             size_t shb = sh_ok ? (size_t)words * 4 : 0;
             if (d->entries) {
                 const bool aligned = L % 4 == 0 && lam % 4 == 0;
