@@ -1553,10 +1553,15 @@ __device__ __forceinline__ uint32_t eg_dec16(uint32_t* w, uint32_t i) {
 // Optional endgame trace (FC_PEEL_TRACE): per column and level, the level's
 // start time (globaltimer ns), its rounds, the nodes it removed and the row
 // entries it expanded.
+// The cluster kernel adds, from its first block's first thread, the SM cycles
+// of each level's phases: the scan round up to its cluster barrier, the
+// rounds' row-offset loads and scans, their entry expansions, and their waits
+// at the cluster barrier.
 constexpr uint32_t EG_TRACE_LEVELS = 2048;
+constexpr uint32_t EG_TR_W = 8;  // words per record
 __device__ __forceinline__ unsigned long long* eg_tr(unsigned long long* tr, uint32_t c,
                                                      uint32_t lv) {
-    return (tr && lv < EG_TRACE_LEVELS) ? tr + 4ull * ((uint64_t)c * EG_TRACE_LEVELS + lv)
+    return (tr && lv < EG_TRACE_LEVELS) ? tr + EG_TR_W * ((uint64_t)c * EG_TRACE_LEVELS + lv)
                                         : nullptr;
 }
 
@@ -1746,6 +1751,11 @@ constexpr uint32_t EGC_BIG = 0x4000u;
 constexpr uint32_t EGC_CNT = 0x3FFFu;
 // Long rows queued in one round, per cluster (more go to their owners)
 constexpr uint32_t EGC_BIG_MAX = 256;
+// Capacity of each of a block's two local halves: rows found removed by the
+// block's own threads, expanded by the block before the round ends
+constexpr uint32_t EGC_LQ = 2048;
+// set in block 0's count of a round by a block whose local iterations ran out
+constexpr uint32_t EGC_FAIL = 0x80000000u;
 
 // Block 0's counters of round rho + 1 (pushes, kept nodes) and its long-row
 // list of round rho + 2 start empty; called at the start of round rho, when
@@ -1801,17 +1811,18 @@ __device__ __forceinline__ uint32_t egc_dec16(uint32_t* w, uint32_t i) {
 }
 
 // shared bytes per survivor a block owns: degrees (L halves), count (a half),
-// alive flag, two lists and two queue halves (16-bit indices)
+// alive flag, two lists and two queue halves (16-bit indices); besides them
+// the batch prefixes and row starts and the two local halves
 static uint32_t egc_node_bytes(uint32_t L) { return 2 * L + 11; }
 static uint32_t egc_block_capacity(uint32_t L) {
-    const uint64_t fixed = 8ull * EG_THREADS + 256;
+    const uint64_t fixed = 8ull * EG_THREADS + 4ull * EGC_LQ + 256;
     uint64_t cap = (EG_SMEM - fixed) / egc_node_bytes(L);
     if (cap > 65535) cap = 65535;
     return cap >= 1024 ? (uint32_t)cap : 0u;
 }
 static uint64_t egc_smem_bytes(uint32_t mo, uint32_t L) {
     return 4ull * (((uint64_t)mo * L + 1) / 2 + (mo + 1) / 2 + 2ull * EG_THREADS) + mo + 4 +
-           8ull * mo + 16;
+           8ull * mo + 4ull * EGC_LQ + 16;
 }
 
 __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
@@ -1820,10 +1831,14 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
     const uint32_t* __restrict__ l2g, const uint32_t* __restrict__ deg, uint32_t n, uint32_t L,
     FastDiv divL, uint32_t* __restrict__ t, uint32_t col0, uint32_t k0, uint32_t max_level,
     uint32_t* __restrict__ levels, uint32_t* __restrict__ err, unsigned long long* __restrict__ tr,
-    uint32_t split, uint32_t whole) {
+    uint32_t split, uint32_t whole, uint32_t lq_cap) {
     extern __shared__ __align__(16) uint32_t sm[];
     __shared__ uint32_t s_warp[33];
-    __shared__ uint32_t s_next, s_tail[2];
+    __shared__ uint32_t s_next, s_tail[2], s_lt[2];
+    // FC_PEEL_TRACE counters of a level, kept by thread 0: entries, cluster
+    // rounds, removals counted in block 0, local iterations, local removals,
+    // the four phases' cycles, and three timestamps
+    __shared__ unsigned long long s_tq[12];
     __shared__ uint32_t s_cnt[3], s_kept[3];  // block 0's are the cluster's
     __shared__ uint32_t s_big[3][EGC_BIG_MAX], s_bign[3];  // block 0's are the cluster's
     cg::cluster_group cl = cg::this_cluster();
@@ -1850,6 +1865,7 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
     uint16_t* list0 = (uint16_t*)(((uintptr_t)(alive + mo_max) + 3) & ~(uintptr_t)3);
     uint16_t* list1 = list0 + mo_max;
     uint16_t* qh[2] = {list1 + mo_max, list1 + 2 * mo_max};  // the two queue halves
+    uint16_t* lq[2] = {list1 + 3 * mo_max, list1 + 3 * mo_max + EGC_LQ};  // the local halves
     for (uint32_t i = threadIdx.x; i < ((uint64_t)mo_max * L + 1) / 2; i += blockDim.x) dw[i] = 0;
     for (uint32_t i = threadIdx.x; i < (mo_max + 1) / 2; i += blockDim.x) cw[i] = EGC_DEAD2;
     if (threadIdx.x < 3) {
@@ -1857,7 +1873,7 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
         s_kept[threadIdx.x] = 0;
         s_bign[threadIdx.x] = 0;
     }
-    if (threadIdx.x == 0) s_tail[0] = s_tail[1] = 0;
+    if (threadIdx.x == 0) s_tail[0] = s_tail[1] = s_lt[0] = s_lt[1] = 0;
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < mo * L; i += blockDim.x) {
         const uint32_t idx = i / L, l = i - idx * L;
@@ -1882,6 +1898,7 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
     uint16_t* nxt = list1;
     uint32_t na = mo, k = k0, rho = 0;
     bool failed = false;
+    const bool tq = tr && threadIdx.x == 0;
     for (;;) {
         if (k > max_level) {  // k is the same on every block
             failed = true;
@@ -1889,13 +1906,18 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
         }
         // SCAN round rho: removals queue locally in half (rho + 1) & 1
         const uint32_t qn = (rho + 1) & 1;
-        unsigned long long* const trl = threadIdx.x == 0 ? eg_tr(tr, c, k - k0) : nullptr;
-        unsigned long long tr_entries = 0, tr_rounds = 0, tr_items = 0;
+        if (tq) {
+            for (int q = 0; q < 11; q++) s_tq[q] = 0;
+            s_tq[11] = clock64();
+            if (r == 0) {
+                unsigned long long* const trl = eg_tr(tr, c, k - k0);
+                if (trl) trl[0] = global_ns();
+            }
+        }
         if (threadIdx.x == 0) {
             s_next = 0;
             s_tail[0] = s_tail[1] = 0;  // no block queues remotely during a scan round
             if (r == 0) egc_reset(s_cnt, s_kept, s_bign, rho);
-            if (trl && r == 0) trl[0] = global_ns();
         }
         __syncthreads();
         for (uint32_t i = threadIdx.x; i < na; i += blockDim.x) {
@@ -1922,119 +1944,178 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame_cl(
         const uint32_t kept = r0_kept[rho % 3];
         const uint32_t scanned = r0_cnt[rho % 3];
         uint32_t nbig = min(r0_bign[(rho + 1) % 3], EGC_BIG_MAX);  // the next round's long rows
+        if (tq) s_tq[5] = clock64() - s_tq[11];
         // with no survivor left in the column the rows of this scan's
         // removals name no node that could still change
         uint32_t pushes = kept ? scanned : 0u;
-        tr_items = scanned;
+        if (tq) s_tq[2] = scanned;
         rho++;
-        // DRAIN rounds while the last round queued anything (bounded: every
-        // node is queued at most once per level)
+        // DRAIN rounds while the last round queued anything for the cluster
+        // (bounded: every node is queued at most once per level)
         for (uint32_t round = 0; pushes && round <= m; round++) {
             const uint32_t qc = rho & 1, qp = (rho + 1) & 1;
-            // this block's queued rows, then its slice of every long row (the
-            // queue half and the list are final since the cluster barrier)
-            const uint32_t qe = s_tail[qc], items = qe + nbig;
             const uint32_t* const bl = r0_big + (rho % 3) * EGC_BIG_MAX;
             if (threadIdx.x == 0 && r == 0) egc_reset(s_cnt, s_kept, s_bign, rho);
-            tr_rounds++;
-            for (uint32_t b0 = 0; b0 < items; b0 += EG_THREADS) {
-                if (b0) __syncthreads();  // the last batch's pre and rs are read
-                const uint32_t nb = min(EG_THREADS, items - b0);
-                uint32_t len = 0, start = 0;
-                const uint32_t it = b0 + threadIdx.x;
-                if (it < qe) {
-                    const uint32_t lid = ((uint32_t)qh[qc][it] << lg) + r;
-                    start = rp[lid];
-                    len = rp[lid + 1] - start;
-                    tc[whole ? lid : g_of[lid]] = k;  // again for a scan removal: the same value
-                } else if (it < items) {
-                    const uint32_t u = bl[it - qe];
-                    const uint32_t s0 = rp[u], l0 = rp[u + 1] - s0;
-                    const uint32_t e0 = (uint32_t)((uint64_t)l0 * r / CS);
-                    start = s0 + e0;
-                    len = (uint32_t)((uint64_t)l0 * (r + 1) / CS) - e0;
-                    if ((u & (CS - 1)) == r) tc[whole ? u : g_of[u]] = k;  // its owner
-                }
-                uint32_t ex;
-                const uint32_t total = egc_block_scan(len, &ex, s_warp);
-                // every thread has read the queue's length (before the
-                // scan's barrier): the half takes round rho + 1's queue
-                if (b0 == 0 && threadIdx.x == 0) s_tail[qc] = 0;
-                tr_entries += total;
-                pre[threadIdx.x] = ex;
-                rs[threadIdx.x] = start;
-                __syncthreads();
-                uint32_t lo0 = 0;
-                for (uint32_t e0 = threadIdx.x; e0 < total; e0 += 4 * blockDim.x) {
-                    uint32_t slot[4];
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        const uint32_t e = e0 + q * blockDim.x;
-                        slot[q] = UNSET;
-                        if (e < total) {
-                            uint32_t lo = lo0, hi = nb - 1;
-                            while (lo < hi) {
-                                const uint32_t mid = (lo + hi + 1) >> 1;
-                                if (pre[mid] <= e) lo = mid;
-                                else hi = mid - 1;
-                            }
-                            lo0 = lo;
-                            slot[q] = Hc[rs[lo] + (e - pre[lo])];
-                        }
-                    }
-                    // the degree decrements first, independent of one another;
-                    // removed neighbours are decremented too (a half counts
-                    // the alive neighbours, so it never drops below 0), and
-                    // their count halves, EGC_DEAD less at most L crossings,
-                    // never equal lmd
-                    uint32_t ow[4], ui[4], old[4];
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        old[q] = 0;  // never k + 1
-                        ow[q] = ui[q] = 0;
-                        if (slot[q] == UNSET) continue;
-                        const uint32_t u = divL.div(slot[q]);
-                        if (u >= m) continue;
-                        const uint32_t l = slot[q] - u * L;
-                        ow[q] = u & (CS - 1);
-                        ui[q] = u >> lg;
-                        old[q] = egc_dec16(cl.map_shared_rank(dw, ow[q]), ui[q] * L + l);
-                    }
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        if (old[q] != k + 1) continue;
-                        const uint32_t oc = egc_dec16(cl.map_shared_rank(cw, ow[q]), ui[q]);
-                        if ((oc & EGC_CNT) != lmd) continue;
-                        // removed: expanded next round, by its owner or, for
-                        // a long row, by every block (the table entry is
-                        // written then)
-                        cl.map_shared_rank(alive, ow[q])[ui[q]] = 0;
-                        if (!((oc & EGC_BIG) &&
-                              egc_push_big(r0_big, r0_bign, (rho + 1) % 3, (ui[q] << lg) | ow[q]))) {
-                            uint32_t* const t_ow = cl.map_shared_rank(s_tail, ow[q]);
-                            const uint32_t pos = atomicAdd(t_ow + qp, 1u);
-                            cl.map_shared_rank(qh[qp], ow[q])[pos] = (uint16_t)ui[q];
-                        }
-                        egc_count(r0_cnt + rho % 3);
-                    }
-                }
+            if (tq) {
+                s_tq[1]++;
+                s_tq[9] = clock64();
             }
+            // Local iterations: the first expands this block's queued rows and
+            // its slice of every long row, each later one the rows that the
+            // block's own threads found removed in the one before (of any
+            // owner), until they find none.  A row found removed goes to the
+            // cluster's list when it is long, else to the local half while it
+            // has room, else to its owner's queue; the list and the queues are
+            // expanded in the next round (block 0 holds their counts).
+            uint32_t lcnt = 0;
+            bool ldone = false;
+            for (uint32_t li = 0; li <= m; li++) {
+                const uint32_t hw = (li + 1) & 1;  // the local half this iteration fills
+                const uint32_t qe = li ? lcnt : s_tail[qc];
+                const uint32_t items = li ? lcnt : qe + nbig;
+                const uint16_t* const lr = lq[li & 1];  // read by iterations >= 1
+                if (tq) s_tq[3]++;
+                for (uint32_t b0 = 0; b0 < items; b0 += EG_THREADS) {
+                    if (b0) __syncthreads();  // the last batch's pre and rs are read
+                    const uint32_t nb = min(EG_THREADS, items - b0);
+                    uint32_t len = 0, start = 0;
+                    const uint32_t it = b0 + threadIdx.x;
+                    if (it < qe) {
+                        const uint32_t lid =
+                            li ? (uint32_t)lr[it] : ((uint32_t)qh[qc][it] << lg) + r;
+                        start = rp[lid];
+                        len = rp[lid + 1] - start;
+                        tc[whole ? lid : g_of[lid]] = k;  // again for a scan removal: the same value
+                    } else if (it < items) {
+                        const uint32_t u = bl[it - qe];
+                        const uint32_t s0 = rp[u], l0 = rp[u + 1] - s0;
+                        const uint32_t e0 = (uint32_t)((uint64_t)l0 * r / CS);
+                        start = s0 + e0;
+                        len = (uint32_t)((uint64_t)l0 * (r + 1) / CS) - e0;
+                        if ((u & (CS - 1)) == r) tc[whole ? u : g_of[u]] = k;  // its owner
+                    }
+                    uint32_t ex;
+                    const uint32_t total = egc_block_scan(len, &ex, s_warp);
+                    // every thread has read the half's length (before the
+                    // scan's barrier): it takes a later iteration's (round's)
+                    if (b0 == 0 && threadIdx.x == 0) {
+                        if (li) s_lt[li & 1] = 0;
+                        else s_tail[qc] = 0;
+                    }
+                    if (tq) s_tq[0] += total;
+                    pre[threadIdx.x] = ex;
+                    rs[threadIdx.x] = start;
+                    __syncthreads();
+                    if (tq) {
+                        s_tq[10] = clock64();
+                        s_tq[6] += s_tq[10] - s_tq[9];
+                    }
+                    uint32_t lo0 = 0;
+                    for (uint32_t e0 = threadIdx.x; e0 < total; e0 += 4 * blockDim.x) {
+                        uint32_t slot[4];
+#pragma unroll
+                        for (int q = 0; q < 4; q++) {
+                            const uint32_t e = e0 + q * blockDim.x;
+                            slot[q] = UNSET;
+                            if (e < total) {
+                                uint32_t lo = lo0, hi = nb - 1;
+                                while (lo < hi) {
+                                    const uint32_t mid = (lo + hi + 1) >> 1;
+                                    if (pre[mid] <= e) lo = mid;
+                                    else hi = mid - 1;
+                                }
+                                lo0 = lo;
+                                slot[q] = Hc[rs[lo] + (e - pre[lo])];
+                            }
+                        }
+                        // the degree decrements first, independent of one
+                        // another; removed neighbours are decremented too (a
+                        // half counts the alive neighbours, so it never drops
+                        // below 0), and their count halves, EGC_DEAD less at
+                        // most L crossings, never equal lmd
+                        uint32_t ow[4], ui[4], old[4];
+#pragma unroll
+                        for (int q = 0; q < 4; q++) {
+                            old[q] = 0;  // never k + 1
+                            ow[q] = ui[q] = 0;
+                            if (slot[q] == UNSET) continue;
+                            const uint32_t u = divL.div(slot[q]);
+                            if (u >= m) continue;
+                            const uint32_t l = slot[q] - u * L;
+                            ow[q] = u & (CS - 1);
+                            ui[q] = u >> lg;
+                            old[q] = egc_dec16(cl.map_shared_rank(dw, ow[q]), ui[q] * L + l);
+                        }
+#pragma unroll
+                        for (int q = 0; q < 4; q++) {
+                            if (old[q] != k + 1) continue;
+                            const uint32_t oc = egc_dec16(cl.map_shared_rank(cw, ow[q]), ui[q]);
+                            if ((oc & EGC_CNT) != lmd) continue;
+                            // removed: its row is expanded by this block, by
+                            // its owner or, when long, by every block (the
+                            // table entry is written then)
+                            cl.map_shared_rank(alive, ow[q])[ui[q]] = 0;
+                            const uint32_t u2 = (ui[q] << lg) | ow[q];
+                            // (the list's own count tells the cluster)
+                            if ((oc & EGC_BIG) && egc_push_big(r0_big, r0_bign, (rho + 1) % 3, u2))
+                                continue;
+                            const uint32_t pos = lq_cap ? atomicAdd(&s_lt[hw], 1u) : 0u;
+                            if (pos < lq_cap) {
+                                lq[hw][pos] = (uint16_t)u2;
+                            } else {
+                                uint32_t* const t_ow = cl.map_shared_rank(s_tail, ow[q]);
+                                const uint32_t p2 = atomicAdd(t_ow + qp, 1u);
+                                cl.map_shared_rank(qh[qp], ow[q])[p2] = (uint16_t)ui[q];
+                                egc_count(r0_cnt + rho % 3);
+                            }
+                        }
+                    }
+                    if (tq) {
+                        s_tq[9] = clock64();
+                        s_tq[7] += s_tq[9] - s_tq[10];
+                    }
+                }
+                if (!lq_cap) {  // no local halves: the round ends here
+                    ldone = true;
+                    break;
+                }
+                __syncthreads();  // this iteration's local pushes are in place
+                lcnt = min(s_lt[hw], lq_cap);
+                if (lcnt == 0) {
+                    ldone = true;
+                    break;
+                }
+                if (tq) s_tq[4] += lcnt;
+            }
+            // (cannot happen: every node is found removed at most once a level)
+            if (!ldone && threadIdx.x == 0) atomicOr(r0_cnt + rho % 3, EGC_FAIL);
             cl.sync();  // every push is counted in block 0 and queued
-            pushes = r0_cnt[rho % 3];
+            const uint32_t cnt = r0_cnt[rho % 3];
             nbig = min(r0_bign[(rho + 1) % 3], EGC_BIG_MAX);
-            tr_items += pushes;
+            pushes = (cnt & ~EGC_FAIL) + nbig;
+            if (cnt & EGC_FAIL) {  // the same on every block
+                pushes = 1;
+                break;
+            }
+            if (tq) {
+                s_tq[8] += clock64() - s_tq[9];
+                s_tq[2] += pushes;
+            }
             rho++;
         }
         if (pushes) {  // the round bound ended the level with rows unexpanded
             failed = true;  // (the cluster-wide count: every block breaks)
             break;
         }
+        unsigned long long* const trl = tq ? eg_tr(tr, c, k - k0) : nullptr;
         if (trl) {
             if (r == 0) {
-                trl[1] = tr_rounds;
-                trl[2] = tr_items;
+                trl[1] = s_tq[1] | s_tq[3] << 32;  // cluster rounds, block 0's iterations
+                for (int q = 0; q < 4; q++) trl[4 + q] = s_tq[5 + q];
             }
-            atomicAdd(trl + 3, tr_entries);  // every block's rows
+            // every block's removals and rows
+            atomicAdd(trl + 2, r == 0 ? s_tq[2] + s_tq[4] : s_tq[4]);
+            atomicAdd(trl + 3, s_tq[0]);
         }
         // counts are rebuilt by the next scan: every half back to EGC_DEAD
         for (uint32_t i = threadIdx.x; i < (mo_max + 1) / 2; i += blockDim.x) cw[i] = EGC_DEAD2;
@@ -2131,7 +2212,13 @@ static uint32_t eg_cluster_size() {
 // Rows longer than this are expanded by every block of the cluster, a slice
 // each, instead of by their owner alone: FC_PEEL_EG_SPLIT (entries; 0 = never)
 static uint32_t eg_split() {
-    static const uint32_t v = env_u32("FC_PEEL_EG_SPLIT", 512);
+    static const uint32_t v = env_u32("FC_PEEL_EG_SPLIT", 2048);
+    return v;
+}
+// FC_PEEL_EG_LOCAL=0: every row found removed waits for the next cluster
+// round (no local iterations)
+static uint32_t eg_local_cap() {
+    static const uint32_t v = env_u32("FC_PEEL_EG_LOCAL", 1) ? EGC_LQ : 0u;
     return v;
 }
 
@@ -2184,7 +2271,7 @@ static fc_status endgame_run(const PeelJob& j, const PeelGraph& g, const PeelCtl
         ~TraceBuf() { dev_free(p, s); }
     } etr_own{nullptr, s};
     if (instrument && env_u32("FC_PEEL_TRACE", 0)) {
-        const uint64_t bytes = 32ull * ncols * EG_TRACE_LEVELS;
+        const uint64_t bytes = 8ull * EG_TR_W * ncols * EG_TRACE_LEVELS;
         FC_TRY(dev_alloc((void**)&etr_own.p, bytes, s));
         FC_CUDA_TRY(cudaMemsetAsync(etr_own.p, 0, bytes, s));
         etr = etr_own.p;
@@ -2255,7 +2342,7 @@ static fc_status endgame_run(const PeelJob& j, const PeelGraph& g, const PeelCtl
                     &cfg, k_endgame_cl, capE, (const uint32_t*)c->eg_cnt, (const uint32_t*)rowptr,
                     (const uint64_t*)c->eg_base, (const uint32_t*)H, (const uint32_t*)l2g, deg, g.n,
                     g.L, divL, j.seg0.t, col0, K + 1, j.max_level, c->eg_levels, &c->eg_err,
-                    etr, eg_split(), 0u);
+                    etr, eg_split(), 0u, eg_local_cap());
                 count_launch(5);
                 if (le != cudaSuccess) {
                     set_last_cuda_error(le, "k_endgame_cl", __FILE__, __LINE__);
@@ -2294,18 +2381,25 @@ static fc_status endgame_run(const PeelJob& j, const PeelGraph& g, const PeelCtl
     FC_TRY(rc);
     if (etr) {
         // one line per column and level: us, rounds, removals, row entries
-        std::vector<unsigned long long> tr(4ull * ncols * EG_TRACE_LEVELS);
+        std::vector<unsigned long long> tr((uint64_t)EG_TR_W * ncols * EG_TRACE_LEVELS);
         FC_TRY(to_host(tr.data(), etr, tr.size() * 8, s));
         fprintf(stderr, "eg-trace start level %u, %u blocks per column, survivors", K + 1, cs);
         for (uint32_t i = 0; i < ncols; i++) fprintf(stderr, " %u", cnts[i]);
-        fprintf(stderr, ", entries %llu\n", (unsigned long long)total);
+        uint32_t nbig = 0;
+        FC_TRY(to_host(&nbig, &c->eg_nbig, 4, s));
+        fprintf(stderr, ", entries %llu, rows filled by a block %u\n", (unsigned long long)total,
+                nbig);
         for (uint32_t i = 0; i < ncols; i++)
             for (uint32_t lv = 0; lv + 1 < EG_TRACE_LEVELS; lv++) {
-                const unsigned long long* r = tr.data() + 4ull * (i * EG_TRACE_LEVELS + lv);
+                const unsigned long long* r =
+                    tr.data() + (uint64_t)EG_TR_W * (i * EG_TRACE_LEVELS + lv);
                 if (!r[0]) break;
-                const unsigned long long nx = r[4] ? r[4] : r[0];
-                fprintf(stderr, "eg-trace col %u level %u us %.1f rounds %llu items %llu entries %llu\n",
-                        col0 + i, K + 1 + lv, (nx - r[0]) * 1e-3, r[1], r[2], r[3]);
+                const unsigned long long nx = r[EG_TR_W] ? r[EG_TR_W] : r[0];
+                fprintf(stderr,
+                        "eg-trace col %u level %u us %.1f rounds %llu local %llu items %llu"
+                        " entries %llu cycles scan %llu rows %llu expand %llu sync %llu\n",
+                        col0 + i, K + 1 + lv, (nx - r[0]) * 1e-3, r[1] & 0xFFFFFFFFull,
+                        r[1] >> 32, r[2], r[3], r[4], r[5], r[6], r[7]);
             }
     }
     if (tail[EG_MAX_COLS]) return tail[EG_MAX_COLS] == 2 ? FC_ERR_ITER_LIMIT : FC_ERR_DEVICE;
@@ -2373,7 +2467,8 @@ static fc_status whole_run(const PeelJob& j, const PeelGraph& g, uint32_t col0, 
         le = cudaLaunchKernelEx(&cfg, k_endgame_cl, n, (const uint32_t*)nullptr, g.node_ptr,
                                 (const uint64_t*)nullptr, g.adj, (const uint32_t*)nullptr,
                                 g.deg0, n, L, divL, j.seg0.t, col0, 0u, j.max_level, j.cnt,
-                                &j.ctl->eg_err, (unsigned long long*)nullptr, eg_split(), 1u);
+                                &j.ctl->eg_err, (unsigned long long*)nullptr, eg_split(), 1u,
+                                eg_local_cap());
     } else {
         k_endgame<<<ncols, EG_THREADS, (size_t)smem, s>>>(
             n, nullptr, g.node_ptr, nullptr, g.adj, nullptr, g.deg0, n, L, divL, j.seg0.t, col0,
