@@ -91,6 +91,21 @@ __global__ void k_colmax(const uint32_t* __restrict__ table, uint32_t n, uint32_
     if ((threadIdx.x & 31) == 0 && m) atomicMax(kmax + lam, m);
 }
 
+// L < 32: one node per thread; each of its L loads is coalesced across the
+// warp, and its values are stored as one row (a 16-byte store for L = 4)
+__global__ void k_transpose_rows(const uint32_t* __restrict__ table, uint32_t n, uint32_t L,
+                                 uint32_t* __restrict__ coreT) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        if (L == 4) {
+            const uint4 q = make_uint4(table[v], table[(uint64_t)n + v], table[2ull * n + v],
+                                       table[3ull * n + v]);
+            *(uint4*)(coreT + 4ull * v) = q;
+        } else {
+            for (uint32_t l = 0; l < L; l++) coreT[(uint64_t)v * L + l] = table[(uint64_t)l * n + v];
+        }
+    }
+}
+
 __global__ void k_transpose(const uint32_t* __restrict__ table, uint32_t n, uint32_t L,
                             uint32_t* __restrict__ coreT) {
     // 32x32 tiles through shared memory
@@ -464,8 +479,11 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st, uint32_t lo, uint32
     // per-lambda maxima
     if (!s->d_kmax) FC_TRY(dev_alloc((void**)&s->d_kmax, (L + 1) * 4, st));
     FC_CUDA_TRY(cudaMemsetAsync(s->d_kmax, 0, (L + 1) * 4, st));
-    dim3 g((n + 255) / 256 < 64 ? (n + 255) / 256 : 64, hi - lo);
-    if (g.x == 0) g.x = 1;
+    // blocks per column: enough to fill the SMs, at least 2048 nodes each
+    const uint32_t per_col = std::max<uint32_t>(
+        1u, std::min<uint32_t>((n + 2047) / 2048,
+                               8u * (uint32_t)sm_count() / std::max<uint32_t>(1u, hi - lo)));
+    dim3 g(per_col, hi - lo);
     k_colmax<<<g, 256, 0, st>>>(d->table + (uint64_t)lo * n, n, L, s->d_kmax + lo);
     count_launch();
     FC_CUDA_TRY(cudaGetLastError());
@@ -515,10 +533,16 @@ static fc_status build_hist(DeviceGraph* d, cudaStream_t st, uint32_t lo, uint32
     FC_CUDA_TRY(cudaMemsetAsync(s->H, 0, hw * 4 + 4, st));
     FC_CUDA_TRY(cudaMemsetAsync(s->N, 0, nw * 4 + 4, st));
     if (n && L) {
-        dim3 tg((n + 31) / 32, (L + 31) / 32);
-        k_transpose<<<tg, dim3(32, 8), 0, st>>>(d->table, n, L, s->coreT);
+        if (L < 32) {
+            const uint32_t tb =
+                std::max<uint32_t>(1u, std::min<uint32_t>((n + 255) / 256, 8u * sm_count()));
+            k_transpose_rows<<<tb, 256, 0, st>>>(d->table, n, L, s->coreT);
+        } else {
+            dim3 tg((n + 31) / 32, (L + 31) / 32);
+            k_transpose<<<tg, dim3(32, 8), 0, st>>>(d->table, n, L, s->coreT);
+        }
         FC_CUDA_TRY(cudaGetLastError());
-        dim3 ng((n + 255) / 256 < 32 ? (n + 255) / 256 : 32, hi - lo);
+        dim3 ng(per_col, hi - lo);
         k_node_hist<<<ng, 256, 12288 * 4, st>>>(d->table + (uint64_t)lo * n, n, s->d_nbase + lo,
                                                s->d_kmax + lo, s->N);
         count_launch(2);
@@ -772,6 +796,7 @@ void densest_preload() {
     cudaFuncAttributes a;
     cudaFuncGetAttributes(&a, k_colmax);
     cudaFuncGetAttributes(&a, k_transpose);
+    cudaFuncGetAttributes(&a, k_transpose_rows);
     cudaFuncGetAttributes(&a, k_node_hist);
     cudaFuncGetAttributes(&a, k_edge_hist<EH_SCALAR>);
     cudaFuncGetAttributes(&a, k_edge_hist<EH_V4>);
