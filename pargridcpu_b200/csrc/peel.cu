@@ -1729,15 +1729,20 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame(
 // and lists, and every block reaches the others' shared memory directly
 // (distributed shared memory).  A level is a SCAN round, in which each block
 // scans its own survivors, then DRAIN rounds: in each, every block expands
-// the rows of its own nodes queued in the round before, and a removal it
-// causes is queued on the removed node's owner for the next round.  Rounds
-// are separated by cluster barriers.  Block 0 holds, per round (three of
-// them in rotation), the cluster-wide counts of nodes queued and of nodes a
-// scan kept; every block reads them right after the round's barrier, so all
-// blocks take the same decisions.  The queue of round r+1 is the other half
-// of a two-half queue, so a block never reads a slot another block may still
-// be writing.  Every loop is bounded as in k_endgame, and no block leaves
-// while another may still reach its shared memory.
+// the rows of its own nodes queued in the round before and its slice of
+// every long row on block 0's list.  A removal its threads cause goes to
+// that list when the node's row is long, else to one of the block's local
+// halves, whose rows the block expands at once in further local iterations
+// (separated by block barriers) until its threads cause no removal; only a
+// removal that finds the local half full is queued on the removed node's
+// owner for the next round.  Rounds are separated by cluster barriers.
+// Block 0 holds, per round (three of them in rotation), the cluster-wide
+// counts of nodes queued and of nodes a scan kept, and the long-row list;
+// every block reads them right after the round's barrier, so all blocks take
+// the same decisions.  The queue of round r+1 is the other half of a
+// two-half queue, so a block never reads a slot another block may still be
+// writing.  Every loop is bounded as in k_endgame, and no block leaves while
+// another may still reach its shared memory.
 constexpr uint32_t EGC_MAX = 16;
 // The count half of a node that is not kept in the current level: decrements
 // of a removed node's count (at most L, one per layer degree passing k + 1)
@@ -1749,7 +1754,8 @@ constexpr uint32_t EGC_DEAD2 = 0x80008000u;
 // its row is long; a removed node's never matches lmd in bits 0-13.
 constexpr uint32_t EGC_BIG = 0x4000u;
 constexpr uint32_t EGC_CNT = 0x3FFFu;
-// Long rows queued in one round, per cluster (more go to their owners)
+// Long rows listed in one round, per cluster (more are expanded like short
+// rows, by the block that found them removed or by their owners)
 constexpr uint32_t EGC_BIG_MAX = 256;
 // Capacity of each of a block's two local halves: rows found removed by the
 // block's own threads, expanded by the block before the round ends
@@ -2210,7 +2216,10 @@ static uint32_t eg_cluster_size() {
 }
 
 // Rows longer than this are expanded by every block of the cluster, a slice
-// each, instead of by their owner alone: FC_PEEL_EG_SPLIT (entries; 0 = never)
+// each, in the round after their node's removal, instead of by one block:
+// FC_PEEL_EG_SPLIT (entries; 0 = never).  2048 measured best with local
+// iterations (shorter rows then cascade inside a block; longer ones would
+// leave one block with the dense core's ~6,400-entry rows).
 static uint32_t eg_split() {
     static const uint32_t v = env_u32("FC_PEEL_EG_SPLIT", 2048);
     return v;
