@@ -54,3 +54,14 @@ def test_reference_arm_line_on_c1():
 def test_reference_arm_c4_is_unavailable_not_an_error():
     d = bench_line("--impl", "reference", "--workload", "c4", "--steps", "1", "--warmup", "0")
     assert d["impl"] == "reference" and d["unavailable"]
+
+
+def test_reference_arm_other_ranks_exit_without_work():
+    # under torchrun rank 0 alone times the reference; the others print nothing
+    env = dict(os.environ, RANK="1", LOCAL_RANK="1", WORLD_SIZE="2",
+               MASTER_ADDR="127.0.0.1", MASTER_PORT="29533")
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                          "--workload", "c1", "--gpus", "2", "--steps", "1", "--warmup", "0"],
+                         cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    assert not [l for l in out.stdout.splitlines() if l.startswith("{")]
