@@ -155,3 +155,74 @@ def test_oracle_matches_reference_on_the_c4_mix_sample():
         assert np.float32(d["max_density_f"]) == np.float32(f["max_density_f"])
         if d["k"]:
             assert d["density"] == f["density"]
+
+
+def brute_force_table(layers, ids):
+    """The (k, lambda)-core index straight from its definition, for tiny
+    graphs: core_lambda(v) is the largest k such that v belongs to a node set
+    in which every node has at least k neighbours inside the set in at least
+    lambda layers.  For each lambda and k = 1, 2, ... nodes are removed from
+    the previous k's set until every one left qualifies (the largest such set
+    is unique: the union of qualifying sets qualifies).  Self-loops and
+    repeated pairs count once, as undirected edges without loops."""
+    L, n = len(layers), len(ids)
+    pos = {int(v): i for i, v in enumerate(ids)}
+    nb = [[set() for _ in range(n)] for _ in range(L)]
+    for l, e in enumerate(layers):
+        for u, v in np.asarray(e, np.int64).reshape(-1, 2):
+            if u != v:
+                nb[l][pos[int(u)]].add(pos[int(v)])
+                nb[l][pos[int(v)]].add(pos[int(u)])
+    t = np.zeros((L, n), np.uint32)
+    for lam in range(1, L + 1):
+        alive = set(range(n))
+        k = 1
+        while alive:
+            changed = True
+            while changed:
+                changed = False
+                for v in list(alive):
+                    if sum(len(nb[l][v] & alive) >= k for l in range(L)) < lam:
+                        alive.discard(v)
+                        changed = True
+            for v in alive:
+                t[lam - 1, v] = k
+            k += 1
+    return t
+
+
+def _tiny_cases():
+    from pargridcpu_b200 import synth
+    rng = np.random.default_rng(77)
+    cases = []
+    for seed in range(4):  # random multilayer graphs
+        g = synth.chung_lu_graph(48, 5, 120, 2.2, 0.5, 500 + seed)
+        cases.append((f"chung_lu_{seed}", g.layers))
+    cases.append(("one_layer", synth.chung_lu_graph(60, 1, 200, 2.2, 0.0, 42).layers))
+    # more than 32 layers: Top-lambda over a block of layers
+    cases.append(("33_layers", synth.erdos_renyi_graph(24, 33, 0.1, 0.3, 43).layers))
+    # an empty layer, nodes isolated in some layers, repeated pairs, self-loops
+    a = rng.integers(0, 30, (150, 2))
+    b = rng.integers(10, 40, (90, 2))
+    dup = np.concatenate([a[:40], a[:40], [[5, 5], [7, 7], [5, 9]]])
+    cases.append(("empty_dup_loops", [a, np.zeros((0, 2), np.int64), b, dup]))
+    return cases
+
+
+@pytest.mark.parametrize("name,layers", _tiny_cases(), ids=[c[0] for c in _tiny_cases()])
+def test_oracle_matches_the_definition_on_tiny_graphs(name, layers):
+    og = O.OracleGraph(layers)
+    assert np.array_equal(og.coreindex(), brute_force_table(layers, og.id2vtx()))
+
+
+def test_node_relabelling_permutes_the_table():
+    """Renaming the vertex ids (a bijection) leaves the first-seen numbering's
+    positions, hence the table, unchanged, and id2vtx renamed alike."""
+    from pargridcpu_b200 import synth
+    g = synth.chung_lu_graph(200, 4, 700, 2.3, 0.4, 909)
+    og = O.OracleGraph(g.layers)
+    top = int(max(int(np.asarray(e).max(initial=0)) for e in g.layers)) + 1
+    ren = np.random.default_rng(5).permutation(top).astype(np.int64) * 3 + 11
+    og2 = O.OracleGraph([ren[np.asarray(e, np.int64)] for e in g.layers])
+    assert np.array_equal(og2.coreindex(), og.coreindex())
+    assert np.array_equal(og2.id2vtx(), ren[og.id2vtx().astype(np.int64)].astype(np.uint64))
