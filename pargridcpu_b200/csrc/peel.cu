@@ -1746,8 +1746,9 @@ __global__ void __launch_bounds__(EG_THREADS) k_endgame(
 constexpr uint32_t EGC_MAX = 16;
 // The count half of a node that is not kept in the current level: decrements
 // of a removed node's count (at most L, one per layer degree passing k + 1)
-// leave it far above any lmd, and never borrow (L is at most 100 here: the
-// block capacity needs 2L + 11 shared bytes per survivor).
+// leave it far above any lmd, and never borrow (L is at most 96 here: a
+// block holds at least 1024 survivors at 2L + 11 shared bytes each, beside
+// its fixed arrays; for larger L the cluster endgame is not used).
 constexpr uint32_t EGC_DEAD = 0x8000u;
 constexpr uint32_t EGC_DEAD2 = 0x80008000u;
 // A kept node's count half is its count (bits 0-13) and, in bit 14, whether
